@@ -1,0 +1,393 @@
+"""B200-native fermion hot path of CLGLib (CudaLatticeGauge).
+
+Python mirror of the reference's field / operator / solver interface over the
+C ABI of ``libclgb200.so`` (include/clg_b200.h).  Class and method names follow
+the reference (Code/CLGLib/...):
+
+  CFieldGaugeSU3                 Data/Field/Gauge/CFieldGaugeSU3.h:18-121
+  CFieldFermionWilsonSquareSU3   Data/Field/WilsonDirac/CFieldFermionWilsonSquareSU3.h
+  CFieldFermionKSSU3             Data/Field/Staggered/CFieldFermionKSSU3.h
+  CSLASolverGMRES / BiCGStab     SparseLinearAlgebra/CSolverGMRES.cpp, CSolverBiCGstab.cpp
+  CMultiShiftCG / CMultiShiftFOM SparseLinearAlgebra/CMultiShiftSolver.h:38-47
+
+Every device computation runs in the CUDA library; there is no Python or CPU
+fallback: without the library or a B200 the calls raise CLGError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libclgb200.so")
+
+# ------------------------------------------------------------------ enums (include/clg_b200.h)
+SUCCESS, ERR_BAD_ARG, ERR_CUDA, ERR_OOM, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(9)
+
+EFO_F_D, EFO_F_Ddagger, EFO_F_DDdagger, EFO_F_DD = 0, 1, 2, 3
+OP_MEE, OP_MEE_DAG, OP_MEE_MEEDAG, OP_DEO, OP_DOE, OP_DDDAG_EE = 4, 5, 6, 7, 8, 9
+EOCT_None, EOCT_Minus, EOCT_Real, EOCT_Complex = 0, 1, 2, 3
+WILSON, STAGGERED = 0, 1
+FULL, EVEN = 0, 1
+DOUBLE, SINGLE, HALF = 0, 1, 2
+LAYOUT_CLGBIN, LAYOUT_BRIDGEPP = 0, 1
+GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH = 0, 1, 2
+SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT = 0, 1, 2, 3
+SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS = 0, 1, 2, 3, 4
+
+
+class CLGError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class SolverParams(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("max_dim", C.c_int32), ("restart", C.c_int32), ("accuracy", C.c_double),
+        ("absolute_accuracy", C.c_int32), ("deviation_step", C.c_int32), ("max_step", C.c_int32),
+        ("small_rho", C.c_double), ("inner_precision", C.c_int32), ("tol_true_rel", C.c_double),
+        ("inner_tol", C.c_double), ("max_iterations", C.c_int32), ("max_outer", C.c_int32),
+        ("even_odd", C.c_int32), ("use_graphs", C.c_int32),
+    ]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32), ("outer", C.c_int32),
+        ("true_rel_residual", C.c_double), ("seconds", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# (name, restype, argtypes) for every entry point of include/clg_b200.h
+_P, _I, _D, _U64, _U32, _I64 = C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_uint32, C.c_int64
+_S = C.c_int32
+SIGNATURES = [
+    ("clg_context_create", _S, [_I, _P, C.POINTER(_P)]),
+    ("clg_context_destroy", _S, [_P]),
+    ("clg_context_set_stream", _S, [_P, _P]),
+    ("clg_context_synchronize", _S, [_P]),
+    ("clg_status_string", C.c_char_p, [_S]),
+    ("clg_last_error", C.c_char_p, [_P]),
+    ("clg_context_kernel_count", _S, [_P, C.POINTER(_I64)]),
+    ("clg_lattice_create", _S, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_P)]),
+    ("clg_lattice_destroy", _S, [_P]),
+    ("clg_gauge_create", _S, [_P, C.POINTER(_P)]),
+    ("clg_gauge_destroy", _S, [_P]),
+    ("clg_gauge_import", _S, [_P, _P, _I, _I]),
+    ("clg_gauge_export", _S, [_P, _P, _I]),
+    ("clg_gauge_random", _S, [_P, _I, _U64, _U32, _D]),
+    ("clg_gauge_plaquette", _S, [_P, C.POINTER(_D)]),
+    ("clg_gauge_unitarity", _S, [_P, C.POINTER(_D)]),
+    ("clg_field_create", _S, [_P, _I, _I, _I, _I, _D, C.POINTER(_P)]),
+    ("clg_field_destroy", _S, [_P]),
+    ("clg_field_set_param", _S, [_P, _D]),
+    ("clg_field_import", _S, [_P, _I, _P, _I]),
+    ("clg_field_export", _S, [_P, _I, _P, _I]),
+    ("clg_field_random", _S, [_P, _I, _I, _U64, _U32, _I64, _I]),
+    ("clg_field_copy", _S, [_P, _P]),
+    ("clg_apply", _S, [_I, _P, _P, _I, _D, _D]),
+    ("clg_apply_to", _S, [_I, _P, _P, _P, _I, _D, _D]),
+    ("clg_dot", _S, [_P, _P, _P]),
+    ("clg_norm2", _S, [_P, _P]),
+    ("clg_axpy", _S, [_P, _D, _D, _P]),
+    ("clg_scale", _S, [_P, _D, _D]),
+    ("clg_zero", _S, [_P]),
+    ("clg_solver_default_params", _S, [_I, C.POINTER(SolverParams)]),
+    ("clg_solver_create", _S, [_P, C.POINTER(SolverParams), C.POINTER(_P)]),
+    ("clg_solver_destroy", _S, [_P]),
+    ("clg_solve", _S, [_P, _P, _P, _P, _I, _P, _P]),
+    ("clg_solve_multishift", _S, [_P, _P, _I, _P, _P, _P, _I, _P]),
+    ("clg_rational_apply", _S, [_P, _P, _P, _I, _I, _D, _P, _P, _P]),
+]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libclgb200.so (raises CLGError if it is missing: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise CLGError(ERR_NO_DEVICE, f"{path} is missing; build it with `python -m cudalatticegauge_b200.build`")
+    lib = C.CDLL(path)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return C.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """CUDA device + stream that owns every object created from it."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.clg_context_create(device, C.c_void_p(stream) if stream else None, C.byref(h))
+        if st != SUCCESS:
+            raise CLGError(st, f"clg_context_create: {self.lib.clg_status_string(st).decode()}")
+        self.h = h
+
+    def check(self, st: int, what: str):
+        if st != SUCCESS:
+            raise CLGError(st, f"{what}: {self.lib.clg_status_string(st).decode()}: {self.lib.clg_last_error(self.h).decode()}")
+
+    def synchronize(self):
+        self.check(self.lib.clg_context_synchronize(self.h), "synchronize")
+
+    def set_stream(self, stream: Optional[int]):
+        self.check(self.lib.clg_context_set_stream(self.h, C.c_void_p(stream) if stream else None), "set_stream")
+
+    def kernel_count(self) -> int:
+        n = C.c_int64()
+        self.check(self.lib.clg_context_kernel_count(self.h, C.byref(n)), "kernel_count")
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.clg_context_destroy(self.h)
+            self.h = None
+
+
+class Lattice:
+    def __init__(self, ctx: Context, dims: Sequence[int], fermion_bc: Sequence[int] = (1, 1, 1, -1)):
+        self.ctx, self.dims, self.bc = ctx, tuple(int(d) for d in dims), tuple(int(b) for b in fermion_bc)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.clg_lattice_create(ctx.h, (C.c_int * 4)(*self.dims), (C.c_int * 4)(*self.bc), C.byref(h)),
+                  "clg_lattice_create")
+        self.h = h
+        self.volume = int(np.prod(self.dims))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.clg_lattice_destroy(self.h)
+            self.h = None
+
+
+class CFieldGaugeSU3:
+    """SU(3) gauge field (Data/Field/Gauge/CFieldGaugeSU3.h:18-121)."""
+
+    def __init__(self, lattice: Lattice):
+        self.lat, self.ctx = lattice, lattice.ctx
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.clg_gauge_create(lattice.h, C.byref(h)), "clg_gauge_create")
+        self.h = h
+
+    def InitialField(self, kind: int, seed: int = 0, field_id: int = 1, eps: float = 0.0):
+        self.ctx.check(self.ctx.lib.clg_gauge_random(self.h, kind, seed, field_id, eps), "clg_gauge_random")
+
+    def InitialWithByte(self, links: np.ndarray, layout: int = LAYOUT_CLGBIN):
+        """links: complex128 [V*4, 3, 3] (or float64 raw 18 reals per link) in CLGBin or Bridge++ order."""
+        a = np.ascontiguousarray(links)
+        if a.dtype == np.complex128:
+            a = a.view(np.float64)
+        a = np.ascontiguousarray(a, np.float64)
+        if a.size != self.lat.volume * 4 * 18:
+            raise CLGError(ERR_BAD_ARG, "gauge data has the wrong size")
+        self.ctx.check(self.ctx.lib.clg_gauge_import(self.h, _ptr(a), layout, 0), "clg_gauge_import")
+
+    def CopyDataOut(self) -> np.ndarray:
+        out = np.empty((self.lat.volume * 4, 3, 3), np.complex128)
+        self.ctx.check(self.ctx.lib.clg_gauge_export(self.h, _ptr(out), 0), "clg_gauge_export")
+        return out
+
+    def plaquette(self) -> float:
+        v = C.c_double()
+        self.ctx.check(self.ctx.lib.clg_gauge_plaquette(self.h, C.byref(v)), "clg_gauge_plaquette")
+        return v.value
+
+    def unitarity(self) -> float:
+        v = C.c_double()
+        self.ctx.check(self.ctx.lib.clg_gauge_unitarity(self.h, C.byref(v)), "clg_gauge_unitarity")
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.clg_gauge_destroy(self.h)
+            self.h = None
+
+
+class _FermionField:
+    KIND = WILSON
+    NC = 12
+
+    def __init__(self, lattice: Lattice, param: float, subset: int = FULL, precision: int = DOUBLE, nrhs: int = 1):
+        self.lat, self.ctx = lattice, lattice.ctx
+        self.subset, self.precision, self.nrhs, self.param = subset, precision, nrhs, param
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.clg_field_create(lattice.h, self.KIND, subset, precision, nrhs, param, C.byref(h)),
+                       "clg_field_create")
+        self.h = h
+
+    # ------------------------------------------------------------ data movement (CLGBin order)
+    def _shape(self):
+        return (self.lat.volume, 4, 3) if self.NC == 12 else (self.lat.volume, 3)
+
+    def from_numpy(self, data: np.ndarray, rhs: int = 0):
+        a = np.ascontiguousarray(data, np.complex128)
+        if a.size != self.lat.volume * self.NC:
+            raise CLGError(ERR_BAD_ARG, "field data has the wrong size")
+        self.ctx.check(self.ctx.lib.clg_field_import(self.h, rhs, _ptr(a), 0), "clg_field_import")
+
+    def to_numpy(self, rhs: int = 0) -> np.ndarray:
+        out = np.empty(self._shape(), np.complex128)
+        self.ctx.check(self.ctx.lib.clg_field_export(self.h, rhs, _ptr(out), 0), "clg_field_export")
+        return out
+
+    def InitialField(self, kind: int, seed: int = 0, field_id: int = 2, rhs: int = 0, site: int = 0, comp: int = 0):
+        self.ctx.check(self.ctx.lib.clg_field_random(self.h, rhs, kind, seed, field_id, site, comp), "clg_field_random")
+
+    def InitialAsSource(self, site: int, comp: int, rhs: int = 0):
+        self.InitialField(SOURCE_POINT, rhs=rhs, site=site, comp=comp)
+
+    # ------------------------------------------------------------ operators (CField::ApplyOperator)
+    def ApplyOperator(self, op: int, gauge: CFieldGaugeSU3, coeff_type: int = EOCT_None, cre: float = 1.0,
+                      cim: float = 0.0):
+        self.ctx.check(self.ctx.lib.clg_apply(op, self.h, gauge.h, coeff_type, cre, cim), "clg_apply")
+
+    def apply_to(self, op: int, out: "_FermionField", gauge: CFieldGaugeSU3, coeff_type: int = EOCT_None,
+                 cre: float = 1.0, cim: float = 0.0):
+        self.ctx.check(self.ctx.lib.clg_apply_to(op, out.h, self.h, gauge.h, coeff_type, cre, cim), "clg_apply_to")
+
+    def D(self, gauge, coeff_type=EOCT_None, cre=1.0, cim=0.0):
+        self.ApplyOperator(EFO_F_D, gauge, coeff_type, cre, cim)
+
+    def Ddagger(self, gauge, coeff_type=EOCT_None, cre=1.0, cim=0.0):
+        self.ApplyOperator(EFO_F_Ddagger, gauge, coeff_type, cre, cim)
+
+    def DDdagger(self, gauge, coeff_type=EOCT_None, cre=1.0, cim=0.0):
+        self.ApplyOperator(EFO_F_DDdagger, gauge, coeff_type, cre, cim)
+
+    # ------------------------------------------------------------ BLAS (CField.h:127-201)
+    def Dot(self, other: "_FermionField"):
+        out = np.zeros(2 * self.nrhs)
+        self.ctx.check(self.ctx.lib.clg_dot(self.h, other.h, _ptr(out)), "clg_dot")
+        z = out[0::2] + 1j * out[1::2]
+        return z[0] if self.nrhs == 1 else z
+
+    def norm2(self):
+        out = np.zeros(self.nrhs)
+        self.ctx.check(self.ctx.lib.clg_norm2(self.h, _ptr(out)), "clg_norm2")
+        return out[0] if self.nrhs == 1 else out
+
+    def Axpy(self, a, other: "_FermionField"):
+        a = complex(a)
+        self.ctx.check(self.ctx.lib.clg_axpy(self.h, a.real, a.imag, other.h), "clg_axpy")
+
+    def AxpyPlus(self, other):
+        self.Axpy(1.0, other)
+
+    def AxpyMinus(self, other):
+        self.Axpy(-1.0, other)
+
+    def ScalarMultply(self, a):
+        a = complex(a)
+        self.ctx.check(self.ctx.lib.clg_scale(self.h, a.real, a.imag), "clg_scale")
+
+    def Zero(self):
+        self.ctx.check(self.ctx.lib.clg_zero(self.h), "clg_zero")
+
+    def CopyTo(self, other: "_FermionField"):
+        self.ctx.check(self.ctx.lib.clg_field_copy(other.h, self.h), "clg_field_copy")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.clg_field_destroy(self.h)
+            self.h = None
+
+
+class CFieldFermionWilsonSquareSU3(_FermionField):
+    """Wilson fermion, param = Hopping (kappa)."""
+    KIND, NC = WILSON, 12
+
+
+class CFieldFermionKSSU3(_FermionField):
+    """Staggered (Kogut-Susskind) fermion, param = Mass (= 2am)."""
+    KIND, NC = STAGGERED, 3
+
+
+class _Solver:
+    KIND = SOLVER_GMRES
+
+    def __init__(self, ctx: Context, **kw):
+        self.ctx = ctx
+        p = SolverParams()
+        ctx.check(ctx.lib.clg_solver_default_params(self.KIND, C.byref(p)), "clg_solver_default_params")
+        names = {
+            "MaxDim": "max_dim", "Restart": "restart", "Accuracy": "accuracy", "AbsoluteAccuracy": "absolute_accuracy",
+            "DiviationStep": "deviation_step", "MaxStep": "max_step", "SmallRho": "small_rho",
+        }
+        for k, v in kw.items():
+            setattr(p, names.get(k, k), v)
+        self.params = p
+        h = C.c_void_p()
+        ctx.check(ctx.lib.clg_solver_create(ctx.h, C.byref(p), C.byref(h)), "clg_solver_create")
+        self.h = h
+
+    def Solve(self, x: _FermionField, b: _FermionField, gauge: CFieldGaugeSU3, op: int = EFO_F_D,
+              start: Optional[_FermionField] = None, raise_on_fail: bool = True):
+        infos = (SolveInfo * b.nrhs)()
+        st = self.ctx.lib.clg_solve(self.h, x.h, b.h, gauge.h, op, start.h if start else None, infos)
+        out = [i.as_dict() for i in infos]
+        if st != SUCCESS and raise_on_fail:
+            self.ctx.check(st, "clg_solve")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.clg_solver_destroy(self.h)
+            self.h = None
+
+
+class CSLASolverGMRES(_Solver):
+    KIND = SOLVER_GMRES
+
+
+class CSLASolverBiCGStab(_Solver):
+    KIND = SOLVER_BICGSTAB
+
+
+class CSLASolverCG(_Solver):
+    KIND = SOLVER_CG
+
+
+class _MultiShift(_Solver):
+    def Solve(self, xs: Sequence[_FermionField], shifts: Sequence[complex], b: _FermionField, gauge: CFieldGaugeSU3,
+              op: int = EFO_F_DDdagger, raise_on_fail: bool = True):
+        n = len(shifts)
+        arr = (C.c_void_p * n)(*[x.h.value for x in xs])
+        sh = np.ascontiguousarray(np.asarray(shifts, np.complex128).view(np.float64))
+        infos = (SolveInfo * n)()
+        st = self.ctx.lib.clg_solve_multishift(self.h, arr, n, _ptr(sh), b.h, gauge.h, op, infos)
+        out = [i.as_dict() for i in infos]
+        if st != SUCCESS and raise_on_fail:
+            self.ctx.check(st, "clg_solve_multishift")
+        return out
+
+
+class CMultiShiftCG(_MultiShift):
+    KIND = SOLVER_CGM
+
+
+class CMultiShiftFOM(_MultiShift):
+    KIND = SOLVER_FOM_MS
+
+
+def eo_parity(dims) -> np.ndarray:
+    """Parity (x+y+z+t)&1 of every site in CLG order."""
+    x, y, z, t = np.meshgrid(*[np.arange(n) for n in dims], indexing="ij")
+    return ((x + y + z + t) & 1).ravel()

@@ -1,0 +1,81 @@
+// clg_common.cuh -- shared device types for the B200 fermion hot path.
+//
+// Data layout in HBM (all fields even-odd split, structure of arrays):
+//   site s = ((x*Ly + y)*Lz + z)*Lt + t (the reference's order, Data/CCommonData.h:274-277),
+//   parity p = (x+y+z+t)&1, checkerboard index h = s >> 1 (Lt even), V_h = V/2.
+//   Wilson spinor, per parity and right-hand side, "chunk-major" [chunk][h]:
+//     FP64 : 12 x double2            (192 B / site)
+//     FP32 :  6 x float4             ( 96 B / site)
+//     FP16 :  3 x uint4 (4 half2)    ( 48 B / site) + float norm per site (4 B)
+//   staggered vector: FP64 3 x double2, FP32 3 x float2 (24 B), FP16 3 x half2 + norm.
+//   Gauge links, per parity p and direction mu, [chunk][h]:
+//     FP64 : 9 x double2 (18 reals)
+//     FP32 : 3 x float4 (12 reals: rows 0,1; row 2 = conj(row0 x row1))   or 9 x float2 (18 reals)
+//     FP16 : uint4 + uint2 (12 reals as 6 half2)
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace clg {
+
+enum Prec : int { P64 = 0, P32 = 1, P16 = 2 };
+
+struct Geom {
+  int L[4];      // Lx Ly Lz Lt
+  int bc[4];     // fermion boundary signs
+  int64_t V;     // volume
+  int64_t Vh;    // V/2
+};
+
+// ---------------------------------------------------------------- complex helpers
+template <typename T> struct cpx;
+template <> struct cpx<double> { double x, y; };
+template <> struct cpx<float> { float x, y; };
+
+template <typename T> __host__ __device__ __forceinline__ cpx<T> mk(T a, T b) { cpx<T> r; r.x = a; r.y = b; return r; }
+template <typename T> __device__ __forceinline__ cpx<T> operator+(cpx<T> a, cpx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __device__ __forceinline__ cpx<T> operator-(cpx<T> a, cpx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __device__ __forceinline__ cpx<T> operator*(cpx<T> a, cpx<T> b) {
+  return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T> __device__ __forceinline__ cpx<T> operator*(T s, cpx<T> a) { return mk<T>(s * a.x, s * a.y); }
+template <typename T> __device__ __forceinline__ cpx<T> cj(cpx<T> a) { return mk<T>(a.x, -a.y); }
+// conj(a) * b
+template <typename T> __device__ __forceinline__ cpx<T> cjmul(cpx<T> a, cpx<T> b) {
+  return mk<T>(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+// multiply by i^b (b known at compile time after unrolling)
+template <typename T> __device__ __forceinline__ cpx<T> mul_i(cpx<T> a, int b) {
+  switch (b & 3) {
+    case 0: return a;
+    case 1: return mk<T>(-a.y, a.x);
+    case 2: return mk<T>(-a.x, -a.y);
+    default: return mk<T>(a.y, -a.x);
+  }
+}
+
+// ---------------------------------------------------------------- geometry
+// Coordinates of the checkerboard site (parity p, index h).
+__device__ __forceinline__ void eo_coords(const Geom& g, int p, int64_t h, int c[4]) {
+  const int64_t s0 = 2 * h;
+  const int t0 = (int)(s0 % g.L[3]);
+  int64_t r = s0 / g.L[3];
+  c[2] = (int)(r % g.L[2]);
+  r /= g.L[2];
+  c[1] = (int)(r % g.L[1]);
+  c[0] = (int)(r / g.L[1]);
+  c[3] = t0 + ((c[0] + c[1] + c[2] + p) & 1);
+}
+__device__ __forceinline__ int64_t site_index(const Geom& g, const int c[4]) {
+  return (((int64_t)c[0] * g.L[1] + c[1]) * g.L[2] + c[2]) * g.L[3] + c[3];
+}
+
+// ---------------------------------------------------------------- errors
+#define CLG_CUDA_OK(expr)                                   \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) return clg::cuda_status(_e);     \
+  } while (0)
+
+}  // namespace clg

@@ -1,0 +1,173 @@
+// dslash.cu -- launchers for the checkerboard hopping kernels and the
+// low-precision link copies (12-real reconstruction) they read.
+#include <string>
+
+#include "dslash.cuh"
+#include "internal.h"
+
+namespace clg {
+
+namespace {
+
+// the launch is idempotent (safe to repeat while timing block sizes) unless
+// the output aliases the xpay source
+bool idempotent(const HopArgs& a) { return a.x == nullptr || a.x != a.out; }
+
+template <int P, int RECON>
+cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
+  auto go = [&](int bs) {
+    dim3 grid((unsigned)((a.g.Vh + bs - 1) / bs), (unsigned)nrhs);
+    if (dagger)
+      wilson_hop_kernel<P, RECON, true><<<grid, bs, 0, ctx->stream>>>(a);
+    else
+      wilson_hop_kernel<P, RECON, false><<<grid, bs, 0, ctx->stream>>>(a);
+    ctx->kernels++;
+    return cudaGetLastError();
+  };
+  return go(tune_block(ctx, key, idempotent(a), go));
+}
+
+template <int P, int RECON>
+cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
+  auto go = [&](int bs) {
+    dim3 grid((unsigned)((a.g.Vh + bs - 1) / bs), (unsigned)nrhs);
+    staggered_hop_kernel<P, RECON><<<grid, bs, 0, ctx->stream>>>(a);
+    ctx->kernels++;
+    return cudaGetLastError();
+  };
+  return go(tune_block(ctx, key, idempotent(a), go));
+}
+
+// FP64 [mu][9][h] double2 -> FP32 12-real [mu][3][h] float4 or 18-real [mu][9][h] float2
+__global__ void links_to_fp32(const double2* __restrict__ u64, void* out, int64_t Vh, int recon) {
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (h >= Vh) return;
+  const double2* src = u64 + (int64_t)mu * 9 * Vh + h;
+  if (recon == 12) {
+    float4* dst = reinterpret_cast<float4*>(out) + (int64_t)mu * 3 * Vh + h;
+    for (int k = 0; k < 3; ++k) {
+      const double2 a = src[(2 * k) * Vh], b = src[(2 * k + 1) * Vh];
+      dst[k * Vh] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+    }
+  } else {
+    float2* dst = reinterpret_cast<float2*>(out) + (int64_t)mu * 9 * Vh + h;
+    for (int k = 0; k < 9; ++k) {
+      const double2 a = src[k * Vh];
+      dst[k * Vh] = make_float2((float)a.x, (float)a.y);
+    }
+  }
+}
+
+// FP64 -> FP16 12-real: [mu][h] uint4 (u0..u3) then [mu][h] uint2 (u4, u5)
+__global__ void links_to_fp16(const double2* __restrict__ u64, void* out, int64_t Vh) {
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (h >= Vh) return;
+  const double2* src = u64 + (int64_t)mu * 9 * Vh + h;
+  uint32_t w[6];
+  for (int k = 0; k < 6; ++k) {
+    const double2 a = src[k * Vh];
+    __half2 hv = __floats2half2_rn((float)a.x, (float)a.y);
+    w[k] = *reinterpret_cast<uint32_t*>(&hv);
+  }
+  uint4* d4 = reinterpret_cast<uint4*>(out);
+  uint2* d2 = reinterpret_cast<uint2*>(d4 + 4 * Vh);
+  d4[(int64_t)mu * Vh + h] = make_uint4(w[0], w[1], w[2], w[3]);
+  d2[(int64_t)mu * Vh + h] = make_uint2(w[4], w[5]);
+}
+
+}  // namespace
+
+clg_status gauge_prepare(clg_gauge_s* U, int prec) {
+  if (prec == CLG_PREC_DOUBLE) return CLG_SUCCESS;
+  clg_context_s* ctx = U->lat->ctx;
+  const int64_t Vh = U->lat->g.Vh;
+  if (U->dirty_lowp) {
+    for (int p = 0; p < 2; ++p) {
+      dfree(U->u32[p]);
+      dfree(U->u16[p]);
+      U->u32[p] = U->u16[p] = nullptr;
+    }
+    U->dirty_lowp = false;
+  }
+  if (prec == CLG_PREC_HALF && !U->su3)
+    return ctx->fail(CLG_ERR_UNSUPPORTED, "half-precision links need SU(3) links (12-real reconstruction)");
+  for (int p = 0; p < 2; ++p) {
+    dim3 grid((unsigned)((Vh + 255) / 256), 4);
+    if (prec == CLG_PREC_SINGLE && !U->u32[p]) {
+      U->recon32 = U->su3 ? 12 : 18;
+      const size_t bytes = (size_t)4 * Vh * U->recon32 * 4;
+      clg_status st = dalloc(ctx, &U->u32[p], bytes);
+      if (st) return st;
+      links_to_fp32<<<grid, 256, 0, ctx->stream>>>((const double2*)U->u64[p], U->u32[p], Vh, U->recon32);
+      ctx->kernels++;
+      CLG_CUDA_OK(cudaGetLastError());
+    }
+    if (prec == CLG_PREC_HALF && !U->u16[p]) {
+      const size_t bytes = (size_t)4 * Vh * 24;
+      clg_status st = dalloc(ctx, &U->u16[p], bytes);
+      if (st) return st;
+      links_to_fp16<<<grid, 256, 0, ctx->stream>>>((const double2*)U->u64[p], U->u16[p], Vh);
+      ctx->kernels++;
+      CLG_CUDA_OK(cudaGetLastError());
+    }
+  }
+  return CLG_SUCCESS;
+}
+
+clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
+  const int p = s.out_parity;
+  if (!s.in.has_parity(1 - p) || !s.out.has_parity(p) || (s.x && !s.x->has_parity(p)))
+    return ctx->fail(CLG_ERR_BAD_ARG, "hop: field does not hold the required checkerboard");
+  if (s.in.prec != s.prec || s.out.prec != s.prec || (s.x && s.x->prec != s.prec))
+    return ctx->fail(CLG_ERR_BAD_ARG, "hop: precision mismatch");
+  HopArgs a;
+  a.g = U->lat->g;
+  a.out_parity = p;
+  a.in = s.in.base(0, 1 - p);
+  a.in_norm = s.in.nbase(0, 1 - p);
+  a.out = s.out.base(0, p);
+  a.out_norm = s.out.nbase(0, p);
+  a.x = s.x ? s.x->base(0, p) : nullptr;
+  a.x_norm = s.x ? s.x->nbase(0, p) : nullptr;
+  a.in_stride = s.in.rstride;
+  a.out_stride = s.out.rstride;
+  a.x_stride = s.x ? s.x->rstride : 0;
+  a.in_nstride = s.in.nrstride;
+  a.out_nstride = s.out.nrstride;
+  a.x_nstride = s.x ? s.x->nrstride : 0;
+  a.a = s.a;
+  a.xa = s.xa;
+  a.scale_dev = s.scale_dev;
+  a.scale_stride = s.scale_stride;
+  a.skip_dev = s.skip_dev;
+  a.skip_stride = s.skip_stride;
+  const bool wilson = s.kind == CLG_FERMION_WILSON;
+  std::string key = std::string(wilson ? "wilson" : "ks") + "_p" + std::to_string(s.prec) + "_d" +
+                    std::to_string((int)s.dagger) + "_V" + std::to_string((long long)a.g.Vh) + "_n" +
+                    std::to_string(s.nrhs);
+  cudaError_t e = cudaSuccess;
+  if (s.prec == CLG_PREC_DOUBLE) {
+    a.U_here = U->u64[p];
+    a.U_there = U->u64[1 - p];
+    e = wilson ? launch_wilson<P64, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P64, 18>(ctx, a, s.nrhs, key);
+  } else if (s.prec == CLG_PREC_SINGLE) {
+    a.U_here = U->u32[p];
+    a.U_there = U->u32[1 - p];
+    if (!a.U_here || !a.U_there) return ctx->fail(CLG_ERR_BAD_ARG, "hop: FP32 links not prepared");
+    if (U->recon32 == 12)
+      e = wilson ? launch_wilson<P32, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 12>(ctx, a, s.nrhs, key);
+    else
+      e = wilson ? launch_wilson<P32, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 18>(ctx, a, s.nrhs, key);
+  } else {
+    a.U_here = U->u16[p];
+    a.U_there = U->u16[1 - p];
+    if (!a.U_here || !a.U_there) return ctx->fail(CLG_ERR_BAD_ARG, "hop: FP16 links not prepared");
+    e = wilson ? launch_wilson<P16, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P16, 12>(ctx, a, s.nrhs, key);
+  }
+  if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("hop launch: ") + cudaGetErrorString(e));
+  return CLG_SUCCESS;
+}
+
+}  // namespace clg

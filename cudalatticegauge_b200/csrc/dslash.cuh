@@ -1,0 +1,236 @@
+// dslash.cuh -- Wilson and staggered hopping stencils on one checkerboard.
+//
+// Wilson (restating _kernelDFermionWilsonSquareSU3,
+// Data/Field/WilsonDirac/CFieldFermionWilsonSquareSU3.cu:32-163, as a hop):
+//   H psi(x)   = sum_mu [ s+ (1 - g_mu) U_mu(x) psi(x+mu) + s- (1 + g_mu) U_mu(x-mu)^+ psi(x-mu) ]
+//   H^+ psi(x) = the same with (1 -/+ g_mu) swapped   (D^+ = g5 D g5, :53-56, :149-152)
+// evaluated with spin projection: (1 -/+ g_mu) has rank two in the chiral basis of
+// Tools/Math/GammaMatrix.h:447-478, so two colour vectors are multiplied by the
+// link instead of four and the lower spin components are rebuilt by a phase.
+// D = 1 - kappa H on the full lattice is two checkerboard launches with
+// out_p = in_p - kappa H in_(1-p);  M_ee = 1 - kappa^2 H_eo H_oe (Docs/SparseLinearAlgebra/evenodd.tex:11-16).
+//
+// Staggered (restating _kernelDFermionKS, Data/Field/Staggered/CFieldFermionKSSU3.cu:33-117):
+//   H chi(x) = sum_mu eta_mu(x) [ s+ U_mu(x) chi(x+mu) - s- U_mu(x-mu)^+ chi(x-mu) ],
+//   D = 2am + H, D^+ = 2am - H, eta_mu(x) = (-1)^(x_0+..+x_(mu-1)) (Data/CCommonData.h:228-236).
+//
+// The epilogue computes out = xa * x + a * (H in), optionally times a real
+// device-resident scalar (used for lazily normalised Krylov vectors).
+#pragma once
+#include "field_io.cuh"
+
+namespace clg {
+
+struct HopArgs {
+  Geom g;
+  int out_parity;
+  const void* in;      // input spinors at parity 1-out_parity (rhs 0)
+  const float* in_norm;
+  void* out;           // output at out_parity
+  float* out_norm;
+  const void* x;       // xpay source at out_parity (nullable)
+  const float* x_norm;
+  const void* U_here;  // links of parity out_parity
+  const void* U_there; // links of parity 1-out_parity
+  int64_t in_stride;   // bytes between right-hand sides
+  int64_t out_stride;
+  int64_t x_stride;
+  int64_t in_nstride;  // floats between right-hand sides of the FP16 norms
+  int64_t out_nstride;
+  int64_t x_nstride;
+  double2 a;           // multiplies H in
+  double2 xa;          // multiplies x
+  const double* scale_dev;  // optional: whole result times scale_dev[rhs * scale_stride]
+  int scale_stride;
+  const int* skip_dev;      // optional: rhs with skip_dev[rhs * skip_stride] != 0 are not computed
+  int skip_stride;
+};
+
+// chiral gamma tables (GammaMatrix.h:447-478): row r -> column perm[r] with phase i^z4[r]
+__device__ __forceinline__ constexpr int gperm(int mu, int r) {
+  return (mu < 2) ? (3 - r) : ((r + 2) & 3);
+}
+__device__ __forceinline__ constexpr int gz4(int mu, int r) {
+  // mu=0: {3,3,1,1}; mu=1: {2,0,0,2}; mu=2: {3,1,1,3}; mu=3: {0,0,0,0}
+  return mu == 0 ? (r < 2 ? 3 : 1) : mu == 1 ? ((r == 0 || r == 3) ? 2 : 0) : mu == 2 ? ((r == 0 || r == 3) ? 3 : 1) : 0;
+}
+
+template <typename AT, bool DAG>
+__device__ __forceinline__ void su3_mv(const cpx<AT> u[9], const cpx<AT> v[3], cpx<AT> o[3]) {
+  if constexpr (!DAG) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) o[r] = u[3 * r] * v[0] + u[3 * r + 1] * v[1] + u[3 * r + 2] * v[2];
+  } else {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) o[r] = cjmul(u[r], v[0]) + cjmul(u[3 + r], v[1]) + cjmul(u[6 + r], v[2]);
+  }
+}
+
+// acc += s * P^{SGN}_mu (Udag? U^+ : U) psi   with P^{SGN} = (1 + SGN g_mu)
+template <typename AT, int MU, int SGN, bool UDAG>
+__device__ __forceinline__ void wilson_hop_dir(cpx<AT> acc[12], const cpx<AT> psi[12], const cpx<AT> u[9], AT s) {
+  constexpr int add = SGN < 0 ? 2 : 0;
+  cpx<AT> h0[3], h1[3], g0[3], g1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    h0[c] = psi[c] + mul_i(psi[3 * gperm(MU, 0) + c], gz4(MU, 0) + add);
+    h1[c] = psi[3 + c] + mul_i(psi[3 * gperm(MU, 1) + c], gz4(MU, 1) + add);
+  }
+  su3_mv<AT, UDAG>(u, h0, g0);
+  su3_mv<AT, UDAG>(u, h1, g1);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    g0[c] = s * g0[c];
+    g1[c] = s * g1[c];
+    acc[c] = acc[c] + g0[c];
+    acc[3 + c] = acc[3 + c] + g1[c];
+    // rows 2,3: coefficient SGN*i^z4[r] times the projected row perm[r] (in {0,1})
+    acc[6 + c] = acc[6 + c] + mul_i(gperm(MU, 2) == 0 ? g0[c] : g1[c], gz4(MU, 2) + add);
+    acc[9 + c] = acc[9 + c] + mul_i(gperm(MU, 3) == 0 ? g0[c] : g1[c], gz4(MU, 3) + add);
+  }
+}
+
+struct NbrInfo {
+  int64_t hf[4], hb[4];
+  float sf[4], sb[4];
+};
+
+__device__ __forceinline__ void neighbours(const Geom& g, int p, int64_t h, NbrInfo& nb, int c[4]) {
+  eo_coords(g, p, h, c);
+  const int64_t s = site_index(g, c);
+  int64_t st[4];
+  st[3] = 1;
+  st[2] = g.L[3];
+  st[1] = (int64_t)g.L[2] * g.L[3];
+  st[0] = (int64_t)g.L[1] * st[1];
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu) {
+    int64_t sf = s + st[mu], sb = s - st[mu];
+    float bf = 1.f, bb = 1.f;
+    if (c[mu] == g.L[mu] - 1) { sf -= (int64_t)g.L[mu] * st[mu]; bf = (float)g.bc[mu]; }
+    if (c[mu] == 0) { sb += (int64_t)g.L[mu] * st[mu]; bb = (float)g.bc[mu]; }
+    nb.hf[mu] = sf >> 1;
+    nb.hb[mu] = sb >> 1;
+    nb.sf[mu] = bf;
+    nb.sb[mu] = bb;
+  }
+}
+
+template <int P, int RECON, bool DAGGER>
+__global__ void __launch_bounds__(256) wilson_hop_kernel(HopArgs a) {
+  using AT = typename AccT<P>::T;
+  const int64_t Vh = a.g.Vh;
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (h >= Vh) return;
+  if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
+  const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
+  const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
+
+  NbrInfo nb;
+  int c[4];
+  neighbours(a.g, a.out_parity, h, nb, c);
+
+  cpx<AT> acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = mk<AT>(0, 0);
+
+  // D: forward (1 - g), backward (1 + g); D^+: swapped
+  constexpr int SF = DAGGER ? 1 : -1;
+  constexpr int SB = -SF;
+#define CLG_WILSON_DIR(MU)                                                              \
+  {                                                                                     \
+    cpx<AT> psi[12], u[9];                                                              \
+    load_site<P, 12, AT>(in, in_norm, Vh, nb.hf[MU], psi);                              \
+    load_link<P, RECON, AT>(a.U_here, MU, Vh, h, u);                                    \
+    wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (AT)nb.sf[MU]);                      \
+    load_site<P, 12, AT>(in, in_norm, Vh, nb.hb[MU], psi);                              \
+    load_link<P, RECON, AT>(a.U_there, MU, Vh, nb.hb[MU], u);                           \
+    wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU]);                       \
+  }
+  CLG_WILSON_DIR(0)
+  CLG_WILSON_DIR(1)
+  CLG_WILSON_DIR(2)
+  CLG_WILSON_DIR(3)
+#undef CLG_WILSON_DIR
+
+  const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = ca * acc[k];
+  if (a.x) {
+    cpx<AT> xv[12];
+    const char* xp = reinterpret_cast<const char*>(a.x) + rhs * a.x_stride;
+    load_site<P, 12, AT>(xp, a.x_norm ? a.x_norm + rhs * a.x_nstride : nullptr, Vh, h, xv);
+    const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = acc[k] + cx * xv[k];
+  }
+  if (a.scale_dev) {
+    const AT sc = (AT)a.scale_dev[rhs * a.scale_stride];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];
+  }
+  store_site<P, 12, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
+                        a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
+}
+
+template <int P, int RECON>
+__global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
+  using AT = typename AccT<P>::T;
+  const int64_t Vh = a.g.Vh;
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (h >= Vh) return;
+  if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
+  const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
+  const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
+
+  NbrInfo nb;
+  int c[4];
+  neighbours(a.g, a.out_parity, h, nb, c);
+
+  cpx<AT> acc[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) acc[k] = mk<AT>(0, 0);
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu) {
+    int es = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < mu) es += c[k];
+    const AT eta = (es & 1) ? (AT)-1 : (AT)1;
+    cpx<AT> v[3], u[9], o[3];
+    load_site<P, 3, AT>(in, in_norm, Vh, nb.hf[mu], v);
+    load_link<P, RECON, AT>(a.U_here, mu, Vh, h, u);
+    su3_mv<AT, false>(u, v, o);
+    const AT sf = eta * (AT)nb.sf[mu];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = acc[k] + sf * o[k];
+    load_site<P, 3, AT>(in, in_norm, Vh, nb.hb[mu], v);
+    load_link<P, RECON, AT>(a.U_there, mu, Vh, nb.hb[mu], u);
+    su3_mv<AT, true>(u, v, o);
+    const AT sb = -eta * (AT)nb.sb[mu];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = acc[k] + sb * o[k];
+  }
+  const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) acc[k] = ca * acc[k];
+  if (a.x) {
+    cpx<AT> xv[3];
+    const char* xp = reinterpret_cast<const char*>(a.x) + rhs * a.x_stride;
+    load_site<P, 3, AT>(xp, a.x_norm ? a.x_norm + rhs * a.x_nstride : nullptr, Vh, h, xv);
+    const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = acc[k] + cx * xv[k];
+  }
+  if (a.scale_dev) {
+    const AT sc = (AT)a.scale_dev[rhs * a.scale_stride];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = sc * acc[k];
+  }
+  store_site<P, 3, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
+                       a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
+}
+
+}  // namespace clg

@@ -1,0 +1,200 @@
+// internal.h -- host-side object model behind the C ABI (include/clg_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/clg_b200.h"
+#include "clg_common.cuh"
+
+namespace clg {
+
+clg_status cuda_status(cudaError_t e);
+
+// A view of one field: (rhs, parity) block at data + rhs*rstride + (p-first_parity)*blk.
+struct FieldRef {
+  char* data = nullptr;
+  float* norm = nullptr;   // FP16 per-site norms, same block structure in floats
+  int64_t blk = 0;         // bytes of one parity block
+  int64_t rstride = 0;     // bytes between right-hand sides
+  int64_t nrstride = 0;    // floats between right-hand sides (norms)
+  int nparity = 1;         // 2 = full field, 1 = single checkerboard
+  int first_parity = 0;    // parity of block 0
+  int prec = 0;
+  int nc = 12;             // complex per site (12 Wilson, 3 staggered)
+  int nrhs = 1;
+  int64_t Vh = 0;
+  __host__ __device__ char* base(int rhs, int p) const {
+    return data + (int64_t)rhs * rstride + (int64_t)(p - first_parity) * blk;
+  }
+  __host__ __device__ float* nbase(int rhs, int p) const {
+    return norm ? norm + (int64_t)rhs * nrstride + (int64_t)(p - first_parity) * Vh : nullptr;
+  }
+  bool has_parity(int p) const { return p >= first_parity && p < first_parity + nparity; }
+  FieldRef parity_view(int p) const {
+    FieldRef r = *this;
+    r.data = data + (int64_t)(p - first_parity) * blk;
+    r.norm = norm ? norm + (int64_t)(p - first_parity) * Vh : nullptr;
+    r.first_parity = p;
+    r.nparity = 1;
+    return r;
+  }
+  FieldRef rhs_view(int r0, int n) const {
+    FieldRef r = *this;
+    r.data = data + (int64_t)r0 * rstride;
+    r.norm = norm ? norm + (int64_t)r0 * nrstride : nullptr;
+    r.nrhs = n;
+    return r;
+  }
+};
+
+int64_t site_bytes_of(int prec, int nc);
+
+}  // namespace clg
+
+struct clg_context_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  int num_sms = 148;
+  int64_t kernels = 0;
+  // reduction scratch (device): partial sums and the arrival counter
+  double* red_partials = nullptr;
+  int64_t red_capacity = 0;  // doubles
+  unsigned int* red_counter = nullptr;
+  // block size chosen per kernel variant by the autotuner
+  std::map<std::string, int> tuned;
+  bool tuning_enabled = true;
+  clg_status fail(clg_status s, const std::string& msg) {
+    last_error = msg;
+    return s;
+  }
+};
+
+struct clg_lattice_s {
+  clg_context_s* ctx = nullptr;
+  clg::Geom g;
+};
+
+struct clg_gauge_s {
+  clg_lattice_s* lat = nullptr;
+  // per parity link arrays [mu][chunk][h]
+  void* u64[2] = {nullptr, nullptr};   // FP64, 18 reals
+  void* u32[2] = {nullptr, nullptr};   // FP32, 12 reals (SU(3)) or 18
+  void* u16[2] = {nullptr, nullptr};   // FP16, 12 reals (SU(3) only)
+  int recon32 = 12;
+  bool su3 = false;
+  bool dirty_lowp = true;  // low-precision copies need a rebuild
+  double unitarity = -1.0;
+};
+
+struct clg_field_s {
+  clg_lattice_s* lat = nullptr;
+  int kind = CLG_FERMION_WILSON;
+  int subset = CLG_SUBSET_FULL;
+  int prec = CLG_PREC_DOUBLE;
+  int nrhs = 1;
+  double param = 0.0;
+  char* data = nullptr;
+  float* norm = nullptr;
+  int64_t blk = 0;
+  int nparity() const { return subset == CLG_SUBSET_FULL ? 2 : 1; }
+  int nc() const { return kind == CLG_FERMION_WILSON ? 12 : 3; }
+  clg::FieldRef ref() const {
+    clg::FieldRef r;
+    r.data = data;
+    r.norm = norm;
+    r.blk = blk;
+    r.rstride = blk * nparity();
+    r.nrstride = norm ? (int64_t)nparity() * lat->g.Vh : 0;
+    r.nparity = nparity();
+    r.first_parity = 0;
+    r.prec = prec;
+    r.nc = nc();
+    r.nrhs = nrhs;
+    r.Vh = lat->g.Vh;
+    return r;
+  }
+};
+
+namespace clg {
+
+// ------------------------------------------------------------ device allocation
+clg_status dalloc(clg_context_s* ctx, void** p, size_t bytes);
+void dfree(void* p);
+clg_status ensure_reduction(clg_context_s* ctx, int64_t doubles);
+
+// ------------------------------------------------------------ launch helpers
+bool stream_capturing(cudaStream_t s);
+// Autotuner: the block size for kernel variant `key`.  On first use (outside
+// stream capture, when the launch is idempotent) each candidate block size is
+// timed with CUDA events on the context stream and the fastest is cached.
+template <class Go>
+int tune_block(clg_context_s* ctx, const std::string& key, bool can_repeat, Go&& go) {
+  auto it = ctx->tuned.find(key);
+  if (it != ctx->tuned.end()) return it->second;
+  const int fallback = 128;
+  if (!ctx->tuning_enabled || !can_repeat || stream_capturing(ctx->stream)) return fallback;
+  const int cand[4] = {64, 128, 256, 512};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return fallback;
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return fallback; }
+  int best = fallback;
+  float best_ms = 1e30f;
+  for (int bs : cand) {
+    if (go(bs) != cudaSuccess) continue;  // warm-up / validity
+    cudaEventRecord(e0, ctx->stream);
+    for (int r = 0; r < 3; ++r) go(bs);
+    cudaEventRecord(e1, ctx->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) { best_ms = ms; best = bs; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  ctx->tuned[key] = best;
+  return best;
+}
+
+// ------------------------------------------------------------ operators (dslash.cu)
+// A single checkerboard hop:  out_p = xa * x_p + a * H in_(1-p)  [ * scale_dev[rhs] ]
+struct HopSpec {
+  int kind;        // CLG_FERMION_WILSON / STAGGERED
+  int prec;
+  bool dagger;     // Wilson H^+ (ignored for staggered: the sign is in `a`)
+  int out_parity;
+  FieldRef in;     // must hold parity 1-out_parity
+  FieldRef out;    // must hold out_parity
+  const FieldRef* x;  // nullable, must hold out_parity
+  double2 a, xa;
+  const double* scale_dev;
+  int scale_stride;
+  const int* skip_dev;
+  int skip_stride;
+  int nrhs;
+};
+clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s);
+clg_status gauge_prepare(clg_gauge_s* U, int prec);  // builds the FP32 / FP16 copies on first use
+
+// ------------------------------------------------------------ operator composition (api.cu)
+// out = coeff * op(in) on fields of one precision. tmp: scratch with at least
+// the parity the operator needs (nullable: allocated internally).
+clg_status apply_op(clg_context_s* ctx, int op, const clg_gauge_s* U, int kind, double param,
+                    const FieldRef& out, const FieldRef& in, const FieldRef* tmp, double2 coeff, int nrhs,
+                    const double* scale_dev = nullptr, int scale_stride = 0, const int* skip_dev = nullptr,
+                    int skip_stride = 1);
+
+// ------------------------------------------------------------ BLAS (blas.cu)
+clg_status blas_dot(clg_context_s* ctx, const FieldRef& a, const FieldRef& b, double* dev_out);  // 2*nrhs doubles
+clg_status blas_norm2(clg_context_s* ctx, const FieldRef& a, double* dev_out);                    // nrhs doubles
+clg_status blas_axpby(clg_context_s* ctx, const FieldRef& y, double2 a, const FieldRef& x, double2 b);  // y = a x + b y
+clg_status blas_copy(clg_context_s* ctx, const FieldRef& dst, const FieldRef& src);               // converts precision
+clg_status blas_zero(clg_context_s* ctx, const FieldRef& y);
+
+}  // namespace clg

@@ -1,0 +1,690 @@
+// solvers.cu -- CSLASolver::Solve (SparseLinearAlgebra/CSLASolver.h:42-50) on the B200.
+//
+// Structure of one solve of  A x = b  (A = D, D^+, D D^+, M_ee, ...):
+//   outer loop in FP64 (defect correction / iterative refinement):
+//       r = b - A x            (FP64 operator, FP64 reductions)
+//       stop when |r| <= tol_true_rel |b| for every right-hand side
+//       e ~= A^{-1} r          (inner Krylov solve in the inner precision)
+//       x += e
+//   the inner solve of D (Wilson or staggered) goes through the even-odd Schur
+//   complement (Docs/SparseLinearAlgebra/evenodd.tex:11-16); its Krylov method is
+//   GMRES(k) (CSolverGMRES.cpp:111-358), BiCGStab (CSolverBiCGstab.cpp:403-607)
+//   or CG, with every scalar on the device and the iterations replayed from
+//   CUDA graphs.  All right-hand sides of a field are solved together: one
+//   launch per step covers every rhs, finished ones are skipped.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "krylov.cuh"
+
+namespace clg {
+
+__global__ void gm_solve_y(KState* st, int nrhs) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrhs) return;
+  KState& k = st[r];
+  if (k.done || k.j == 0) return;
+  const int m = k.j;
+  for (int i = m - 1; i >= 0; --i) {
+    double2 acc = k.g[i];
+    for (int l = i + 1; l < m; ++l) {
+      const double2 p = cmul(k.H[i * GM_MAXK + l], k.y[l]);
+      acc.x -= p.x;
+      acc.y -= p.y;
+    }
+    k.y[i] = cdiv(acc, k.H[i * GM_MAXK + i]);
+  }
+  for (int i = 0; i < m; ++i) k.y[i] = make_double2(k.y[i].x * k.s[i], k.y[i].y * k.s[i]);
+  if (k.resid_est * k.resid_est <= k.tol2 * k.rr0) k.status = ST_CONVERGED;
+}
+
+namespace {
+
+__global__ void gm_finish(KState* st, int nrhs) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrhs) return;
+  KState& k = st[r];
+  if (k.done) return;
+  if (k.status != ST_RUNNING) k.done = k.skip = 1;
+  k.j = 0;
+}
+
+__global__ void kstate_reset(KState* st, const int* outer_done, int nrhs) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrhs) return;
+  KState& k = st[r];
+  const int d = outer_done[r];
+  k.done = k.skip = d;
+  k.conv_s = 0;
+  k.status = d ? ST_CONVERGED : ST_RUNNING;
+  k.iters = 0;
+  k.j = 0;
+  k.rr = k.rr0 = 0.0;
+}
+
+struct Summary {
+  int done, status, iters, pad;
+  double rr, rr0, resid_est, pad2;
+};
+
+__global__ void kstate_summary(const KState* st, Summary* out, int nrhs) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrhs) return;
+  const KState& k = st[r];
+  out[r].done = k.done;
+  out[r].status = k.status;
+  out[r].iters = k.iters;
+  out[r].rr = k.rr;
+  out[r].rr0 = k.rr0;
+  out[r].resid_est = k.resid_est;
+}
+
+// x64 += e (converted), r64 = b64 - r64 are plain BLAS; this adds a lower-precision
+// correction into the FP64 iterate for the rhs still running.
+template <int PS, int NC>
+struct AddConv {
+  DField x, e;
+  const int* skip;
+  __device__ bool active(int r) const { return !skip[r]; }
+  __device__ void operator()(int rhs, int p, int64_t h, double*) const {
+    cpx<double> vx[NC], ve[NC];
+    load_site<P64, NC, double>(x.base(rhs, p), nullptr, x.Vh, h, vx);
+    load_site<PS, NC, double>(e.base(rhs, p), e.nbase(rhs, p), e.Vh, h, ve);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) vx[k] = vx[k] + ve[k];
+    store_site<P64, NC, double>(x.base(rhs, p), nullptr, x.Vh, h, vx);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
+// r = b - r ; |r|^2
+template <int NC>
+struct Resid {
+  DField b, r;
+  double* out;
+  __device__ bool active(int) const { return true; }
+  __device__ void operator()(int rhs, int p, int64_t h, double* acc) const {
+    cpx<double> vb[NC], vr[NC];
+    load_site<P64, NC, double>(b.base(rhs, p), nullptr, b.Vh, h, vb);
+    load_site<P64, NC, double>(r.base(rhs, p), nullptr, r.Vh, h, vr);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) vr[k] = vb[k] - vr[k];
+    store_site<P64, NC, double>(r.base(rhs, p), nullptr, r.Vh, h, vr);
+    acc[0] += site_norm2<NC, double>(vr);
+  }
+  __device__ void finalize(int rhs, const double* s) const { out[rhs] = s[0]; }
+};
+
+template <int P, int NC>
+struct CopySkip {
+  DField d, s;
+  const int* skip;
+  __device__ bool active(int r) const { return !skip[r]; }
+  __device__ void operator()(int rhs, int p, int64_t h, double*) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> v[NC];
+    ldv<P, NC, AT>(s, rhs, p, h, v);
+    stv<P, NC, AT>(d, rhs, p, h, v);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
+// ------------------------------------------------------------------ owned fields
+struct Owned {
+  FieldRef ref;
+  void* data = nullptr;
+  float* norm = nullptr;
+  Owned() = default;
+  Owned(const Owned&) = delete;
+  Owned& operator=(const Owned&) = delete;
+  ~Owned() {
+    dfree(data);
+    dfree(norm);
+  }
+  clg_status alloc(clg_context_s* ctx, int prec, int nc, int nparity, int first_parity, int nrhs, int64_t Vh) {
+    const int64_t blk = Vh * site_bytes_of(prec, nc);
+    clg_status st = dalloc(ctx, &data, (size_t)blk * nparity * nrhs);
+    if (st) return st;
+    if (prec == CLG_PREC_HALF) {
+      st = dalloc(ctx, (void**)&norm, (size_t)Vh * nparity * nrhs * sizeof(float));
+      if (st) return st;
+    }
+    ref.data = (char*)data;
+    ref.norm = norm;
+    ref.blk = blk;
+    ref.rstride = blk * nparity;
+    ref.nrstride = norm ? Vh * nparity : 0;
+    ref.nparity = nparity;
+    ref.first_parity = first_parity;
+    ref.prec = prec;
+    ref.nc = nc;
+    ref.nrhs = nrhs;
+    ref.Vh = Vh;
+    return CLG_SUCCESS;
+  }
+};
+
+bool hermitian_op(int op) { return op == CLG_OP_DDDAG || op == CLG_OP_DDDAG_EE || op == CLG_OP_MEE_MEEDAG; }
+
+}  // namespace
+
+}  // namespace clg
+
+using namespace clg;
+
+// ------------------------------------------------------------------ solver object
+struct clg_solver_s {
+  clg_context_s* ctx = nullptr;
+  clg_solver_params p;
+};
+
+namespace {
+
+// Everything one solve needs, allocated per call.
+struct Work {
+  clg_context_s* ctx;
+  clg_gauge_s* U;
+  int kind, op, P, nc, nrhs;
+  double param;
+  int64_t Vh;
+  const clg_solver_params* prm;
+  // device state
+  KState* st = nullptr;
+  Summary* sum_d = nullptr;
+  Summary* sum_h = nullptr;
+  int* outer_done_d = nullptr;
+  double* tol_d = nullptr;
+  double* red_d = nullptr;   // per-rhs reduction outputs
+  double* host_buf = nullptr;
+  // Krylov operator temporaries (precision P)
+  Owned kt_odd, kt_even, kt_full;
+  // Krylov vectors per graph slot: they persist for the whole solve so a
+  // captured graph stays valid across defect-correction cycles
+  std::map<int, std::vector<std::unique_ptr<Owned>>> kv;
+  // graphs
+  std::vector<cudaGraphExec_t> graphs;
+  int total_iters = 0;
+  clg_status kvec(int slot, int idx, int np, int fp, FieldRef& out) {
+    auto& v = kv[slot];
+    while ((int)v.size() <= idx) v.emplace_back(nullptr);
+    if (!v[idx]) {
+      v[idx].reset(new Owned());
+      clg_status s = v[idx]->alloc(ctx, P, nc, np, fp, nrhs, Vh);
+      if (s) {
+        v[idx].reset();
+        return s;
+      }
+    }
+    out = v[idx]->ref;
+    return CLG_SUCCESS;
+  }
+  ~Work() {
+    for (auto g : graphs)
+      if (g) cudaGraphExecDestroy(g);
+    dfree(st);
+    dfree(sum_d);
+    dfree(outer_done_d);
+    dfree(tol_d);
+    dfree(red_d);
+    if (sum_h) cudaFreeHost(sum_h);
+    if (host_buf) cudaFreeHost(host_buf);
+  }
+};
+
+clg_status read_summary(Work& w) {
+  kstate_summary<<<(w.nrhs + 63) / 64, 64, 0, w.ctx->stream>>>(w.st, w.sum_d, w.nrhs);
+  w.ctx->kernels++;
+  cudaError_t e = cudaMemcpyAsync(w.sum_h, w.sum_d, sizeof(Summary) * w.nrhs, cudaMemcpyDeviceToHost, w.ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(w.ctx->stream);
+  if (e != cudaSuccess) return w.ctx->fail(cuda_status(e), std::string("solver sync: ") + cudaGetErrorString(e));
+  return CLG_SUCCESS;
+}
+
+// Krylov operator K on fields of precision P: out = K in (optionally * scale_dev[rhs])
+clg_status kapply(Work& w, int op, const FieldRef& out, const FieldRef& in, const double* scale, int sstride,
+                  const int* skip, int kstride) {
+  const double2 one = make_double2(1, 0);
+  if (op == CLG_OP_MEE_MEEDAG) {
+    clg_status s = apply_op(w.ctx, CLG_OP_MEE_DAG, w.U, w.kind, w.param, w.kt_even.ref, in, &w.kt_odd.ref, one, w.nrhs,
+                            nullptr, 0, skip, kstride);
+    if (s) return s;
+    return apply_op(w.ctx, CLG_OP_MEE, w.U, w.kind, w.param, out, w.kt_even.ref, &w.kt_odd.ref, one, w.nrhs, scale,
+                    sstride, skip, kstride);
+  }
+  const FieldRef* tmp = (op == CLG_OP_DDDAG || op == CLG_OP_DD) ? &w.kt_full.ref : &w.kt_odd.ref;
+  return apply_op(w.ctx, op, w.U, w.kind, w.param, out, in, tmp, one, w.nrhs, scale, sstride, skip, kstride);
+}
+
+// Run `body` (one iteration or one cycle) repeatedly until every rhs is done
+// or the budget runs out.  Chunks after the first are replayed from a CUDA graph.
+template <class Body>
+clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& body) {
+  const bool graphs = w.prm->use_graphs && w.ctx->stream != nullptr;
+  while ((int)w.graphs.size() <= graph_slot) w.graphs.push_back(nullptr);
+  for (int c = 0; c < max_chunks; ++c) {
+    clg_status s = CLG_SUCCESS;
+    if (graphs && c > 0 && !w.graphs[graph_slot]) {
+      cudaGraph_t g = nullptr;
+      if (cudaStreamBeginCapture(w.ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        for (int i = 0; i < chunk && !s; ++i) s = body();
+        cudaError_t e = cudaStreamEndCapture(w.ctx->stream, &g);
+        if (!s && e == cudaSuccess && g) {
+          cudaGraphExec_t ex = nullptr;
+          if (cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) w.graphs[graph_slot] = ex;
+        }
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (s) return s;
+      } else {
+        cudaGetLastError();
+      }
+    }
+    if (graphs && w.graphs[graph_slot]) {
+      cudaError_t e = cudaGraphLaunch(w.graphs[graph_slot], w.ctx->stream);
+      if (e != cudaSuccess) return w.ctx->fail(cuda_status(e), std::string("graph launch: ") + cudaGetErrorString(e));
+    } else {
+      for (int i = 0; i < chunk && !s; ++i) s = body();
+      if (s) return s;
+    }
+    s = read_summary(w);
+    if (s) return s;
+    bool all = true;
+    int most = 0;
+    for (int r = 0; r < w.nrhs; ++r) {
+      all = all && w.sum_h[r].done;
+      most = std::max(most, w.sum_h[r].iters);
+    }
+    if (all || most >= w.prm->max_iterations) break;
+  }
+  return CLG_SUCCESS;
+}
+
+// ------------------------------------------------------------------ Krylov methods
+// Solve K x = b (precision P, the subset of b) for every rhs not marked in outer_done.
+clg_status krylov(Work& w, int op, const FieldRef& x, const FieldRef& b, int slot_base) {
+  clg_context_s* ctx = w.ctx;
+  const int nrhs = w.nrhs;
+  kstate_reset<<<(nrhs + 63) / 64, 64, 0, ctx->stream>>>(w.st, w.outer_done_d, nrhs);
+  ctx->kernels++;
+  const int ks = (int)(sizeof(KState) / sizeof(int));
+  const int* skip = &w.st[0].skip;
+  const int fp = b.first_parity, np = b.nparity;
+  const int64_t Vh = b.Vh;
+  const int method = w.prm->kind;
+  struct Ref {
+    FieldRef ref;
+  };
+  int vidx = 0;
+  auto vec = [&](Ref& o) { return w.kvec(slot_base, vidx++, np, fp, o.ref); };
+
+  if (method == CLG_SOLVER_BICGSTAB || (method == CLG_SOLVER_CG && !hermitian_op(op))) {
+    if (method == CLG_SOLVER_CG) return ctx->fail(CLG_ERR_BAD_ARG, "CG needs a Hermitian operator (DDdagger forms)");
+    Ref r, rh, p, v, t;
+    clg_status s;
+    if ((s = vec(r)) || (s = vec(rh)) || (s = vec(p)) || (s = vec(v)) || (s = vec(t))) return s;
+    s = with_pn(w.P, w.nc, [&](auto PP, auto NN) -> clg_status {
+      constexpr int PV = PP.value, NV = NN.value;
+      BiInit<PV, NV> init{dfield(b), dfield(x), dfield(r.ref), dfield(rh.ref), dfield(p.ref), w.st, w.tol_d};
+      clg_status q = launch_sites<1>(ctx, init, fp, np, Vh, nrhs);
+      if (q) return q;
+      auto body = [&]() -> clg_status {
+        clg_status e;
+        if ((e = kapply(w, op, v.ref, p.ref, nullptr, 0, skip, ks))) return e;
+        if ((e = launch_sites<2>(ctx, BiAlpha<PV, NV>{dfield(rh.ref), dfield(v.ref), w.st}, fp, np, Vh, nrhs))) return e;
+        if ((e = launch_sites<1>(ctx, BiS<PV, NV>{dfield(r.ref), dfield(v.ref), w.st}, fp, np, Vh, nrhs))) return e;
+        if ((e = kapply(w, op, t.ref, r.ref, nullptr, 0, skip, ks))) return e;
+        if ((e = launch_sites<3>(ctx, BiOmega<PV, NV>{dfield(t.ref), dfield(r.ref), w.st}, fp, np, Vh, nrhs))) return e;
+        BiUpdate<PV, NV> up{dfield(x), dfield(p.ref), dfield(r.ref), dfield(t.ref), dfield(rh.ref), w.st};
+        if ((e = launch_sites<3>(ctx, up, fp, np, Vh, nrhs))) return e;
+        return launch_sites<0>(ctx, BiP<PV, NV>{dfield(p.ref), dfield(r.ref), dfield(v.ref), w.st}, fp, np, Vh, nrhs);
+      };
+      const int chunk = 8;
+      return iterate(w, slot_base + 0, chunk, w.prm->max_iterations / (2 * chunk) + 2, body);
+    });
+    return s;
+  }
+
+  if (method == CLG_SOLVER_CG) {
+    Ref r, p, q;
+    clg_status s;
+    if ((s = vec(r)) || (s = vec(p)) || (s = vec(q))) return s;
+    return with_pn(w.P, w.nc, [&](auto PP, auto NN) -> clg_status {
+      constexpr int PV = PP.value, NV = NN.value;
+      CgInit<PV, NV> init{dfield(b), dfield(x), dfield(r.ref), dfield(p.ref), w.st, w.tol_d};
+      clg_status e = launch_sites<1>(ctx, init, fp, np, Vh, nrhs);
+      if (e) return e;
+      auto body = [&]() -> clg_status {
+        clg_status e2;
+        if ((e2 = kapply(w, op, q.ref, p.ref, nullptr, 0, skip, ks))) return e2;
+        if ((e2 = launch_sites<2>(ctx, CgAlpha<PV, NV>{dfield(p.ref), dfield(q.ref), w.st}, fp, np, Vh, nrhs))) return e2;
+        CgUpdate<PV, NV> up{dfield(x), dfield(r.ref), dfield(p.ref), dfield(q.ref), w.st};
+        if ((e2 = launch_sites<1>(ctx, up, fp, np, Vh, nrhs))) return e2;
+        return launch_sites<0>(ctx, CgP<PV, NV>{dfield(p.ref), dfield(r.ref), w.st}, fp, np, Vh, nrhs);
+      };
+      const int chunk = 16;
+      return iterate(w, slot_base + 1, chunk, w.prm->max_iterations / chunk + 2, body);
+    });
+  }
+
+  if (method == CLG_SOLVER_GMRES) {
+    const int k = std::min(std::max(w.prm->max_dim, 1), GM_MAXK);
+    Ref V[GM_MAXK + 1], wv;
+    clg_status s;
+    for (int i = 0; i <= k; ++i)
+      if ((s = vec(V[i]))) return s;
+    if ((s = vec(wv))) return s;
+    if ((s = blas_zero(ctx, x))) return s;
+    return with_pn(w.P, w.nc, [&](auto PP, auto NN) -> clg_status {
+      constexpr int PV = PP.value, NV = NN.value;
+      VList vl;
+      for (int i = 0; i <= GM_MAXK; ++i) vl.v[i] = dfield(V[std::min(i, k)].ref);
+      // first cycle start (x = 0)
+      GmStart<PV, NV> st0{dfield(b), dfield(wv.ref), dfield(V[0].ref), w.st, 0, w.tol_d, 1};
+      clg_status e = launch_sites<1>(ctx, st0, fp, np, Vh, nrhs);
+      if (e) return e;
+      bool first_cycle = true;
+      auto cycle = [&]() -> clg_status {
+        clg_status e2;
+        if (!first_cycle) {
+          // restart: V'_0 = b - K x
+          if ((e2 = kapply(w, op, wv.ref, x, nullptr, 0, &w.st[0].done, ks))) return e2;
+          GmStart<PV, NV> sr{dfield(b), dfield(wv.ref), dfield(V[0].ref), w.st, 1, w.tol_d, 0};
+          if ((e2 = launch_sites<1>(ctx, sr, fp, np, Vh, nrhs))) return e2;
+        }
+        for (int j = 0; j < k; ++j) {
+          if ((e2 = kapply(w, op, wv.ref, V[j].ref, &w.st[0].s[j], (int)(sizeof(KState) / sizeof(double)), skip, ks)))
+            return e2;
+          if ((e2 = launch_sites<2 * GM_MAXK>(ctx, GmDots<PV, NV>{vl, dfield(wv.ref), w.st, j}, fp, np, Vh, nrhs))) return e2;
+          if ((e2 = launch_sites<1>(ctx, GmOrtho<PV, NV>{vl, dfield(wv.ref), w.st, j}, fp, np, Vh, nrhs))) return e2;
+        }
+        gm_solve_y<<<(nrhs + 63) / 64, 64, 0, ctx->stream>>>(w.st, nrhs);
+        ctx->kernels++;
+        if ((e2 = launch_sites<0>(ctx, GmUpdate<PV, NV>{vl, dfield(x), w.st, k}, fp, np, Vh, nrhs))) return e2;
+        gm_finish<<<(nrhs + 63) / 64, 64, 0, ctx->stream>>>(w.st, nrhs);
+        ctx->kernels++;
+        return CLG_SUCCESS;
+      };
+      // the first cycle runs eagerly (it has no restart prologue); later cycles replay a graph
+      e = cycle();
+      if (e) return e;
+      first_cycle = false;
+      e = read_summary(w);
+      if (e) return e;
+      bool all = true;
+      for (int r = 0; r < nrhs; ++r) all = all && w.sum_h[r].done;
+      if (all) return CLG_SUCCESS;
+      return iterate(w, slot_base + 2, 1, w.prm->max_iterations / k + 2, cycle);
+    });
+  }
+  return ctx->fail(CLG_ERR_UNSUPPORTED, "solver kind not available for clg_solve");
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+clg_status clg_solver_default_params(int kind, clg_solver_params* p) {
+  if (!p) return CLG_ERR_BAD_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->kind = kind;
+  p->max_dim = 12;          // TestSuit_FermionUpdator.yaml:529-645 (GMRES MaxDim 12)
+  p->restart = 100;
+  p->accuracy = 1e-20;
+  p->absolute_accuracy = 0;
+  p->deviation_step = 10;   // CSolverBiCGstab.cpp:33-93 keys
+  p->max_step = 100;
+  p->small_rho = 1e-30;
+  p->inner_precision = CLG_PREC_SINGLE;
+  p->tol_true_rel = 1e-10;
+  p->inner_tol = 1e-5;
+  p->max_iterations = 200000;
+  p->max_outer = 40;
+  p->even_odd = 1;
+  p->use_graphs = 1;
+  return CLG_SUCCESS;
+}
+
+clg_status clg_solver_create(clg_context ctx, const clg_solver_params* p, clg_solver* out) {
+  if (!ctx || !p || !out) return CLG_ERR_BAD_ARG;
+  if (p->kind < 0 || p->kind > CLG_SOLVER_FOM_MS || p->inner_precision < 0 || p->inner_precision > 2 ||
+      !(p->tol_true_rel > 0) || p->max_iterations < 1 || p->max_outer < 1)
+    return ctx->fail(CLG_ERR_BAD_ARG, "invalid solver parameters");
+  if ((p->kind == CLG_SOLVER_GMRES || p->kind == CLG_SOLVER_FOM_MS) && (p->max_dim < 1 || p->max_dim > GM_MAXK))
+    return ctx->fail(CLG_ERR_UNSUPPORTED, "GMRES / FOM MaxDim must be in [1, 16] on the device");
+  clg_solver_s* s = new clg_solver_s();
+  s->ctx = ctx;
+  s->p = *p;
+  *out = s;
+  return CLG_SUCCESS;
+}
+
+clg_status clg_solver_destroy(clg_solver s) {
+  if (!s) return CLG_ERR_BAD_ARG;
+  delete s;
+  return CLG_SUCCESS;
+}
+
+clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op, clg_field X0, clg_solve_info* info) {
+  if (!S || !X || !B || !U || !info) return CLG_ERR_BAD_ARG;
+  clg_context_s* ctx = S->ctx;
+  const double t0 = now_s();
+  if (X->lat != B->lat || U->lat != B->lat || X->kind != B->kind || X->subset != B->subset || X->nrhs != B->nrhs ||
+      (X0 && (X0->lat != B->lat || X0->subset != B->subset || X0->nrhs != B->nrhs || X0->kind != B->kind)))
+    return ctx->fail(CLG_ERR_BAD_ARG, "solve: field shapes differ");
+  if (S->p.kind == CLG_SOLVER_CGM || S->p.kind == CLG_SOLVER_FOM_MS)
+    return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift solvers are called through clg_solve_multishift");
+  const bool full = B->subset == CLG_SUBSET_FULL;
+  const bool wilson = B->kind == CLG_FERMION_WILSON;
+  const bool even_ops = op == CLG_OP_MEE || op == CLG_OP_MEE_DAG || op == CLG_OP_MEE_MEEDAG || op == CLG_OP_DDDAG_EE;
+  if (even_ops == full) return ctx->fail(CLG_ERR_BAD_ARG, "solve: Schur operators act on EVEN fields, D forms on FULL");
+  if (!(op == CLG_OP_D || op == CLG_OP_DDAG || op == CLG_OP_DDDAG || even_ops))
+    return ctx->fail(CLG_ERR_UNSUPPORTED, "solve: operator not supported");
+  if ((op == CLG_OP_MEE || op == CLG_OP_MEE_DAG || op == CLG_OP_MEE_MEEDAG) && !wilson)
+    return ctx->fail(CLG_ERR_BAD_ARG, "MEE forms are Wilson operators");
+  if (op == CLG_OP_DDDAG_EE && wilson) return ctx->fail(CLG_ERR_BAD_ARG, "DDDAG_EE is the staggered Schur operator");
+
+  Work w;
+  w.ctx = ctx;
+  w.U = U;
+  w.kind = B->kind;
+  w.op = op;
+  w.P = S->p.inner_precision;
+  w.nc = B->nc();
+  w.nrhs = B->nrhs;
+  w.param = B->param;
+  w.Vh = B->lat->g.Vh;
+  w.prm = &S->p;
+  const int nrhs = w.nrhs;
+  clg_status s = CLG_SUCCESS;
+  if ((s = gauge_prepare(U, w.P))) return s;
+  if ((s = dalloc(ctx, (void**)&w.st, sizeof(KState) * nrhs)) || (s = dalloc(ctx, (void**)&w.sum_d, sizeof(Summary) * nrhs)) ||
+      (s = dalloc(ctx, (void**)&w.outer_done_d, sizeof(int) * nrhs)) ||
+      (s = dalloc(ctx, (void**)&w.tol_d, sizeof(double) * nrhs)) || (s = dalloc(ctx, (void**)&w.red_d, sizeof(double) * 2 * nrhs)))
+    return s;
+  if (cudaMallocHost((void**)&w.sum_h, sizeof(Summary) * nrhs) != cudaSuccess ||
+      cudaMallocHost((void**)&w.host_buf, sizeof(double) * 4 * nrhs + 64) != cudaSuccess)
+    return ctx->fail(CLG_ERR_OOM, "pinned host buffer");
+  cudaMemsetAsync(w.st, 0, sizeof(KState) * nrhs, ctx->stream);
+
+  // Schur (even-odd) path for D / D^+ on full fields; Wilson DD^+ = two Schur solves
+  const bool schur = full && S->p.even_odd && (op == CLG_OP_D || op == CLG_OP_DDAG || (op == CLG_OP_DDDAG && wilson));
+  const int kop_d = wilson ? CLG_OP_MEE : CLG_OP_DDDAG_EE;
+  const int kop_ddag = wilson ? CLG_OP_MEE_DAG : CLG_OP_DDDAG_EE;
+  const int64_t Vh = w.Vh;
+  const int nc = w.nc;
+
+  // FP64 outer vectors
+  Owned x64, b64, r64, t64;
+  const int npar = full ? 2 : 1;
+  if ((s = x64.alloc(ctx, 0, nc, npar, 0, nrhs, Vh)) || (s = b64.alloc(ctx, 0, nc, npar, 0, nrhs, Vh)) ||
+      (s = r64.alloc(ctx, 0, nc, npar, 0, nrhs, Vh)))
+    return s;
+  if ((s = t64.alloc(ctx, 0, nc, full ? 2 : 1, full ? 0 : 1, nrhs, Vh))) return s;
+  // inner-precision vectors
+  Owned rP, eP, yP, bS;
+  if ((s = rP.alloc(ctx, w.P, nc, npar, 0, nrhs, Vh)) || (s = eP.alloc(ctx, w.P, nc, npar, 0, nrhs, Vh))) return s;
+  if (schur) {
+    if ((s = bS.alloc(ctx, w.P, nc, 1, 0, nrhs, Vh))) return s;
+    if (op == CLG_OP_DDDAG && (s = yP.alloc(ctx, w.P, nc, 2, 0, nrhs, Vh))) return s;
+  }
+  if ((s = w.kt_odd.alloc(ctx, w.P, nc, 1, 1, nrhs, Vh))) return s;
+  if (op == CLG_OP_MEE_MEEDAG && (s = w.kt_even.alloc(ctx, w.P, nc, 1, 0, nrhs, Vh))) return s;
+  if (!schur && op == CLG_OP_DDDAG && (s = w.kt_full.alloc(ctx, w.P, nc, 2, 0, nrhs, Vh))) return s;
+
+  // b64 = B, x64 = X0 or 0
+  if ((s = blas_copy(ctx, b64.ref, B->ref()))) return s;
+  if (X0) s = blas_copy(ctx, x64.ref, X0->ref());
+  else s = blas_zero(ctx, x64.ref);
+  if (s) return s;
+  if ((s = blas_norm2(ctx, b64.ref, w.red_d))) return s;
+  std::vector<double> bn2(nrhs), rn2(nrhs);
+  if (cudaMemcpyAsync(w.host_buf, w.red_d, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return ctx->fail(CLG_ERR_CUDA, "solve: reading |b|");
+  for (int r = 0; r < nrhs; ++r) bn2[r] = w.host_buf[r];
+
+  const double tol = S->p.tol_true_rel;
+  std::vector<int> done(nrhs, 0), outer_count(nrhs, 0), status(nrhs, CLG_ERR_NOT_CONVERGED), iters(nrhs, 0);
+  std::vector<int> inner_fail(nrhs, 0);
+  const double2 one = make_double2(1, 0);
+  const double lo_tol = w.P == CLG_PREC_DOUBLE ? 1e-14 : (w.P == CLG_PREC_SINGLE ? 1e-6 : 2e-3);
+  int outer = 0;
+  for (;; ++outer) {
+    // r = b - A x  (FP64, true residual)
+    const FieldRef* tmp = (op == CLG_OP_DDDAG) ? nullptr : &t64.ref;
+    Owned tf;
+    if (op == CLG_OP_DDDAG) {
+      if ((s = tf.alloc(ctx, 0, nc, 2, 0, nrhs, Vh))) return s;
+      tmp = &tf.ref;
+    }
+    if (op == CLG_OP_MEE_MEEDAG) {
+      Owned te;
+      if ((s = te.alloc(ctx, 0, nc, 1, 0, nrhs, Vh))) return s;
+      if ((s = apply_op(ctx, CLG_OP_MEE_DAG, U, w.kind, w.param, te.ref, x64.ref, &t64.ref, one, nrhs))) return s;
+      if ((s = apply_op(ctx, CLG_OP_MEE, U, w.kind, w.param, r64.ref, te.ref, &t64.ref, one, nrhs))) return s;
+      if ((s = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? CLG_SUCCESS : CLG_ERR_CUDA)) return s;
+    } else {
+      if ((s = apply_op(ctx, op, U, w.kind, w.param, r64.ref, x64.ref, tmp, one, nrhs))) return s;
+    }
+    s = with_pn(0, nc, [&](auto, auto NN) {
+      return launch_sites<1>(ctx, Resid<NN.value>{dfield(b64.ref), dfield(r64.ref), w.red_d}, 0, npar, Vh, nrhs);
+    });
+    if (s) return s;
+    if (cudaMemcpyAsync(w.host_buf, w.red_d, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+      return ctx->fail(CLG_ERR_CUDA, "solve: reading |r|");
+    bool all = true;
+    for (int r = 0; r < nrhs; ++r) {
+      rn2[r] = w.host_buf[r];
+      if (!done[r]) {
+        const bool ok = bn2[r] == 0.0 ? rn2[r] == 0.0 : std::sqrt(rn2[r]) <= tol * std::sqrt(bn2[r]);
+        if (ok) {
+          done[r] = 1;
+          status[r] = CLG_SUCCESS;
+        } else if (!(rn2[r] == rn2[r])) {
+          done[r] = 1;
+          status[r] = CLG_ERR_BREAKDOWN;
+        }
+      }
+      all = all && done[r];
+    }
+    if (all || outer >= S->p.max_outer) break;
+    int budget_left = 0;
+    for (int r = 0; r < nrhs; ++r)
+      if (!done[r]) budget_left = std::max(budget_left, S->p.max_iterations - iters[r]);
+    if (budget_left <= 0) break;
+    // inner tolerances
+    for (int r = 0; r < nrhs; ++r) {
+      double want = done[r] ? 1.0 : 0.5 * tol * std::sqrt(bn2[r] / std::max(rn2[r], 1e-300));
+      if (w.P != CLG_PREC_DOUBLE) want = std::max(want, S->p.inner_tol);
+      w.host_buf[r] = std::min(0.5, std::max(want, lo_tol));
+      ((int*)(w.host_buf + nrhs))[r] = done[r];
+      if (!done[r]) outer_count[r]++;
+    }
+    cudaMemcpyAsync(w.tol_d, w.host_buf, sizeof(double) * nrhs, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(w.outer_done_d, w.host_buf + nrhs, sizeof(int) * nrhs, cudaMemcpyHostToDevice, ctx->stream);
+    // e ~= A^{-1} r in the inner precision
+    if ((s = blas_copy(ctx, rP.ref, r64.ref))) return s;
+    auto schur_solve = [&](bool dag, const FieldRef& rhs, const FieldRef& sol) -> clg_status {
+      clg_status q;
+      FieldRef rhs_e = rhs.parity_view(0), rhs_o = rhs.parity_view(1);
+      FieldRef sol_e = sol.parity_view(0), sol_o = sol.parity_view(1);
+      // bS = rhs_e + kappa H_eo rhs_o  (Wilson) ; m rhs_e -/+ H_eo rhs_o (staggered D / D^+)
+      HopSpec h1{};
+      h1.kind = w.kind;
+      h1.prec = w.P;
+      h1.dagger = dag && wilson;
+      h1.out_parity = 0;
+      h1.in = rhs_o;
+      h1.out = bS.ref;
+      h1.x = &rhs_e;
+      h1.a = wilson ? make_double2(w.param, 0) : make_double2(dag ? 1.0 : -1.0, 0);
+      h1.xa = wilson ? one : make_double2(w.param, 0);
+      h1.skip_dev = w.outer_done_d;
+      h1.skip_stride = 1;
+      h1.nrhs = nrhs;
+      if ((q = hop(ctx, U, h1))) return q;
+      if ((q = krylov(w, dag ? kop_ddag : kop_d, sol_e, bS.ref, dag ? 10 : 0))) return q;
+      // sol_o = rhs_o + kappa H_oe sol_e (Wilson) ; (rhs_o -/+ H_oe sol_e) / m (staggered)
+      HopSpec h2 = h1;
+      h2.out_parity = 1;
+      h2.in = sol_e;
+      h2.out = sol_o;
+      h2.x = &rhs_o;
+      h2.a = wilson ? make_double2(w.param, 0) : make_double2((dag ? 1.0 : -1.0) / w.param, 0);
+      h2.xa = wilson ? one : make_double2(1.0 / w.param, 0);
+      return hop(ctx, U, h2);
+    };
+    if (schur) {
+      if (op == CLG_OP_DDDAG) {
+        if ((s = schur_solve(false, rP.ref, yP.ref))) return s;
+        s = schur_solve(true, yP.ref, eP.ref);
+      } else {
+        s = schur_solve(op == CLG_OP_DDAG, rP.ref, eP.ref);
+      }
+    } else {
+      s = krylov(w, op, eP.ref, rP.ref, 0);
+    }
+    if (s) return s;
+    if ((s = read_summary(w))) return s;
+    for (int r = 0; r < nrhs; ++r) {
+      if (done[r]) continue;
+      iters[r] += w.sum_h[r].iters;
+      if (w.sum_h[r].status == ST_BREAKDOWN) inner_fail[r]++;
+    }
+    // x += e
+    s = with_pn(w.P, nc, [&](auto PP, auto NN) {
+      AddConv<PP.value, NN.value> f{dfield(x64.ref), dfield(eP.ref), w.outer_done_d};
+      return launch_sites<0>(ctx, f, 0, npar, Vh, nrhs);
+    });
+    if (s) return s;
+  }
+  // write the solution
+  if ((s = blas_copy(ctx, X->ref(), x64.ref))) return s;
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return ctx->fail(CLG_ERR_CUDA, "solve: final sync");
+  const double t1 = now_s();
+  clg_status overall = CLG_SUCCESS;
+  for (int r = 0; r < nrhs; ++r) {
+    info[r].status = status[r];
+    if (status[r] != CLG_SUCCESS && inner_fail[r] && status[r] == CLG_ERR_NOT_CONVERGED) info[r].status = CLG_ERR_BREAKDOWN;
+    info[r].iterations = iters[r];
+    info[r].restarts = 0;
+    info[r].outer = outer_count[r];
+    info[r].true_rel_residual = bn2[r] > 0 ? std::sqrt(rn2[r] / bn2[r]) : std::sqrt(rn2[r]);
+    info[r].seconds = t1 - t0;
+    if (info[r].status != CLG_SUCCESS && overall == CLG_SUCCESS) overall = info[r].status;
+  }
+  return overall;
+}
+
+}  // extern "C"

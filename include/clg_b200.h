@@ -1,0 +1,207 @@
+/*
+ * clg_b200.h -- C ABI of the B200 (sm_100a) fermion hot path of CLGLib.
+ *
+ * Drop-in boundary for CLGLib's Wilson / staggered Dirac operators and the
+ * Krylov solvers that apply them.  Each entry point names the reference
+ * interface it replaces (paths relative to the CudaLatticeGauge tree,
+ * Code/CLGLib/...).  Plain C types only: opaque handles, pointers, sizes.
+ *
+ * Conventions shared with the reference (CLGBin order):
+ *   site   s = ((x*Ly + y)*Lz + z)*Lt + t                  Data/CCommonData.h:274-277
+ *   link   l = s*4 + mu (mu = x,y,z,t), 18 reals row-major  Data/Field/Gauge/CFieldGaugeSU3.cu:1199-1222
+ *   Wilson spinor: 24 reals per site, spin-major then colour Tools/Math/Vectors.h:575-888
+ *   staggered vector: 6 reals per site                      Tools/Math/Vectors.h:287-571
+ *
+ * Every call returns a clg_status; nothing exits or aborts the process (the
+ * reference exits on CUDA errors, Core/CudaHelperFunctions.h:1264-1275).
+ * All device work of a context is ordered on the context's CUDA stream.
+ */
+#ifndef CLG_B200_H
+#define CLG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef int32_t clg_status;
+enum {
+    CLG_SUCCESS = 0,
+    CLG_ERR_BAD_ARG = 1,        /* invalid handle, size or option                       */
+    CLG_ERR_CUDA = 2,           /* a CUDA runtime call failed (see clg_last_error)       */
+    CLG_ERR_OOM = 3,            /* device allocation failed                              */
+    CLG_ERR_NOT_CONVERGED = 4,  /* solver reached its iteration limit (reference: FALSE)  */
+    CLG_ERR_BREAKDOWN = 5,      /* Krylov breakdown (rho ~ 0, NaN/Inf)                   */
+    CLG_ERR_TIMEOUT = 6,        /* a bounded device wait ran out                         */
+    CLG_ERR_UNSUPPORTED = 7,    /* combination not implemented (e.g. odd extents)        */
+    CLG_ERR_NO_DEVICE = 8       /* no CUDA device / not an sm_100 device                  */
+};
+
+/* ------------------------------------------------------------------ enums */
+/* EFieldOperator (Data/Field/CField.h:37-56) plus the even-odd forms of
+ * Docs/SparseLinearAlgebra/evenodd.tex:11-16 */
+typedef enum {
+    CLG_OP_D = 0,            /* EFO_F_D                                           */
+    CLG_OP_DDAG = 1,         /* EFO_F_Ddagger                                     */
+    CLG_OP_DDDAG = 2,        /* EFO_F_DDdagger : D (D^+ x)                        */
+    CLG_OP_DD = 3,           /* EFO_F_DD                                          */
+    CLG_OP_MEE = 4,          /* Wilson: 1 - k^2 H_eo H_oe on even sites            */
+    CLG_OP_MEE_DAG = 5,      /* Wilson: 1 - k^2 H^+_eo H^+_oe                      */
+    CLG_OP_MEE_MEEDAG = 6,   /* Wilson: M_ee M_ee^+                               */
+    CLG_OP_DEO = 7,          /* hopping even <- odd (no kappa / mass)              */
+    CLG_OP_DOE = 8,          /* hopping odd <- even                                */
+    CLG_OP_DDDAG_EE = 9      /* staggered: (2am)^2 - H_eo H_oe on even sites       */
+} clg_op;
+
+/* EOperatorCoefficientType (Data/Field/CField.h:62-68) */
+typedef enum { CLG_COEFF_NONE = 0, CLG_COEFF_MINUS = 1, CLG_COEFF_REAL = 2, CLG_COEFF_COMPLEX = 3 } clg_coeff;
+
+typedef enum { CLG_FERMION_WILSON = 0, CLG_FERMION_STAGGERED = 1 } clg_fermion_kind;
+typedef enum { CLG_SUBSET_FULL = 0, CLG_SUBSET_EVEN = 1 } clg_subset;
+typedef enum { CLG_PREC_DOUBLE = 0, CLG_PREC_SINGLE = 1, CLG_PREC_HALF = 2 } clg_precision;
+typedef enum { CLG_LAYOUT_CLGBIN = 0, CLG_LAYOUT_BRIDGEPP = 1 } clg_layout;
+typedef enum { CLG_GAUGE_IDENTITY = 0, CLG_GAUGE_HAAR = 1, CLG_GAUGE_EXPH = 2 } clg_gauge_init;
+typedef enum { CLG_SOURCE_ZERO = 0, CLG_SOURCE_GAUSS = 1, CLG_SOURCE_Z2 = 2, CLG_SOURCE_POINT = 3 } clg_source_kind;
+typedef enum {
+    CLG_SOLVER_GMRES = 0,       /* CSLASolverGMRES    SparseLinearAlgebra/CSolverGMRES.cpp:111-358   */
+    CLG_SOLVER_BICGSTAB = 1,    /* CSLASolverBiCGStab SparseLinearAlgebra/CSolverBiCGstab.cpp:403-607 */
+    CLG_SOLVER_CG = 2,          /* CG on Hermitian positive operators (DD^+, staggered (DD^+)_ee)     */
+    CLG_SOLVER_CGM = 3,         /* multi-shift CG (no reference twin; CMultiShiftSolver.h:38-47 API)  */
+    CLG_SOLVER_FOM_MS = 4       /* CMultiShiftFOM     SparseLinearAlgebra/CMultiShiftFOM.cpp:97-270   */
+} clg_solver_kind;
+
+/* ------------------------------------------------------------------ handles */
+typedef struct clg_context_s* clg_context;
+typedef struct clg_lattice_s* clg_lattice;
+typedef struct clg_gauge_s* clg_gauge;
+typedef struct clg_field_s* clg_field;
+typedef struct clg_solver_s* clg_solver;
+
+/* ------------------------------------------------------------------ context
+ * Replaces appInitialCLG / CCLGLibManager::InitialWithParameter device setup
+ * (Core/CLGLibManager.cpp:882-917).  stream == NULL creates a private stream. */
+clg_status clg_context_create(int device, void* cuda_stream, clg_context* out);
+clg_status clg_context_destroy(clg_context ctx);
+clg_status clg_context_set_stream(clg_context ctx, void* cuda_stream);
+clg_status clg_context_synchronize(clg_context ctx);
+const char* clg_status_string(clg_status s);
+const char* clg_last_error(clg_context ctx);
+/* number of kernels this context has launched (all kinds), for accounting */
+clg_status clg_context_kernel_count(clg_context ctx, int64_t* count);
+
+/* ------------------------------------------------------------------ lattice
+ * Replaces InitialLatticeAndConstant (Core/CLGLibManager.cpp:52-348) and the
+ * torus boundary tables (Data/Boundary/CBoundaryConditionTorusSquare.cu:18-64):
+ * dims = (Lx,Ly,Lz,Lt), all even; fermion_bc = boundary sign per direction
+ * (the reference default is (1,1,1,-1), Core/CLGLibManager.cpp:549-566). */
+clg_status clg_lattice_create(clg_context ctx, const int dims[4], const int fermion_bc[4], clg_lattice* out);
+clg_status clg_lattice_destroy(clg_lattice lat);
+
+/* ------------------------------------------------------------------ gauge
+ * CFieldGaugeSU3 (Data/Field/Gauge/CFieldGaugeSU3.h:18-121).
+ * import: InitialFieldWithFile / InitialWithByte (CFieldGaugeSU3.cu:1080-1222),
+ *   layout CLGBIN (EFFT_CLGBinDouble) or BRIDGEPP (_kernelSetConfigurationSU3,
+ *   CFieldGaugeSU3.cu:568-592); `data` holds 4*V*18 doubles, on the host unless
+ *   on_device != 0.
+ * export: CopyDataOutDouble (CFieldGaugeSU3.cu:1693-1760), CLGBin order.
+ * random: seeded Haar SU(3), exp(i eps H) or identity links generated on the device. */
+clg_status clg_gauge_create(clg_lattice lat, clg_gauge* out);
+clg_status clg_gauge_destroy(clg_gauge g);
+clg_status clg_gauge_import(clg_gauge g, const double* data, int layout, int on_device);
+clg_status clg_gauge_export(clg_gauge g, double* data, int on_device);
+clg_status clg_gauge_random(clg_gauge g, int init, uint64_t seed, uint32_t field_id, double eps);
+/* average (1/3) Re tr of the plaquette (TestConfigurationFileIO.cpp:12-38 known answer) */
+clg_status clg_gauge_plaquette(clg_gauge g, double* out);
+/* max |U U^+ - 1| and |det U - 1| over links; the 12-real FP32/FP16 copies are
+ * built only when this is below 1e-12 */
+clg_status clg_gauge_unitarity(clg_gauge g, double* out);
+
+/* ------------------------------------------------------------------ fermion fields
+ * CFieldFermionWilsonSquareSU3 (param = Hopping kappa, CFieldFermionWilsonSquareSU3.cu:637-654)
+ * CFieldFermionKSSU3 (param = Mass = 2am, Data/Field/CField.cpp:150-195).
+ * A field holds nrhs right-hand sides.  import/export move CLGBin-ordered
+ * full-lattice data (V*24 or V*6 doubles per rhs); EVEN fields read / write
+ * only the even sites of that array (odd sites are exported as zero). */
+clg_status clg_field_create(clg_lattice lat, int kind, int subset, int precision, int nrhs, double param,
+                            clg_field* out);
+clg_status clg_field_destroy(clg_field f);
+clg_status clg_field_set_param(clg_field f, double param);
+clg_status clg_field_import(clg_field f, int rhs, const double* data, int on_device);
+clg_status clg_field_export(clg_field f, int rhs, double* data, int on_device);
+/* InitialField / InitialAsSource (CFieldFermionWilsonSquareSU3.cu:1102-1136, :521-566):
+ * GAUSS (E|z|^2 = 1), Z2 ((+-1 +- i)/sqrt 2), POINT (site, spin*3+colour), ZERO. */
+clg_status clg_field_random(clg_field f, int rhs, int kind, uint64_t seed, uint32_t field_id, int64_t site, int comp);
+clg_status clg_field_copy(clg_field dst, clg_field src);  /* CopyTo; converts precision */
+
+/* ------------------------------------------------------------------ operators
+ * CField::ApplyOperator (Data/Field/CField.h:203): in place, the field is both
+ * input and output; coefficient EOCT_None / Minus / Real / Complex. */
+clg_status clg_apply(int op, clg_field inout, clg_gauge g, int coeff_type, double cre, double cim);
+/* out-of-place variant: out = coeff * op(in) */
+clg_status clg_apply_to(int op, clg_field out, clg_field in, clg_gauge g, int coeff_type, double cre, double cim);
+
+/* ------------------------------------------------------------------ BLAS
+ * CField BLAS (Data/Field/CField.h:127-201): Dot = sum conj(a) b, accumulated in
+ * FP64 (re_im holds 2*nrhs doubles), Axpy, ScalarMultply, Zero, CopyTo. */
+clg_status clg_dot(clg_field a, clg_field b, double* re_im);
+clg_status clg_norm2(clg_field a, double* out);
+clg_status clg_axpy(clg_field y, double are, double aim, clg_field x);
+clg_status clg_scale(clg_field y, double are, double aim);
+clg_status clg_zero(clg_field y);
+
+/* ------------------------------------------------------------------ solvers
+ * CSLASolver::Configurate keys (CSolverGMRES.cpp:35-99, CSolverBiCGstab.cpp:33-93)
+ * plus the B200 options.  tol_true_rel is the true relative residual
+ * |b - M x| / |b| every solve must reach, recomputed in FP64. */
+typedef struct {
+    int32_t kind;              /* clg_solver_kind                                         */
+    int32_t max_dim;           /* MaxDim (GMRES / FOM Krylov dimension)                   */
+    int32_t restart;           /* Restart (cycles)                                        */
+    double accuracy;           /* Accuracy (reference stopping quantity, squared)          */
+    int32_t absolute_accuracy; /* AbsoluteAccuracy                                        */
+    int32_t deviation_step;    /* DiviationStep (BiCGStab)                                */
+    int32_t max_step;          /* MaxStep (BiCGStab)                                      */
+    double small_rho;          /* SmallRho (BiCGStab)                                     */
+    int32_t inner_precision;   /* clg_precision of the Krylov iterations                  */
+    double tol_true_rel;       /* required true relative residual (FP64), e.g. 1e-10     */
+    double inner_tol;          /* relative reduction per defect-correction cycle          */
+    int32_t max_iterations;    /* total operator applications allowed                     */
+    int32_t max_outer;         /* defect-correction cycles allowed                        */
+    int32_t even_odd;          /* solve D x = b through the even-odd Schur system         */
+    int32_t use_graphs;        /* capture the inner iterations in CUDA graphs             */
+} clg_solver_params;
+
+typedef struct {
+    int32_t status;            /* clg_status of this right-hand side / shift              */
+    int32_t iterations;        /* operator applications (all precisions)                  */
+    int32_t restarts;          /* restart cycles                                          */
+    int32_t outer;             /* defect-correction cycles                                */
+    double true_rel_residual;  /* |b - M x| / |b| in FP64 at exit                          */
+    double seconds;            /* wall time of the call                                   */
+} clg_solve_info;
+
+clg_status clg_solver_default_params(int kind, clg_solver_params* p);
+clg_status clg_solver_create(clg_context ctx, const clg_solver_params* p, clg_solver* out);
+clg_status clg_solver_destroy(clg_solver s);
+/* CSLASolver::Solve (SparseLinearAlgebra/CSLASolver.h:42-50): solve op x = b for
+ * every right-hand side of b; x may alias b; x0 (nullable) is the start vector
+ * (pStart).  info holds nrhs entries.  Returns CLG_SUCCESS only when every
+ * right-hand side reached tol_true_rel. */
+clg_status clg_solve(clg_solver s, clg_field x, clg_field b, clg_gauge g, int op, clg_field x0, clg_solve_info* info);
+/* CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47):
+ * (op + c_n) x_n = b for n < nshift; shifts_re_im holds nshift complex shifts
+ * (real for CGM); x[n] must not alias b (CMultiShiftSolver.h:35). */
+clg_status clg_solve_multishift(clg_solver s, clg_field* x, int nshift, const double* shifts_re_im, clg_field b,
+                                clg_gauge g, int op, clg_solve_info* info);
+/* CFieldFermion::RationalApproximation (Data/Field/CField.cpp:114-145):
+ * f <- c f + sum_i a_i (op + b_i)^{-1} f through one multi-shift solve. */
+clg_status clg_rational_apply(clg_solver s, clg_field f, clg_gauge g, int op, int degree, double c,
+                              const double* a, const double* b, clg_solve_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

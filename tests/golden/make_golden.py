@@ -1,0 +1,53 @@
+"""Generate the committed golden fixtures from the reference source tree.
+
+Run in a container where the CudaLatticeGauge sources are mounted (default
+path below, or pass it as the first argument).  Outputs, next to this script:
+
+  bridgepp_4x4x4x8.npz   the reference's Bridge++ 4^3x8 configuration
+                         (Bin/Debug/bridgepp_conf_text.dat) as float64, Bridge++
+                         order; known plaquette 0.625129946974942
+                         (Code/CLGTest/Tests/TestConfigurationFileIO.cpp:12-38)
+  gamma_chiral.json      the chiral gamma-matrix table parsed from
+                         Code/CLGLib/Tools/Math/GammaMatrix.h (the `else` branch of
+                         gammaMatrixSet::CreateGammaMatrix): for GAMMA1..GAMMA5, per
+                         row the non-zero column and the power b of i^b
+"""
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def main(ref="/root/reference"):
+    txt = os.path.join(ref, "Bin", "Debug", "bridgepp_conf_text.dat")
+    vals = np.loadtxt(txt, dtype=np.float64)
+    assert vals.size == 4 * 4 * 4 * 8 * 4 * 18
+    np.savez_compressed(os.path.join(HERE, "bridgepp_4x4x4x8.npz"), links=vals,
+                        dims=np.array([4, 4, 4, 8]), plaquette=np.array(0.625129946974942))
+
+    src = open(os.path.join(ref, "Code", "CLGLib", "Tools", "Math", "GammaMatrix.h")).read()
+    start = src.index("CreateGammaMatrix(EGammaMatrixSet eSet")
+    body = src[start:]
+    chiral = body[body.index("else"):]  # the chiral branch follows the EGMS_Dirac branch
+    table = {}
+    for name in ("GAMMA1", "GAMMA2", "GAMMA3", "GAMMA4", "GAMMA5"):
+        rows = {}
+        for line in chiral.splitlines():
+            s = line.strip()
+            if s.startswith("//"):
+                continue
+            m = re.match(r"gmarray\[%s\]\.Set\((\d), (\d), (\d)\);" % name, s)
+            if m:
+                r, c, b = map(int, m.groups())
+                rows.setdefault(r, [c, b])
+        table[name] = [rows[r] for r in range(4)]
+    with open(os.path.join(HERE, "gamma_chiral.json"), "w") as f:
+        json.dump({"source": "Code/CLGLib/Tools/Math/GammaMatrix.h chiral set", "rows": table}, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

@@ -1,0 +1,130 @@
+"""Solver parity on the GPU: every solve must reach the FP64 true relative
+residual 1e-10 (recomputed here by the FP64 oracle) and agree with the oracle's
+own FP64 solve; the reference's solver identities (Tests/TestSolver.cpp:12-120)
+are checked at that tolerance."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+KAPPA = 0.1355
+TOL = 1e-10
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def gauge(clg, lat, kind, seed):
+    U = clg.CFieldGaugeSU3(lat)
+    if kind == "haar":
+        U.InitialField(clg.GAUGE_HAAR, seed, 1)
+    else:
+        U.InitialField(clg.GAUGE_EXPH, seed, 1, 0.25)
+    return U
+
+
+@pytest.mark.parametrize("solver,prec", [("GMRES", 0), ("BiCGStab", 0), ("GMRES", 1), ("BiCGStab", 1), ("BiCGStab", 2)])
+def test_wilson_solve_haar_8x4(ctx, clg, oracle, solver, prec):
+    """BASELINE config 1 shape: 8^4 Haar links, kappa 0.1355, Gaussian source, D x = b."""
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
+    U = gauge(clg, lat, "haar", 0xC1A60000)
+    Uh = U.CopyDataOut()
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    b.InitialField(clg.SOURCE_GAUSS, 0xC1A60000, 2)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    S = (clg.CSLASolverGMRES if solver == "GMRES" else clg.CSLASolverBiCGStab)(ctx, inner_precision=prec)
+    info = S.Solve(x, b, U, clg.EFO_F_D)[0]
+    op = oracle.Operator("WILSON_D", lat.dims, Uh, KAPPA)
+    bh, xh = b.to_numpy(), x.to_numpy()
+    assert info["status"] == 0
+    assert op.true_residual(bh, xh) <= TOL
+    assert info["true_rel_residual"] <= TOL
+    xo, io = oracle.gmres(op, bh, maxdim=12, restart=200, accuracy=1e-24)
+    assert rel(xh, xo) < 1e-8
+
+
+def test_wilson_inverse_identities(ctx, clg, oracle):
+    """|D^-1 D phi - phi|, |D D^-1 phi - phi| and the D^+ / DD^+ forms (TestSolver.cpp:12-120)."""
+    lat = clg.Lattice(ctx, (4, 4, 4, 8))
+    U = gauge(clg, lat, "haar", 17)
+    phi = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    phi.InitialField(clg.SOURCE_GAUSS, 18, 2)
+    ph = phi.to_numpy()
+    S = clg.CSLASolverGMRES(ctx, inner_precision=1)
+    for op, apply in [(clg.EFO_F_D, "D"), (clg.EFO_F_Ddagger, "Ddagger"), (clg.EFO_F_DDdagger, "DDdagger")]:
+        y = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+        phi.CopyTo(y)
+        getattr(y, apply)(U)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+        S.Solve(x, y, U, op)  # D^-1 D phi
+        assert rel(x.to_numpy(), ph) < 1e-8
+        z = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+        S.Solve(z, phi, U, op)  # D D^-1 phi
+        getattr(z, apply)(U)
+        assert rel(z.to_numpy(), ph) <= TOL
+
+
+@pytest.mark.parametrize("solver", ["GMRES", "BiCGStab"])
+def test_wilson_near_critical_small(ctx, clg, oracle, solver):
+    """exp(i eps H) links at eps = 0.25, kappa = 0.1355 (near-critical) on 4^3 x 8."""
+    lat = clg.Lattice(ctx, (4, 4, 4, 8))
+    U = gauge(clg, lat, "expH", 0xC1A60001)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    b.InitialField(clg.SOURCE_GAUSS, 3, 2)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    S = (clg.CSLASolverGMRES if solver == "GMRES" else clg.CSLASolverBiCGStab)(ctx, inner_precision=1)
+    info = S.Solve(x, b, U, clg.EFO_F_D)[0]
+    op = oracle.Operator("WILSON_D", lat.dims, U.CopyDataOut(), KAPPA)
+    assert op.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
+    assert info["status"] == 0
+
+
+def test_wilson_schur_system_direct(ctx, clg, oracle):
+    """Solve M_ee x_e = b_e directly on EVEN fields."""
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
+    U = gauge(clg, lat, "expH", 0xC1A60001)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN)
+    b.InitialField(clg.SOURCE_GAUSS, 4, 2)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN)
+    S = clg.CSLASolverBiCGStab(ctx, inner_precision=1)
+    info = S.Solve(x, b, U, clg.OP_MEE)[0]
+    op = oracle.Operator("WILSON_MEE", lat.dims, U.CopyDataOut(), KAPPA)
+    assert op.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
+    assert info["iterations"] > 0
+
+
+def test_multi_rhs_batch(ctx, clg, oracle):
+    """12 spin-colour point sources + Z2 noise sources solved in one batched call."""
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
+    U = gauge(clg, lat, "expH", 0xC1A60003)
+    n = 14
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=n)
+    for r in range(12):
+        b.InitialAsSource(0, r, rhs=r)
+    for r in range(12, n):
+        b.InitialField(clg.SOURCE_Z2, 0xC1A60003, 10 + r, rhs=r)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=n)
+    S = clg.CSLASolverBiCGStab(ctx, inner_precision=1)
+    infos = S.Solve(x, b, U, clg.EFO_F_D)
+    op = oracle.Operator("WILSON_D", lat.dims, U.CopyDataOut(), KAPPA)
+    for r in range(n):
+        assert infos[r]["status"] == 0
+        assert op.true_residual(b.to_numpy(r), x.to_numpy(r)) <= TOL
+
+
+def test_staggered_cg(ctx, clg, oracle):
+    """Staggered D x = b through CG on (DD^+)_ee, and DD^+ x = b."""
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
+    m = 0.02
+    U = gauge(clg, lat, "expH", 0xC1A60004)
+    b = clg.CFieldFermionKSSU3(lat, m)
+    b.InitialField(clg.SOURCE_GAUSS, 5, 2)
+    x = clg.CFieldFermionKSSU3(lat, m)
+    S = clg.CSLASolverCG(ctx, inner_precision=1)
+    S.Solve(x, b, U, clg.EFO_F_D)
+    Uh = U.CopyDataOut()
+    op = oracle.Operator("KS_D", lat.dims, Uh, m)
+    assert op.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
+    S.Solve(x, b, U, clg.EFO_F_DDdagger)
+    op2 = oracle.Operator("KS_DDDAG", lat.dims, Uh, m)
+    assert op2.true_residual(b.to_numpy(), x.to_numpy()) <= TOL

@@ -1,0 +1,58 @@
+"""CPU-side checks of the C ABI library: it builds, loads, and exports every
+entry point declared in include/clg_b200.h (no device computation)."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "clg_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(clg_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib_path():
+    from cudalatticegauge_b200 import build
+
+    return build.build()
+
+
+def test_exports_every_header_symbol(lib_path):
+    out = subprocess.run(["nm", "-D", "--defined-only", lib_path], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r" T (clg_[a-z0-9_]+)$", out, flags=re.M))
+    missing = [f for f in header_functions() if f not in exported]
+    assert not missing, missing
+    assert len(header_functions()) >= 30
+
+
+def test_library_loads_and_binds_every_symbol(lib_path):
+    import cudalatticegauge_b200 as clg
+
+    lib = clg.load_library(lib_path)
+    names = {n for n, _, _ in clg.SIGNATURES}
+    assert names == set(header_functions())
+    assert lib.clg_status_string(clg.ERR_NOT_CONVERGED) == b"solver did not converge"
+
+
+def test_built_for_sm100a(lib_path):
+    """The device code is sm_100a SASS (checked from cuobjdump's ELF list, no disassembly)."""
+    r = subprocess.run(["cuobjdump", "--list-elf", lib_path], capture_output=True, text=True)
+    assert r.returncode == 0
+    assert "sm_100a" in r.stdout
+
+
+def test_no_device_is_an_error_not_a_crash(lib_path):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import cudalatticegauge_b200 as clg
+
+    with pytest.raises(clg.CLGError) as e:
+        clg.Context(0)
+    assert e.value.status == clg.ERR_NO_DEVICE
