@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 fermion hot path.
+
+Metric: solves per second of the even-odd Wilson system to a true relative
+residual of 1e-10 (FP32 inner Krylov iterations inside FP64 defect correction),
+with the Dslash HBM bandwidth of the dominant kernel as the roofline.
+
+Workload ``wilson_eo_32x32x32x16``: 32^3 x 16 lattice, links exp(i eps H) with a
+seeded traceless-Hermitian Gaussian H and eps = 0.25, kappa = 0.1355, fermion
+boundary (+,+,+,-), one complex Gaussian source per rank (synthetic data).
+A step is one solve of D x = b.  With N GPUs every rank solves its own source
+(independent replicas, weak scaling; the path has no exchange step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Dslash HBM GB/s; solves/s to 1e-10 rel. resid, mixed+batched vs FP64 (1 B200)"
+UNIT = "solves/s"
+WORKLOADS = {
+    "wilson_eo_32x32x32x16": dict(dims=(32, 32, 32, 16), kappa=0.1355, eps=0.25, seed=0xC1A60001, nrhs=1),
+    "wilson_eo_16x16x16x8": dict(dims=(16, 16, 16, 8), kappa=0.1355, eps=0.25, seed=0xC1A60001, nrhs=1),
+}
+DEFAULT_WORKLOAD = "wilson_eo_32x32x32x16"
+TOL = 1e-10
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        if args.impl != "reference":
+            torch.cuda.set_device(local)
+        backend = "nccl" if args.impl != "reference" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ our arm
+def hop_bytes_per_site(prec: int) -> int:
+    """Compulsory HBM bytes of one checkerboard hop per output site: one input
+    spinor, one output spinor and eight links (12-real for FP32/FP16)."""
+    if prec == 0:
+        return (24 + 24 + 8 * 18) * 8
+    if prec == 1:
+        return (24 + 24 + 8 * 12) * 4
+    return (48 + 4) * 2 + 8 * 12 * 2
+
+
+def time_hops(clg, ctx, lat, U, prec, stream, reps=60):
+    """Average duration of the checkerboard Wilson hop (odd -> even), cycling
+    over four input/output pairs so that the working set exceeds L2."""
+    import torch
+
+    kappa = 0.1355
+    fields = []
+    for i in range(4):
+        a = clg.CFieldFermionWilsonSquareSU3(lat, kappa, precision=prec)
+        a.InitialField(clg.SOURCE_GAUSS, 1234 + i, 2)
+        b = clg.CFieldFermionWilsonSquareSU3(lat, kappa, precision=prec)
+        fields.append((a, b))
+    for a, b in fields:  # warm-up (also runs the block-size autotuner)
+        a.apply_to(clg.OP_DEO, b, U)
+    k0 = ctx.kernel_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for r in range(reps):
+        a, b = fields[r % 4]
+        a.apply_to(clg.OP_DEO, b, U)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.kernel_count() - k0
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    for a, b in fields:
+        a.close()
+        b.close()
+    return t, launches
+
+
+def ours(args, world, rank, local):
+    import torch
+
+    import cudalatticegauge_b200 as clg
+
+    W = WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    ctx = clg.Context(local, stream.cuda_stream)
+    lat = clg.Lattice(ctx, W["dims"])
+    V = lat.volume
+    Vh = V // 2
+    kappa = W["kappa"]
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, W["seed"], 1, W["eps"])
+    nrhs = W["nrhs"]
+    b = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
+    for r in range(nrhs):
+        b.InitialField(clg.SOURCE_GAUSS, W["seed"] + 7919 * rank, 2 + r, rhs=r)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
+    mixed = clg.CSLASolverBiCGStab(ctx, inner_precision=clg.SINGLE, tol_true_rel=TOL)
+
+    def check(infos):
+        for i in infos:
+            if i["status"] != 0 or i["true_rel_residual"] > TOL:
+                raise RuntimeError(f"solve failed: {i}")
+        return infos
+
+    for _ in range(args.warmup):
+        check(mixed.Solve(x, b, U, clg.EFO_F_D))
+
+    # ---------------- timed region: K solves, inputs resident in HBM
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    k0 = ctx.kernel_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    infos = []
+    for _ in range(args.steps):
+        infos = check(mixed.Solve(x, b, U, clg.EFO_F_D))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = ctx.kernel_count() - k0
+    t_local = e0.elapsed_time(e1) / 1e3
+    barrier(world)
+    t = max_over_ranks(t_local, world)
+    value = args.steps * nrhs * world / t
+
+    # ---------------- end to end through the public API with host buffers
+    src = torch.empty((V, 4, 3), dtype=torch.complex128, pin_memory=True).numpy()
+    dst = torch.empty((V, 4, 3), dtype=torch.complex128, pin_memory=True).numpy()
+    b.to_numpy(0, out=src)
+    b1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    x1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    barrier(world)
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        b1.from_numpy(src)
+        check(mixed.Solve(x1, b1, U, clg.EFO_F_D))
+        x1.to_numpy(0, out=dst)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3, world)
+    e2e = {"value": args.steps * world / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": int(src.nbytes), "d2h_bytes_per_step": int(dst.nbytes)}
+
+    # ---------------- roofline of the dominant kernel (FP32 checkerboard hop)
+    peak, peak_kind = peaks()
+    t_hop, hop_launches = time_hops(clg, ctx, lat, U, clg.SINGLE, stream)
+    hop_alg = hop_bytes_per_site(1) * Vh
+    achieved = hop_alg / t_hop / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "hop_fp32_traffic.json")
+    if os.path.exists(tp):
+        d = json.load(open(tp))
+        if tuple(d.get("dims", ())) == tuple(W["dims"]):
+            traffic = d.get("bytes_per_launch")
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic,
+            "kernel": "wilson_hop_kernel<P32,12-real>", "bytes_per_launch": hop_alg,
+            "launch_us": round(t_hop * 1e6, 2), "peak_source": peak_kind}
+
+    extra = {}
+    if rank == 0 and not args.quick:
+        # Dslash bandwidth in each precision, FP64 plain solves, CPU baseline
+        dsl = {}
+        for name, prec in (("fp64", clg.DOUBLE), ("fp32", clg.SINGLE), ("fp16", clg.HALF)):
+            th, _ = time_hops(clg, ctx, lat, U, prec, stream, reps=40)
+            dsl[name] = {"GB/s": round(hop_bytes_per_site(prec) * Vh / th / 1e9, 1),
+                         "GFLOP/s": round(1320 * Vh / th / 1e9, 1), "launch_us": round(th * 1e6, 2)}
+        extra["dslash_hop"] = dsl
+        plain = {}
+        for label, cls, prec in (("fp64_gmres12", clg.CSLASolverGMRES, clg.DOUBLE),
+                                 ("fp64_bicgstab", clg.CSLASolverBiCGStab, clg.DOUBLE),
+                                 ("mixed_gmres12", clg.CSLASolverGMRES, clg.SINGLE),
+                                 ("mixed_bicgstab", clg.CSLASolverBiCGStab, clg.SINGLE),
+                                 ("half_bicgstab", clg.CSLASolverBiCGStab, clg.HALF)):
+            s = cls(ctx, inner_precision=prec, tol_true_rel=TOL, MaxDim=12)
+            xs = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            inf = s.Solve(xs, b1, U, clg.EFO_F_D, raise_on_fail=False)[0]
+            dt = time.perf_counter() - t0
+            plain[label] = {"solves_per_s": round(1.0 / dt, 3), "seconds": round(dt, 4),
+                            "applications": inf["iterations"], "outer": inf["outer"],
+                            "true_rel_residual": inf["true_rel_residual"], "status": inf["status"]}
+            s.close()
+            xs.close()
+        extra["solves"] = plain
+        if world == 1 and not args.no_cpu:
+            extra["cpu_baseline"] = cpu_baseline(U, lat, kappa, plain["fp64_gmres12"]["applications"])
+    result = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer (complex)", "data": "synthetic",
+        "config": {"workload": args.workload, "dims": list(W["dims"]), "kappa": kappa, "links": f"exp(i eps H), eps={W['eps']}",
+                   "source": "complex Gaussian", "solver": "BiCGStab, FP32 inner, FP64 defect correction, even-odd",
+                   "tol_true_rel": TOL, "rhs_per_gpu": nrhs, "parallelism": f"replicas x{world}",
+                   "l2": "working set (links 101 MB FP32 + 302 MB FP64, spinors) larger than L2"},
+        "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": launches,
+        "iterations_per_solve": infos[0]["iterations"] if infos else None,
+    }
+    result.update(extra)
+    if "cpu_baseline" not in result:
+        result["cpu_baseline"] = None
+    if rank == 0:
+        print(json.dumps(result))
+    ctx.close()
+
+
+def cpu_baseline(U, lat, kappa, fp64_applications):
+    """Oracle FP64 M_ee on the host cores; solves/s = 1 / (t_apply * A), A the FP64
+    GMRES(12) applications this run's solve needed."""
+    from oracle import oracle as O
+
+    Uh = U.CopyDataOut()
+    L = lat.dims
+    V = lat.volume
+    op = O.Operator("WILSON_MEE", L, Uh, kappa)
+    psi = O.gauss(V, 12, 5, 2).reshape(V, 4, 3)
+    psi[O.parity_mask(L) == 1] = 0
+    op(psi)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        op(psi)
+    t_apply = (time.perf_counter() - t0) / reps
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": round(1.0 / (t_apply * max(fp64_applications, 1)), 6), "unit": UNIT, "cores": cores,
+            "kind": "port",
+            "sample": f"{reps} FP64 M_ee applications of the C/OpenMP oracle on {L} ({t_apply*1e3:.1f} ms each); "
+                      f"solves/s = 1/(t_apply x {fp64_applications} applications of the FP64 GMRES(12) solve)"}
+
+
+# ------------------------------------------------------------------ reference arm
+def reference(args, world, rank):
+    """The reference algorithm on the host cores: the oracle's restatement of
+    CSLASolverGMRES (MGS Arnoldi, Givens; CSolverGMRES.cpp:111-358) on the
+    even-odd system in FP64.  Each step is one GMRES(12) restart cycle (a bounded
+    sample); solves/s = 1 / (t_cycle * cycles per solve), the cycle count of a
+    full solve of this workload recorded by oracle/measure_reference_cycles.py."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    W = WORKLOADS[args.workload]
+    L, kappa = W["dims"], W["kappa"]
+    V = int(np.prod(L))
+    U = O.gauge_expH(L, W["seed"], W["eps"])
+    b = O.gauss(V, 12, W["seed"], 2).reshape(V, 4, 3)
+    pm = O.parity_mask(L)
+    be, bo = b.copy(), b.copy()
+    be[pm == 1] = 0
+    bo[pm == 0] = 0
+    bt = be + kappa * O.wilson_hop(L, U, bo, 0)
+    op = O.Operator("WILSON_MEE", L, U, kappa)
+    x = None
+    for _ in range(args.warmup):
+        x, _ = O.gmres(op, bt, x0=x, maxdim=12, restart=1, accuracy=0.0)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        x, _ = O.gmres(op, bt, x0=x, maxdim=12, restart=1, accuracy=0.0)
+    t_cycle = (time.perf_counter() - t0) / args.steps
+    counts = {}
+    cp = os.path.join(ROOT, "oracle", "reference_cycles.json")
+    if os.path.exists(cp):
+        counts = json.load(open(cp))
+    cycles = counts.get(args.workload, {}).get("cycles")
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if cycles:
+        value = 1.0 / (t_cycle * cycles)
+        how = f"{cycles} GMRES(12) cycles per solve (oracle/reference_cycles.json)"
+    else:
+        value = None
+        how = "cycle count of a full solve not recorded"
+    sample = (f"{args.steps} FP64 even-odd GMRES(12) restart cycles of the C/OpenMP oracle on {L} "
+              f"({t_cycle:.3f} s each); {how}")
+    out = {"metric": METRIC, "value": round(value, 6) if value else None, "unit": UNIT, "impl": "reference",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex)", "data": "synthetic",
+           "ms_per_step": round(t_cycle * 1e3, 3),
+           "config": {"workload": args.workload, "dims": list(L), "kappa": kappa, "links": f"exp(i eps H), eps={W['eps']}",
+                      "solver": "GMRES(12) even-odd FP64 (reference algorithm, CPU)"},
+           "cpu_baseline": {"value": round(value, 6) if value else None, "unit": UNIT, "cores": cores,
+                            "kind": "port", "sample": sample},
+           "e2e": {"value": round(value, 6) if value else None, "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--quick", action="store_true", help="skip the per-precision and FP64 side measurements")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            reference(args, world, rank)
+        else:
+            ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -243,8 +243,11 @@ class _FermionField:
             raise CLGError(ERR_BAD_ARG, "field data has the wrong size")
         self.ctx.check(self.ctx.lib.clg_field_import(self.h, rhs, _ptr(a), 0), "clg_field_import")
 
-    def to_numpy(self, rhs: int = 0) -> np.ndarray:
-        out = np.empty(self._shape(), np.complex128)
+    def to_numpy(self, rhs: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self._shape(), np.complex128)
+        elif out.dtype != np.complex128 or out.size != self.lat.volume * self.NC or not out.flags["C_CONTIGUOUS"]:
+            raise CLGError(ERR_BAD_ARG, "export buffer has the wrong size or type")
         self.ctx.check(self.ctx.lib.clg_field_export(self.h, rhs, _ptr(out), 0), "clg_field_export")
         return out
 
