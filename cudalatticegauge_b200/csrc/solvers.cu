@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -210,6 +212,7 @@ struct Work {
   // graphs
   std::vector<cudaGraphExec_t> graphs;
   int total_iters = 0;
+  int inner_cap = 1 << 30;  // operator applications allowed in the current inner solve
   clg_status kvec(int slot, int idx, int np, int fp, FieldRef& out) {
     auto& v = kv[slot];
     while ((int)v.size() <= idx) v.emplace_back(nullptr);
@@ -267,6 +270,11 @@ template <class Body>
 clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& body) {
   const bool graphs = w.prm->use_graphs && w.ctx->stream != nullptr;
   while ((int)w.graphs.size() <= graph_slot) w.graphs.push_back(nullptr);
+  // stagnation guard: an inner solve ends when no running rhs has improved its
+  // residual (recursive, or the GMRES estimate) for `patience` chunks
+  std::vector<double> best(w.nrhs, 1e300);
+  std::vector<int> since(w.nrhs, 0);
+  const int patience = std::max(8, 400 / std::max(chunk, 1));
   for (int c = 0; c < max_chunks; ++c) {
     clg_status s = CLG_SUCCESS;
     if (graphs && c > 0 && !w.graphs[graph_slot]) {
@@ -294,13 +302,23 @@ clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& bo
     }
     s = read_summary(w);
     if (s) return s;
-    bool all = true;
+    bool all = true, stalled = true;
     int most = 0;
     for (int r = 0; r < w.nrhs; ++r) {
-      all = all && w.sum_h[r].done;
-      most = std::max(most, w.sum_h[r].iters);
+      const Summary& q = w.sum_h[r];
+      all = all && q.done;
+      most = std::max(most, q.iters);
+      if (q.done) continue;
+      const double cur = q.rr > 0 ? q.rr : q.resid_est * q.resid_est;
+      if (cur < 0.9 * best[r]) {
+        best[r] = cur;
+        since[r] = 0;
+      } else {
+        since[r]++;
+      }
+      stalled = stalled && since[r] >= patience;
     }
-    if (all || most >= w.prm->max_iterations) break;
+    if (all || stalled || most >= w.inner_cap) break;
   }
   return CLG_SUCCESS;
 }
@@ -558,6 +576,8 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
   std::vector<int> inner_fail(nrhs, 0);
   const double2 one = make_double2(1, 0);
   const double lo_tol = w.P == CLG_PREC_DOUBLE ? 1e-14 : (w.P == CLG_PREC_SINGLE ? 1e-6 : 2e-3);
+  const char* venv = std::getenv("CLG_VERBOSE");
+  const bool verbose = venv && venv[0] == '1';
   int outer = 0;
   for (;; ++outer) {
     // r = b - A x  (FP64, true residual)
@@ -603,6 +623,7 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
     for (int r = 0; r < nrhs; ++r)
       if (!done[r]) budget_left = std::max(budget_left, S->p.max_iterations - iters[r]);
     if (budget_left <= 0) break;
+    w.inner_cap = budget_left;
     // inner tolerances
     for (int r = 0; r < nrhs; ++r) {
       double want = done[r] ? 1.0 : 0.5 * tol * std::sqrt(bn2[r] / std::max(rn2[r], 1e-300));
@@ -661,6 +682,11 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
       if (done[r]) continue;
       iters[r] += w.sum_h[r].iters;
       if (w.sum_h[r].status == ST_BREAKDOWN) inner_fail[r]++;
+      if (verbose)  // the reference logs per-restart deviations at PARANOIAC level (CSolverGMRES.cpp:234,246)
+        std::fprintf(stderr, "clg_solve outer %d rhs %d: |r|/|b| = %.3e, inner tol %.1e, inner applications %d, "
+                     "inner status %d, inner |r|/|r0| = %.3e\n", outer, r, std::sqrt(rn2[r] / std::max(bn2[r], 1e-300)),
+                     w.host_buf[r], w.sum_h[r].iters, w.sum_h[r].status,
+                     w.sum_h[r].rr0 > 0 ? std::sqrt((w.sum_h[r].rr > 0 ? w.sum_h[r].rr : w.sum_h[r].resid_est * w.sum_h[r].resid_est) / w.sum_h[r].rr0) : 0.0);
     }
     // x += e
     s = with_pn(w.P, nc, [&](auto PP, auto NN) {
