@@ -381,6 +381,17 @@ class _MultiShift(_Solver):
             self.ctx.check(st, "clg_solve_multishift")
         return out
 
+    def rational(self, f: _FermionField, gauge: CFieldGaugeSU3, op: int, c: float, a: Sequence[float],
+                 b: Sequence[float]):
+        """CFieldFermion::RationalApproximation: f <- c f + sum_i a_i (op + b_i)^-1 f."""
+        deg = len(a)
+        aa = np.ascontiguousarray(a, np.float64)
+        bb = np.ascontiguousarray(b, np.float64)
+        infos = (SolveInfo * deg)()
+        st = self.ctx.lib.clg_rational_apply(self.h, f.h, gauge.h, op, deg, c, _ptr(aa), _ptr(bb), infos)
+        self.ctx.check(st, "clg_rational_apply")
+        return [i.as_dict() for i in infos]
+
 
 class CMultiShiftCG(_MultiShift):
     KIND = SOLVER_CGM

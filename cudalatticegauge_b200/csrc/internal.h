@@ -197,4 +197,31 @@ clg_status blas_axpby(clg_context_s* ctx, const FieldRef& y, double2 a, const Fi
 clg_status blas_copy(clg_context_s* ctx, const FieldRef& dst, const FieldRef& src);               // converts precision
 clg_status blas_zero(clg_context_s* ctx, const FieldRef& y);
 
+// ------------------------------------------------------------ solves (solvers.cu)
+// One batched solve of (op + shift_r) x_r = b_r, r < nrhs, to prm->tol_true_rel
+// through the FP64 defect-correction loop.
+struct SolveReq {
+  clg_context_s* ctx = nullptr;
+  const clg_solver_params* prm = nullptr;
+  clg_gauge_s* U = nullptr;
+  clg_lattice_s* lat = nullptr;
+  int kind = 0;
+  double param = 0.0;
+  int op = 0;
+  int subset = 0;
+  int nrhs = 1;
+  FieldRef b;                  // nrhs right-hand sides, or one copied to every rhs
+  bool b_broadcast = false;
+  const FieldRef* x0 = nullptr;      // start vectors (any precision), nullable
+  const double2* shifts = nullptr;   // host, nrhs complex shifts, nullable
+  std::vector<FieldRef> xout;        // one field holding nrhs, or nrhs single fields
+  clg_solve_info* info = nullptr;
+};
+clg_status solve_core(const SolveReq& q);
+
 }  // namespace clg
+
+struct clg_solver_s {
+  clg_context_s* ctx = nullptr;
+  clg_solver_params p;
+};

@@ -1,21 +1,415 @@
-// multishift.cu -- CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47)
-// and CFieldFermion::RationalApproximation (Data/Field/CField.cpp:114-145).
-#include "internal.h"
+// multishift.cu -- CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47):
+// (op + c_n) x_n = b for n < nshift, and CFieldFermion::RationalApproximation
+// (Data/Field/CField.cpp:114-145).
+//
+// CLG_SOLVER_CGM (Hermitian positive operators, real shifts >= 0): multi-shift
+// CG (B. Jegerlehner, hep-lat/9612014) shares one Krylov space for all shifts in
+// the inner precision; every shift is then refined to the FP64 true residual by
+// the batched defect-correction loop with the shifts as right-hand sides.
+// The reference has no CG-M; its multi-shift family (CMultiShiftFOM,
+// CMultiShiftGMRES, CMultiShiftBiCGStab, CMultiShiftNested) shares the interface.
+//
+// CLG_SOLVER_FOM_MS (any operator, complex shifts): all shifts are solved as one
+// batch of right-hand sides (one launch per step covers every shift) by GMRES
+// in the inner precision inside FP64 defect correction, the batched counterpart
+// of CMultiShiftNested::Solve (CMultiShiftNested.cpp:69-145).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "krylov.cuh"
+
+namespace clg {
+
+constexpr int CGM_MAXSHIFT = 64;
+
+struct CgmState {
+  double rr, bb, tol2, alpha, alpha_old, beta, pq;
+  int iters, done, nshift, pad;
+  double shift[CGM_MAXSHIFT];
+  double zeta[CGM_MAXSHIFT], zeta_old[CGM_MAXSHIFT], zeta_new[CGM_MAXSHIFT];
+  double alpha_k[CGM_MAXSHIFT], beta_k[CGM_MAXSHIFT];
+  int active[CGM_MAXSHIFT];
+};
+
+namespace {
+
+// (p, q) -> alpha and the shifted alpha_k (Jegerlehner eq. for zeta_{n+1})
+template <int P, int NC>
+struct CgmAlpha {
+  DField p, q;
+  CgmState* st;
+  __device__ bool active(int) const { return !st->done; }
+  __device__ void operator()(int, int par, int64_t h, double* acc) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> a[NC], b[NC];
+    ldv<P, NC, AT>(p, 0, par, h, a);
+    ldv<P, NC, AT>(q, 0, par, h, b);
+    AT re = 0;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) re += a[k].x * b[k].x + a[k].y * b[k].y;
+    acc[0] += (double)re;
+  }
+  __device__ void finalize(int, const double* s) const {
+    CgmState& c = *st;
+    if (c.done) return;
+    c.iters += 1;
+    if (!(s[0] > 0.0) || bad(s[0])) {
+      c.done = 2;
+      return;
+    }
+    const double alpha = c.rr / s[0];
+    for (int k = 0; k < c.nshift; ++k) {
+      if (!c.active[k]) continue;
+      const double zn = c.zeta[k], zo = c.zeta_old[k];
+      const double den = alpha * c.beta * (zo - zn) + zo * c.alpha_old * (1.0 + c.shift[k] * alpha);
+      const double znew = zn * zo * c.alpha_old / den;
+      c.zeta_new[k] = znew;
+      c.alpha_k[k] = alpha * znew / zn;
+    }
+    c.alpha = alpha;
+  }
+};
+
+// x_k += alpha_k p_k   (grid.y = shift)
+template <int P, int NC>
+struct CgmX {
+  DField x, pk;
+  CgmState* st;
+  __device__ bool active(int k) const { return !st->done && st->active[k]; }
+  __device__ void operator()(int k, int par, int64_t h, double*) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> vx[NC], vp[NC];
+    ldv<P, NC, AT>(x, k, par, h, vx);
+    ldv<P, NC, AT>(pk, k, par, h, vp);
+    const AT a = (AT)st->alpha_k[k];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) vx[i] = vx[i] + a * vp[i];
+    stv<P, NC, AT>(x, k, par, h, vx);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
+// r -= alpha q ; |r|^2 -> beta, beta_k, convergence per shift
+template <int P, int NC>
+struct CgmR {
+  DField r, q;
+  CgmState* st;
+  __device__ bool active(int) const { return !st->done; }
+  __device__ void operator()(int, int par, int64_t h, double* acc) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> vr[NC], vq[NC];
+    ldv<P, NC, AT>(r, 0, par, h, vr);
+    ldv<P, NC, AT>(q, 0, par, h, vq);
+    const AT a = (AT)st->alpha;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) vr[i] = vr[i] - a * vq[i];
+    stv<P, NC, AT>(r, 0, par, h, vr);
+    acc[0] += site_norm2<NC, AT>(vr);
+  }
+  __device__ void finalize(int, const double* s) const {
+    CgmState& c = *st;
+    if (c.done) return;
+    if (bad(s[0])) {
+      c.done = 2;
+      return;
+    }
+    const double beta = s[0] / c.rr;
+    int nact = 0;
+    for (int k = 0; k < c.nshift; ++k) {
+      if (!c.active[k]) continue;
+      const double ratio = c.zeta_new[k] / c.zeta[k];
+      c.beta_k[k] = beta * ratio * ratio;
+      c.zeta_old[k] = c.zeta[k];
+      c.zeta[k] = c.zeta_new[k];
+      if (c.zeta[k] * c.zeta[k] * s[0] <= c.tol2 * c.bb)
+        c.active[k] = 0;
+      else
+        ++nact;
+    }
+    c.alpha_old = c.alpha;
+    c.beta = beta;
+    c.rr = s[0];
+    if (nact == 0) c.done = 1;
+  }
+};
+
+// p_k = zeta_k r + beta_k p_k   (grid.y = shift)
+template <int P, int NC>
+struct CgmPk {
+  DField pk, r;
+  CgmState* st;
+  __device__ bool active(int k) const { return !st->done && st->active[k]; }
+  __device__ void operator()(int k, int par, int64_t h, double*) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> vp[NC], vr[NC];
+    ldv<P, NC, AT>(pk, k, par, h, vp);
+    ldv<P, NC, AT>(r, 0, par, h, vr);
+    const AT z = (AT)st->zeta[k], b = (AT)st->beta_k[k];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) vp[i] = z * vr[i] + b * vp[i];
+    stv<P, NC, AT>(pk, k, par, h, vp);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
+// p = r + beta p
+template <int P, int NC>
+struct CgmP {
+  DField p, r;
+  CgmState* st;
+  __device__ bool active(int) const { return !st->done; }
+  __device__ void operator()(int, int par, int64_t h, double*) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> vp[NC], vr[NC];
+    ldv<P, NC, AT>(p, 0, par, h, vp);
+    ldv<P, NC, AT>(r, 0, par, h, vr);
+    const AT b = (AT)st->beta;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) vp[i] = vr[i] + b * vp[i];
+    stv<P, NC, AT>(p, 0, par, h, vp);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
+// start: r = p = b, x_k = 0, p_k = b, |b|^2
+template <int P, int NC>
+struct CgmInit {
+  DField b, r, p, x, pk;
+  CgmState* st;
+  int nshift;
+  __device__ bool active(int) const { return true; }
+  __device__ void operator()(int, int par, int64_t h, double* acc) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> vb[NC], z[NC];
+    ldv<P, NC, AT>(b, 0, par, h, vb);
+#pragma unroll
+    for (int i = 0; i < NC; ++i) z[i] = mk<AT>(0, 0);
+    stv<P, NC, AT>(r, 0, par, h, vb);
+    stv<P, NC, AT>(p, 0, par, h, vb);
+    for (int k = 0; k < nshift; ++k) {
+      stv<P, NC, AT>(x, k, par, h, z);
+      stv<P, NC, AT>(pk, k, par, h, vb);
+    }
+    acc[0] += site_norm2<NC, AT>(vb);
+  }
+  __device__ void finalize(int, const double* s) const {
+    CgmState& c = *st;
+    c.rr = c.bb = s[0];
+    c.alpha_old = 1.0;
+    c.beta = 0.0;
+    c.iters = 0;
+    c.done = s[0] > 0.0 ? 0 : 1;
+    for (int k = 0; k < c.nshift; ++k) {
+      c.zeta[k] = c.zeta_old[k] = 1.0;
+      c.active[k] = c.done ? 0 : 1;
+    }
+  }
+};
+
+struct OwnedF {
+  FieldRef ref;
+  void* data = nullptr;
+  float* norm = nullptr;
+  ~OwnedF() {
+    dfree(data);
+    dfree(norm);
+  }
+  clg_status alloc(clg_context_s* ctx, int prec, int nc, int nparity, int fp, int nrhs, int64_t Vh) {
+    const int64_t blk = Vh * site_bytes_of(prec, nc);
+    clg_status st = dalloc(ctx, &data, (size_t)blk * nparity * nrhs);
+    if (st) return st;
+    if (prec == CLG_PREC_HALF && (st = dalloc(ctx, (void**)&norm, (size_t)Vh * nparity * nrhs * sizeof(float)))) return st;
+    ref.data = (char*)data;
+    ref.norm = norm;
+    ref.blk = blk;
+    ref.rstride = blk * nparity;
+    ref.nrstride = norm ? Vh * nparity : 0;
+    ref.nparity = nparity;
+    ref.first_parity = fp;
+    ref.prec = prec;
+    ref.nc = nc;
+    ref.nrhs = nrhs;
+    ref.Vh = Vh;
+    return CLG_SUCCESS;
+  }
+};
+
+// Multi-shift CG in precision P on a Hermitian positive operator; X holds nshift rhs.
+clg_status cgm_run(clg_context_s* ctx, clg_gauge_s* U, int kind, double param, int op, const FieldRef& b,
+                   const FieldRef& X, const std::vector<double>& shifts, double tol, int max_iter, int* iters_out) {
+  const int P = X.prec, nc = X.nc, np = b.nparity, fp = b.first_parity;
+  const int64_t Vh = b.Vh;
+  const int ns = (int)shifts.size();
+  OwnedF bP, r, p, q, pk, t_odd, t_full;
+  clg_status s;
+  if ((s = bP.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = r.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
+      (s = p.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = q.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
+      (s = pk.alloc(ctx, P, nc, np, fp, ns, Vh)) || (s = t_odd.alloc(ctx, P, nc, 1, 1, 1, Vh)))
+    return s;
+  if (op == CLG_OP_DDDAG && (s = t_full.alloc(ctx, P, nc, 2, 0, 1, Vh))) return s;
+  if ((s = blas_copy(ctx, bP.ref, b))) return s;
+  CgmState* st = nullptr;
+  if ((s = dalloc(ctx, (void**)&st, sizeof(CgmState)))) return s;
+  CgmState h;
+  std::memset(&h, 0, sizeof(h));
+  h.nshift = ns;
+  h.tol2 = tol * tol;
+  for (int k = 0; k < ns; ++k) h.shift[k] = shifts[k];
+  cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
+  const double2 one = make_double2(1, 0);
+  const int* skip = &st->done;
+  s = with_pn(P, nc, [&](auto PP, auto NN) -> clg_status {
+    constexpr int PV = PP.value, NV = NN.value;
+    clg_status e = launch_sites<1>(ctx, CgmInit<PV, NV>{dfield(bP.ref), dfield(r.ref), dfield(p.ref), dfield(X),
+                                                         dfield(pk.ref), st, ns},
+                                   fp, np, Vh, 1);
+    if (e) return e;
+    const int chunk = 16;
+    cudaGraphExec_t exec = nullptr;
+    auto body = [&]() -> clg_status {
+      clg_status e2;
+      const FieldRef* tmp = (op == CLG_OP_DDDAG) ? &t_full.ref : &t_odd.ref;
+      if ((e2 = apply_op(ctx, op, U, kind, param, q.ref, p.ref, tmp, one, 1, nullptr, 0, skip, 0))) return e2;
+      if ((e2 = launch_sites<1>(ctx, CgmAlpha<PV, NV>{dfield(p.ref), dfield(q.ref), st}, fp, np, Vh, 1))) return e2;
+      if ((e2 = launch_sites<0>(ctx, CgmX<PV, NV>{dfield(X), dfield(pk.ref), st}, fp, np, Vh, ns))) return e2;
+      if ((e2 = launch_sites<1>(ctx, CgmR<PV, NV>{dfield(r.ref), dfield(q.ref), st}, fp, np, Vh, 1))) return e2;
+      if ((e2 = launch_sites<0>(ctx, CgmPk<PV, NV>{dfield(pk.ref), dfield(r.ref), st}, fp, np, Vh, ns))) return e2;
+      return launch_sites<0>(ctx, CgmP<PV, NV>{dfield(p.ref), dfield(r.ref), st}, fp, np, Vh, 1);
+    };
+    int done = 0, it = 0;
+    CgmState* hs = nullptr;
+    if (cudaMallocHost((void**)&hs, sizeof(CgmState)) != cudaSuccess) return ctx->fail(CLG_ERR_OOM, "pinned");
+    e = CLG_SUCCESS;
+    for (int c = 0; c * chunk < max_iter + chunk; ++c) {
+      if (c == 1 && ctx->stream) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+          for (int i = 0; i < chunk && !e; ++i) e = body();
+          if (cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && g && !e) cudaGraphInstantiate(&exec, g, 0);
+          if (g) cudaGraphDestroy(g);
+          cudaGetLastError();
+        }
+      }
+      if (e) break;
+      if (exec) {
+        if (cudaGraphLaunch(exec, ctx->stream) != cudaSuccess) {
+          e = ctx->fail(CLG_ERR_CUDA, "multi-shift graph launch");
+          break;
+        }
+      } else {
+        for (int i = 0; i < chunk && !e; ++i) e = body();
+        if (e) break;
+      }
+      if (cudaMemcpyAsync(hs, st, sizeof(CgmState), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+          cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        e = ctx->fail(CLG_ERR_CUDA, "multi-shift sync");
+        break;
+      }
+      done = hs->done;
+      it = hs->iters;
+      if (done || it >= max_iter) break;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaFreeHost(hs);
+    *iters_out = it;
+    return e;
+  });
+  dfree(st);
+  return s;
+}
+
+}  // namespace
+}  // namespace clg
+
+using namespace clg;
 
 extern "C" {
 
-clg_status clg_solve_multishift(clg_solver s, clg_field* x, int nshift, const double* shifts, clg_field b, clg_gauge g,
+clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const double* shifts, clg_field b, clg_gauge g,
                                 int op, clg_solve_info* info) {
-  (void)x; (void)nshift; (void)shifts; (void)b; (void)g; (void)op; (void)info;
-  if (!s) return CLG_ERR_BAD_ARG;
-  return CLG_ERR_UNSUPPORTED;
+  if (!S || !x || !b || !g || !shifts || !info || nshift < 1) return CLG_ERR_BAD_ARG;
+  clg_context_s* ctx = S->ctx;
+  if (nshift > CGM_MAXSHIFT) return ctx->fail(CLG_ERR_UNSUPPORTED, "at most 64 shifts");
+  if (b->nrhs != 1) return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift solves take one right-hand side");
+  for (int k = 0; k < nshift; ++k) {
+    if (!x[k] || x[k]->lat != b->lat || x[k]->kind != b->kind || x[k]->subset != b->subset || x[k]->nrhs != 1)
+      return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift: solution fields must match b");
+    if (x[k]->data == b->data) return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift: x must not alias b (CMultiShiftSolver.h:35)");
+  }
+  if (S->p.kind != CLG_SOLVER_CGM && S->p.kind != CLG_SOLVER_FOM_MS)
+    return ctx->fail(CLG_ERR_BAD_ARG, "clg_solve_multishift needs a CGM or FOM_MS solver");
+  std::vector<double2> sh(nshift);
+  for (int k = 0; k < nshift; ++k) sh[k] = make_double2(shifts[2 * k], shifts[2 * k + 1]);
+  const bool hermitian = op == CLG_OP_DDDAG || op == CLG_OP_DDDAG_EE || op == CLG_OP_MEE_MEEDAG;
+  clg_solver_params prm = S->p;
+  clg_status s = CLG_SUCCESS;
+  const int P = prm.inner_precision;
+  const int nc = b->nc();
+  const int64_t Vh = b->lat->g.Vh;
+  OwnedF X;
+  int cgm_iters = 0;
+  const bool use_cgm = S->p.kind == CLG_SOLVER_CGM;
+  if (use_cgm) {
+    if (!hermitian) return ctx->fail(CLG_ERR_BAD_ARG, "CG-M needs a Hermitian positive operator (DDdagger forms)");
+    std::vector<double> real(nshift);
+    for (int k = 0; k < nshift; ++k) {
+      if (sh[k].y != 0.0 || sh[k].x < 0.0) return ctx->fail(CLG_ERR_BAD_ARG, "CG-M shifts must be real and >= 0");
+      real[k] = sh[k].x;
+    }
+    if ((s = gauge_prepare(g, P))) return s;
+    if (op == CLG_OP_MEE_MEEDAG) return ctx->fail(CLG_ERR_UNSUPPORTED, "CG-M on MEE_MEEDAG: use FOM_MS");
+    if ((s = X.alloc(ctx, P, nc, b->nparity(), 0, nshift, Vh))) return s;
+    const double itol = P == CLG_PREC_DOUBLE ? prm.tol_true_rel * 0.5 : std::max(prm.inner_tol, 1e-6);
+    if ((s = cgm_run(ctx, g, b->kind, b->param, op, b->ref(), X.ref, real, itol, prm.max_iterations, &cgm_iters)))
+      return s;
+    prm.kind = CLG_SOLVER_CG;  // per-shift refinement
+  } else {
+    prm.kind = hermitian ? CLG_SOLVER_CG : CLG_SOLVER_GMRES;
+  }
+  SolveReq q;
+  q.ctx = ctx;
+  q.prm = &prm;
+  q.U = g;
+  q.lat = b->lat;
+  q.kind = b->kind;
+  q.param = b->param;
+  q.op = op;
+  q.subset = b->subset;
+  q.nrhs = nshift;
+  q.b = b->ref();
+  q.b_broadcast = true;
+  if (use_cgm) q.x0 = &X.ref;
+  q.shifts = sh.data();
+  for (int k = 0; k < nshift; ++k) q.xout.push_back(x[k]->ref());
+  q.info = info;
+  s = solve_core(q);
+  for (int k = 0; k < nshift; ++k) info[k].iterations += cgm_iters;
+  return s;
 }
 
-clg_status clg_rational_apply(clg_solver s, clg_field f, clg_gauge g, int op, int degree, double c, const double* a,
-                              const double* b, clg_solve_info* info) {
-  (void)f; (void)g; (void)op; (void)degree; (void)c; (void)a; (void)b; (void)info;
-  if (!s) return CLG_ERR_BAD_ARG;
-  return CLG_ERR_UNSUPPORTED;
+clg_status clg_rational_apply(clg_solver S, clg_field f, clg_gauge g, int op, int degree, double c, const double* a,
+                              const double* bsh, clg_solve_info* info) {
+  if (!S || !f || !g || !a || !bsh || !info || degree < 1) return CLG_ERR_BAD_ARG;
+  clg_context_s* ctx = S->ctx;
+  if (f->nrhs != 1) return ctx->fail(CLG_ERR_BAD_ARG, "rational approximation acts on one field");
+  std::vector<clg_field> xs(degree, nullptr);
+  clg_status s = CLG_SUCCESS;
+  for (int i = 0; i < degree && !s; ++i) s = clg_field_create(f->lat, f->kind, f->subset, f->prec, 1, f->param, &xs[i]);
+  std::vector<double> sh(2 * degree, 0.0);
+  for (int i = 0; i < degree; ++i) sh[2 * i] = bsh[i];
+  if (!s) s = clg_solve_multishift(S, xs.data(), degree, sh.data(), f, g, op, info);
+  // f <- c f + sum_i a_i x_i   (CField.cpp:140-146)
+  if (!s || s == CLG_ERR_NOT_CONVERGED) {
+    clg_status t = blas_axpby(ctx, f->ref(), make_double2(0, 0), f->ref(), make_double2(c, 0));
+    for (int i = 0; i < degree && !t; ++i) t = blas_axpby(ctx, f->ref(), make_double2(a[i], 0), xs[i]->ref(), make_double2(1, 0));
+    if (t) s = t;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && !s) s = ctx->fail(CLG_ERR_CUDA, "rational sync");
+  }
+  for (auto x : xs)
+    if (x) clg_field_destroy(x);
+  return s;
 }
 
 }  // extern "C"

@@ -123,6 +123,34 @@ struct Resid {
   __device__ void finalize(int rhs, const double* s) const { out[rhs] = s[0]; }
 };
 
+// out += sigma_r * scale_r * in  (the shift of a shifted system; scale for lazily normalised inputs)
+template <int P, int NC>
+struct ShiftAdd {
+  DField out, in;
+  const double2* shift;
+  const double* scale;
+  int sstride;
+  const int* skip;
+  int kstride;
+  __device__ bool active(int r) const { return !(skip && skip[(int64_t)r * kstride]); }
+  __device__ void operator()(int rhs, int p, int64_t h, double*) const {
+    using AT = typename AccT<P>::T;
+    double2 sg = shift[rhs];
+    if (scale) {
+      const double sc = scale[(int64_t)rhs * sstride];
+      sg = make_double2(sg.x * sc, sg.y * sc);
+    }
+    cpx<AT> vo[NC], vi[NC];
+    ldv<P, NC, AT>(out, rhs, p, h, vo);
+    ldv<P, NC, AT>(in, rhs, p, h, vi);
+    const cpx<AT> c = mk<AT>((AT)sg.x, (AT)sg.y);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) vo[k] = vo[k] + c * vi[k];
+    stv<P, NC, AT>(out, rhs, p, h, vo);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
 template <int P, int NC>
 struct CopySkip {
   DField d, s;
@@ -180,12 +208,6 @@ bool hermitian_op(int op) { return op == CLG_OP_DDDAG || op == CLG_OP_DDDAG_EE |
 
 using namespace clg;
 
-// ------------------------------------------------------------------ solver object
-struct clg_solver_s {
-  clg_context_s* ctx = nullptr;
-  clg_solver_params p;
-};
-
 namespace {
 
 // Everything one solve needs, allocated per call.
@@ -204,6 +226,7 @@ struct Work {
   double* tol_d = nullptr;
   double* red_d = nullptr;   // per-rhs reduction outputs
   double* host_buf = nullptr;
+  double2* shift_dev = nullptr;  // per-rhs shift sigma_r: the system is (op + sigma_r) x_r = b_r
   // Krylov operator temporaries (precision P)
   Owned kt_odd, kt_even, kt_full;
   // Krylov vectors per graph slot: they persist for the whole solve so a
@@ -235,6 +258,7 @@ struct Work {
     dfree(outer_done_d);
     dfree(tol_d);
     dfree(red_d);
+    dfree(shift_dev);
     if (sum_h) cudaFreeHost(sum_h);
     if (host_buf) cudaFreeHost(host_buf);
   }
@@ -250,8 +274,8 @@ clg_status read_summary(Work& w) {
 }
 
 // Krylov operator K on fields of precision P: out = K in (optionally * scale_dev[rhs])
-clg_status kapply(Work& w, int op, const FieldRef& out, const FieldRef& in, const double* scale, int sstride,
-                  const int* skip, int kstride) {
+clg_status kapply_base(Work& w, int op, const FieldRef& out, const FieldRef& in, const double* scale, int sstride,
+                       const int* skip, int kstride) {
   const double2 one = make_double2(1, 0);
   if (op == CLG_OP_MEE_MEEDAG) {
     clg_status s = apply_op(w.ctx, CLG_OP_MEE_DAG, w.U, w.kind, w.param, w.kt_even.ref, in, &w.kt_odd.ref, one, w.nrhs,
@@ -262,6 +286,16 @@ clg_status kapply(Work& w, int op, const FieldRef& out, const FieldRef& in, cons
   }
   const FieldRef* tmp = (op == CLG_OP_DDDAG || op == CLG_OP_DD) ? &w.kt_full.ref : &w.kt_odd.ref;
   return apply_op(w.ctx, op, w.U, w.kind, w.param, out, in, tmp, one, w.nrhs, scale, sstride, skip, kstride);
+}
+
+clg_status kapply(Work& w, int op, const FieldRef& out, const FieldRef& in, const double* scale, int sstride,
+                  const int* skip, int kstride) {
+  clg_status s = kapply_base(w, op, out, in, scale, sstride, skip, kstride);
+  if (s || !w.shift_dev) return s;
+  return with_pn(out.prec, out.nc, [&](auto PP, auto NN) {
+    ShiftAdd<PP.value, NN.value> f{dfield(out), dfield(in), w.shift_dev, scale, sstride, skip, kstride};
+    return launch_sites<0>(w.ctx, f, out.first_parity, out.nparity, out.Vh, w.nrhs);
+  });
 }
 
 // Run `body` (one iteration or one cycle) repeatedly until every rhs is done
@@ -495,14 +529,42 @@ clg_status clg_solver_destroy(clg_solver s) {
 clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op, clg_field X0, clg_solve_info* info) {
   if (!S || !X || !B || !U || !info) return CLG_ERR_BAD_ARG;
   clg_context_s* ctx = S->ctx;
-  const double t0 = now_s();
   if (X->lat != B->lat || U->lat != B->lat || X->kind != B->kind || X->subset != B->subset || X->nrhs != B->nrhs ||
       (X0 && (X0->lat != B->lat || X0->subset != B->subset || X0->nrhs != B->nrhs || X0->kind != B->kind)))
     return ctx->fail(CLG_ERR_BAD_ARG, "solve: field shapes differ");
   if (S->p.kind == CLG_SOLVER_CGM || S->p.kind == CLG_SOLVER_FOM_MS)
     return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift solvers are called through clg_solve_multishift");
-  const bool full = B->subset == CLG_SUBSET_FULL;
-  const bool wilson = B->kind == CLG_FERMION_WILSON;
+  SolveReq q;
+  q.ctx = ctx;
+  q.prm = &S->p;
+  q.U = U;
+  q.lat = B->lat;
+  q.kind = B->kind;
+  q.param = B->param;
+  q.op = op;
+  q.subset = B->subset;
+  q.nrhs = B->nrhs;
+  q.b = B->ref();
+  FieldRef x0r;
+  if (X0) {
+    x0r = X0->ref();
+    q.x0 = &x0r;
+  }
+  q.xout.push_back(X->ref());
+  q.info = info;
+  return solve_core(q);
+}
+
+}  // extern "C"
+
+clg_status clg::solve_core(const SolveReq& q) {
+  clg_context_s* ctx = q.ctx;
+  clg_gauge_s* U = q.U;
+  const int op = q.op;
+  const double t0 = now_s();
+  clg_solve_info* info = q.info;
+  const bool full = q.subset == CLG_SUBSET_FULL;
+  const bool wilson = q.kind == CLG_FERMION_WILSON;
   const bool even_ops = op == CLG_OP_MEE || op == CLG_OP_MEE_DAG || op == CLG_OP_MEE_MEEDAG || op == CLG_OP_DDDAG_EE;
   if (even_ops == full) return ctx->fail(CLG_ERR_BAD_ARG, "solve: Schur operators act on EVEN fields, D forms on FULL");
   if (!(op == CLG_OP_D || op == CLG_OP_DDAG || op == CLG_OP_DDDAG || even_ops))
@@ -510,19 +572,22 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
   if ((op == CLG_OP_MEE || op == CLG_OP_MEE_DAG || op == CLG_OP_MEE_MEEDAG) && !wilson)
     return ctx->fail(CLG_ERR_BAD_ARG, "MEE forms are Wilson operators");
   if (op == CLG_OP_DDDAG_EE && wilson) return ctx->fail(CLG_ERR_BAD_ARG, "DDDAG_EE is the staggered Schur operator");
+  if (q.shifts && (op == CLG_OP_D || op == CLG_OP_DDAG) && q.prm->kind == CLG_SOLVER_CG)
+    return ctx->fail(CLG_ERR_BAD_ARG, "CG needs a Hermitian operator");
 
   Work w;
   w.ctx = ctx;
   w.U = U;
-  w.kind = B->kind;
+  w.kind = q.kind;
   w.op = op;
-  w.P = S->p.inner_precision;
-  w.nc = B->nc();
-  w.nrhs = B->nrhs;
-  w.param = B->param;
-  w.Vh = B->lat->g.Vh;
-  w.prm = &S->p;
+  w.P = q.prm->inner_precision;
+  w.nc = q.kind == CLG_FERMION_WILSON ? 12 : 3;
+  w.nrhs = q.nrhs;
+  w.param = q.param;
+  w.Vh = q.lat->g.Vh;
+  w.prm = q.prm;
   const int nrhs = w.nrhs;
+  const clg_solver_params* prm = q.prm;
   clg_status s = CLG_SUCCESS;
   if ((s = gauge_prepare(U, w.P))) return s;
   if ((s = dalloc(ctx, (void**)&w.st, sizeof(KState) * nrhs)) || (s = dalloc(ctx, (void**)&w.sum_d, sizeof(Summary) * nrhs)) ||
@@ -535,7 +600,13 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
   cudaMemsetAsync(w.st, 0, sizeof(KState) * nrhs, ctx->stream);
 
   // Schur (even-odd) path for D / D^+ on full fields; Wilson DD^+ = two Schur solves
-  const bool schur = full && S->p.even_odd && (op == CLG_OP_D || op == CLG_OP_DDAG || (op == CLG_OP_DDDAG && wilson));
+  const bool schur =
+      full && prm->even_odd && !q.shifts && (op == CLG_OP_D || op == CLG_OP_DDAG || (op == CLG_OP_DDDAG && wilson));
+  if (q.shifts) {
+    if ((s = dalloc(ctx, (void**)&w.shift_dev, sizeof(double2) * nrhs))) return s;
+    if (cudaMemcpy(w.shift_dev, q.shifts, sizeof(double2) * nrhs, cudaMemcpyHostToDevice) != cudaSuccess)
+      return ctx->fail(CLG_ERR_CUDA, "solve: shifts upload");
+  }
   const int kop_d = wilson ? CLG_OP_MEE : CLG_OP_DDDAG_EE;
   const int kop_ddag = wilson ? CLG_OP_MEE_DAG : CLG_OP_DDDAG_EE;
   const int64_t Vh = w.Vh;
@@ -560,8 +631,13 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
   if (!schur && op == CLG_OP_DDDAG && (s = w.kt_full.alloc(ctx, w.P, nc, 2, 0, nrhs, Vh))) return s;
 
   // b64 = B, x64 = X0 or 0
-  if ((s = blas_copy(ctx, b64.ref, B->ref()))) return s;
-  if (X0) s = blas_copy(ctx, x64.ref, X0->ref());
+  if (q.b_broadcast) {
+    for (int r = 0; r < nrhs; ++r)
+      if ((s = blas_copy(ctx, b64.ref.rhs_view(r, 1), q.b.rhs_view(0, 1)))) return s;
+  } else if ((s = blas_copy(ctx, b64.ref, q.b))) {
+    return s;
+  }
+  if (q.x0) s = blas_copy(ctx, x64.ref, *q.x0);
   else s = blas_zero(ctx, x64.ref);
   if (s) return s;
   if ((s = blas_norm2(ctx, b64.ref, w.red_d))) return s;
@@ -571,7 +647,7 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
     return ctx->fail(CLG_ERR_CUDA, "solve: reading |b|");
   for (int r = 0; r < nrhs; ++r) bn2[r] = w.host_buf[r];
 
-  const double tol = S->p.tol_true_rel;
+  const double tol = prm->tol_true_rel;
   std::vector<int> done(nrhs, 0), outer_count(nrhs, 0), status(nrhs, CLG_ERR_NOT_CONVERGED), iters(nrhs, 0);
   std::vector<int> inner_fail(nrhs, 0);
   const double2 one = make_double2(1, 0);
@@ -596,6 +672,13 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
     } else {
       if ((s = apply_op(ctx, op, U, w.kind, w.param, r64.ref, x64.ref, tmp, one, nrhs))) return s;
     }
+    if (w.shift_dev) {
+      s = with_pn(0, nc, [&](auto PP, auto NN) {
+        ShiftAdd<PP.value, NN.value> f{dfield(r64.ref), dfield(x64.ref), w.shift_dev, nullptr, 0, nullptr, 0};
+        return launch_sites<0>(ctx, f, 0, npar, Vh, nrhs);
+      });
+      if (s) return s;
+    }
     s = with_pn(0, nc, [&](auto, auto NN) {
       return launch_sites<1>(ctx, Resid<NN.value>{dfield(b64.ref), dfield(r64.ref), w.red_d}, 0, npar, Vh, nrhs);
     });
@@ -618,16 +701,16 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
       }
       all = all && done[r];
     }
-    if (all || outer >= S->p.max_outer) break;
+    if (all || outer >= prm->max_outer) break;
     int budget_left = 0;
     for (int r = 0; r < nrhs; ++r)
-      if (!done[r]) budget_left = std::max(budget_left, S->p.max_iterations - iters[r]);
+      if (!done[r]) budget_left = std::max(budget_left, prm->max_iterations - iters[r]);
     if (budget_left <= 0) break;
     w.inner_cap = budget_left;
     // inner tolerances
     for (int r = 0; r < nrhs; ++r) {
       double want = done[r] ? 1.0 : 0.5 * tol * std::sqrt(bn2[r] / std::max(rn2[r], 1e-300));
-      if (w.P != CLG_PREC_DOUBLE) want = std::max(want, S->p.inner_tol);
+      if (w.P != CLG_PREC_DOUBLE) want = std::max(want, prm->inner_tol);
       w.host_buf[r] = std::min(0.5, std::max(want, lo_tol));
       ((int*)(w.host_buf + nrhs))[r] = done[r];
       if (!done[r]) outer_count[r]++;
@@ -696,7 +779,12 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
     if (s) return s;
   }
   // write the solution
-  if ((s = blas_copy(ctx, X->ref(), x64.ref))) return s;
+  if (q.xout.size() == 1) {
+    if ((s = blas_copy(ctx, q.xout[0], x64.ref))) return s;
+  } else {
+    for (int r = 0; r < nrhs && r < (int)q.xout.size(); ++r)
+      if ((s = blas_copy(ctx, q.xout[r], x64.ref.rhs_view(r, 1)))) return s;
+  }
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return ctx->fail(CLG_ERR_CUDA, "solve: final sync");
   const double t1 = now_s();
   clg_status overall = CLG_SUCCESS;
@@ -712,5 +800,3 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
   }
   return overall;
 }
-
-}  // extern "C"
