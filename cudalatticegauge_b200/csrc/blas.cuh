@@ -56,15 +56,35 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
     if (last) {
+      // every thread of the last block sums a fixed strided subset of the block
+      // partials, then a fixed shuffle / shared-memory tree: parallel and
+      // deterministic (independent of which block arrived last)
+      __shared__ double tot[NRED];
       __threadfence();
-      for (int r = threadIdx.x; r < (int)gridDim.y; r += blockDim.x) {
+      for (int r = 0; r < (int)gridDim.y; ++r) {
         double s[NRED];
 #pragma unroll
         for (int k = 0; k < NRED; ++k) s[k] = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b)
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
 #pragma unroll
           for (int k = 0; k < NRED; ++k) s[k] += __ldcg(partials + ((int64_t)r * gridDim.x + b) * NRED + k);
-        f.finalize(r, s);
+#pragma unroll
+        for (int k = 0; k < NRED; ++k) {
+          double v = s[k];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+          if (lane == 0) sm[k][warp] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < NRED) {
+          double v = 0.0;
+          const int nw = (blockDim.x + 31) >> 5;
+          for (int w = 0; w < nw; ++w) v += sm[threadIdx.x][w];
+          tot[threadIdx.x] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) f.finalize(r, tot);
+        __syncthreads();
       }
       if (threadIdx.x == 0) *counter = 0u;
     }
