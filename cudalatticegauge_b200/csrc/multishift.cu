@@ -280,13 +280,17 @@ clg_status cgm_run(clg_context_s* ctx, clg_gauge_s* U, int kind, double param, i
     };
     int done = 0, it = 0;
     CgmState* hs = nullptr;
+    int64_t graph_kernels = 0;
     if (cudaMallocHost((void**)&hs, sizeof(CgmState)) != cudaSuccess) return ctx->fail(CLG_ERR_OOM, "pinned");
     e = CLG_SUCCESS;
     for (int c = 0; c * chunk < max_iter + chunk; ++c) {
       if (c == 1 && ctx->stream) {
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+          const int64_t k0 = ctx->kernels;  // captured launches are counted per replay
           for (int i = 0; i < chunk && !e; ++i) e = body();
+          graph_kernels = ctx->kernels - k0;
+          ctx->kernels = k0;
           if (cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && g && !e) cudaGraphInstantiate(&exec, g, 0);
           if (g) cudaGraphDestroy(g);
           cudaGetLastError();
@@ -298,6 +302,7 @@ clg_status cgm_run(clg_context_s* ctx, clg_gauge_s* U, int kind, double param, i
           e = ctx->fail(CLG_ERR_CUDA, "multi-shift graph launch");
           break;
         }
+        ctx->kernels += graph_kernels;
       } else {
         for (int i = 0; i < chunk && !e; ++i) e = body();
         if (e) break;

@@ -234,6 +234,7 @@ struct Work {
   std::map<int, std::vector<std::unique_ptr<Owned>>> kv;
   // graphs
   std::vector<cudaGraphExec_t> graphs;
+  std::vector<int64_t> graph_kernels;  // kernel nodes per graph (for the launch count)
   int total_iters = 0;
   int inner_cap = 1 << 30;  // operator applications allowed in the current inner solve
   clg_status kvec(int slot, int idx, int np, int fp, FieldRef& out) {
@@ -304,6 +305,7 @@ template <class Body>
 clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& body) {
   const bool graphs = w.prm->use_graphs && w.ctx->stream != nullptr;
   while ((int)w.graphs.size() <= graph_slot) w.graphs.push_back(nullptr);
+  while ((int)w.graph_kernels.size() <= graph_slot) w.graph_kernels.push_back(0);
   // stagnation guard: an inner solve ends when no running rhs has improved its
   // residual (recursive, or the GMRES estimate) for `patience` chunks
   std::vector<double> best(w.nrhs, 1e300);
@@ -314,7 +316,11 @@ clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& bo
     if (graphs && c > 0 && !w.graphs[graph_slot]) {
       cudaGraph_t g = nullptr;
       if (cudaStreamBeginCapture(w.ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        // captured launches do not run here: count them once per replay instead
+        const int64_t k0 = w.ctx->kernels;
         for (int i = 0; i < chunk && !s; ++i) s = body();
+        w.graph_kernels[graph_slot] = w.ctx->kernels - k0;
+        w.ctx->kernels = k0;
         cudaError_t e = cudaStreamEndCapture(w.ctx->stream, &g);
         if (!s && e == cudaSuccess && g) {
           cudaGraphExec_t ex = nullptr;
@@ -330,6 +336,7 @@ clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& bo
     if (graphs && w.graphs[graph_slot]) {
       cudaError_t e = cudaGraphLaunch(w.graphs[graph_slot], w.ctx->stream);
       if (e != cudaSuccess) return w.ctx->fail(cuda_status(e), std::string("graph launch: ") + cudaGetErrorString(e));
+      w.ctx->kernels += w.graph_kernels[graph_slot];
     } else {
       for (int i = 0; i < chunk && !s; ++i) s = body();
       if (s) return s;
