@@ -95,6 +95,7 @@ SIGNATURES = [
     ("clg_apply", _S, [_I, _P, _P, _I, _D, _D]),
     ("clg_apply_to", _S, [_I, _P, _P, _P, _I, _D, _D]),
     ("clg_dot", _S, [_P, _P, _P]),
+    ("clg_dot_noalloc", _S, [_P, _P, _P]),
     ("clg_norm2", _S, [_P, _P]),
     ("clg_axpy", _S, [_P, _D, _D, _P]),
     ("clg_scale", _S, [_P, _D, _D]),

@@ -147,6 +147,17 @@ clg_status clg_apply_to(int op, clg_field out, clg_field in, clg_gauge g, int co
  * CField BLAS (Data/Field/CField.h:127-201): Dot = sum conj(a) b, accumulated in
  * FP64 (re_im holds 2*nrhs doubles), Axpy, ScalarMultply, Zero, CopyTo. */
 clg_status clg_dot(clg_field a, clg_field b, double* re_im);
+/* No counterpart in the reference.  clg_dot without any device allocation, for
+ * callers that may not call cudaMalloc: code that gives all device memory to its
+ * own pool up front, code under a fixed device-memory budget, or a hot loop that
+ * cannot afford the device-wide synchronisation cudaMalloc / cudaFree imply.
+ * Same result as clg_dot; the scratch lives in one fixed 64 KiB __device__
+ * array of the library (held on every GPU that loads it until exit), so at most
+ * CLG_DOT_NOALLOC_MAX_RHS right-hand sides (CLG_ERR_BAD_ARG beyond).  The first
+ * call on a device looks the array up; make it before any stream capture.  All
+ * calls share the array: calls that overlap on one GPU race. */
+#define CLG_DOT_NOALLOC_MAX_RHS 64
+clg_status clg_dot_noalloc(clg_field a, clg_field b, double* re_im);
 clg_status clg_norm2(clg_field a, double* out);
 clg_status clg_axpy(clg_field y, double are, double aim, clg_field x);
 clg_status clg_scale(clg_field y, double are, double aim);
