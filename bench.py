@@ -33,6 +33,9 @@ UNIT = "solves/s"
 WORKLOADS = {
     "wilson_eo_32x32x32x16": dict(dims=(32, 32, 32, 16), kappa=0.1355, eps=0.25, seed=0xC1A60001, nrhs=1),
     "wilson_eo_16x16x16x8": dict(dims=(16, 16, 16, 8), kappa=0.1355, eps=0.25, seed=0xC1A60001, nrhs=1),
+    # 12 spin-colour point sources + 16 Z2 noise sources in one batched solve
+    "wilson_eo_batched_32x32x32x32": dict(dims=(32, 32, 32, 32), kappa=0.1355, eps=0.25, seed=0xC1A60003, nrhs=28,
+                                          sources="point12_z2_16"),
 }
 DEFAULT_WORKLOAD = "wilson_eo_32x32x32x16"
 TOL = 1e-10
@@ -52,30 +55,54 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    """nvidia-smi sampled every 200 ms by a background process; started before
+    the warm-up (its start-up stalls the driver briefly) and filtered to the
+    samples that arrive inside the timed window."""
+
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.lines = []
+        self.window = (0.0, 0.0)
 
     def start(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, ValueError):
             self.proc = None
+            return
+
+        def reader():
+            for line in self.proc.stdout:
+                self.lines.append((time.monotonic(), line))
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+
+    def mark(self, begin: bool):
+        t = time.monotonic()
+        self.window = (t, self.window[1]) if begin else (self.window[0], t)
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+        self.thread.join(timeout=5)
+        t0, t1 = self.window
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for ts, line in self.lines:
+            if not (t0 <= ts <= t1 + 0.25):
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -186,10 +213,20 @@ def ours(args, world, rank, local):
     U.InitialField(clg.GAUGE_EXPH, W["seed"], 1, W["eps"])
     nrhs = W["nrhs"]
     b = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
-    for r in range(nrhs):
-        b.InitialField(clg.SOURCE_GAUSS, W["seed"] + 7919 * rank, 2 + r, rhs=r)
+    seed = W["seed"] + 7919 * rank
+    if W.get("sources") == "point12_z2_16":
+        # the 12 spin-colour point sources of a meson propagator at the origin
+        # (CMeasureMesonCorrelator.cu:320-340) followed by Z2 noise sources
+        for r in range(12):
+            b.InitialAsSource(0, r, rhs=r)
+        for r in range(12, nrhs):
+            b.InitialField(clg.SOURCE_Z2, seed, 2 + r, rhs=r)
+    else:
+        for r in range(nrhs):
+            b.InitialField(clg.SOURCE_GAUSS, seed, 2 + r, rhs=r)
     x = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
-    mixed = clg.CSLASolverGMRES(ctx, inner_precision=clg.SINGLE, tol_true_rel=TOL, MaxDim=12)
+    inner = {"single": clg.SINGLE, "half": clg.HALF}[args.inner]
+    mixed = clg.CSLASolverGMRES(ctx, inner_precision=inner, tol_true_rel=TOL, MaxDim=12)
 
     def check(infos):
         for i in infos:
@@ -197,22 +234,24 @@ def ours(args, world, rank, local):
                 raise RuntimeError(f"solve failed: {i}")
         return infos
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         check(mixed.Solve(x, b, U, clg.EFO_F_D))
 
     # ---------------- timed region: K solves, inputs resident in HBM
     barrier(world)
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
     k0 = ctx.kernel_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark(True)
     e0.record(stream)
     infos = []
     for _ in range(args.steps):
         infos = check(mixed.Solve(x, b, U, clg.EFO_F_D))
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks.mark(False)
     clk = clocks.stop()
     launches = ctx.kernel_count() - k0
     t_local = e0.elapsed_time(e1) / 1e3
@@ -221,24 +260,31 @@ def ours(args, world, rank, local):
     value = args.steps * nrhs * world / t
 
     # ---------------- end to end through the public API with host buffers
-    src = torch.empty((V, 4, 3), dtype=torch.complex128, pin_memory=True).numpy()
-    dst = torch.empty((V, 4, 3), dtype=torch.complex128, pin_memory=True).numpy()
-    b.to_numpy(0, out=src)
-    b1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
-    x1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    src = torch.empty((nrhs, V, 4, 3), dtype=torch.complex128, pin_memory=True).numpy()
+    dst = torch.empty((nrhs, V, 4, 3), dtype=torch.complex128, pin_memory=True).numpy()
+    for r in range(nrhs):
+        b.to_numpy(r, out=src[r])
+    bh = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
+    xh = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
     barrier(world)
     torch.cuda.synchronize()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for _ in range(args.steps):
-        b1.from_numpy(src)
-        check(mixed.Solve(x1, b1, U, clg.EFO_F_D))
-        x1.to_numpy(0, out=dst)
+        for r in range(nrhs):
+            bh.from_numpy(src[r], r)
+        check(mixed.Solve(xh, bh, U, clg.EFO_F_D))
+        for r in range(nrhs):
+            xh.to_numpy(r, out=dst[r])
     e3.record(stream)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3, world)
-    e2e = {"value": args.steps * world / t_e2e, "unit": UNIT,
+    e2e = {"value": args.steps * nrhs * world / t_e2e, "unit": UNIT,
            "h2d_bytes_per_step": int(src.nbytes), "d2h_bytes_per_step": int(dst.nbytes)}
+    bh.close()
+    xh.close()
+    b1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    b1.from_numpy(src[nrhs - 1])
 
     # ---------------- roofline of the dominant kernel (FP32 checkerboard hop)
     peak, peak_kind = peaks()
@@ -288,11 +334,16 @@ def ours(args, world, rank, local):
     result = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer (complex)", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": ("f32" if args.inner == "single" else "f16 storage / f32 arithmetic") + " inner, f64 outer (complex)",
+        "data": "synthetic",
         "config": {"workload": args.workload, "dims": list(W["dims"]), "kappa": kappa, "links": f"exp(i eps H), eps={W['eps']}",
-                   "source": "complex Gaussian", "solver": "GMRES(12), FP32 inner, FP64 defect correction, even-odd",
+                   "source": ("12 spin-colour point sources + 16 Z2 noise sources" if W.get("sources") else
+                              "complex Gaussian"),
+                   "solver": f"GMRES(12), {'FP32' if args.inner == 'single' else 'FP16'} inner, FP64 defect correction, "
+                             "even-odd, all rhs batched in one call",
                    "tol_true_rel": TOL, "rhs_per_gpu": nrhs, "parallelism": f"replicas x{world}",
-                   "l2": "working set (links 101 MB FP32 + 302 MB FP64, spinors) larger than L2"},
+                   "l2": "working set (links and spinors of the solve) larger than the 126 MB L2"},
         "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": launches,
         "iterations_per_solve": infos[0]["iterations"] if infos else None,
     }
@@ -393,6 +444,7 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--quick", action="store_true", help="skip the per-precision and FP64 side measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--inner", default="single", choices=["single", "half"], help="inner Krylov precision")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)

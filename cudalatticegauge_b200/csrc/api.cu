@@ -1,6 +1,7 @@
 // api.cu -- the C ABI (include/clg_b200.h): contexts, lattices, gauge and
 // fermion fields, operator application (CField::ApplyOperator,
 // Data/Field/CField.h:203) and field BLAS.
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -240,6 +241,8 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   clg_context_s* ctx = new clg_context_s();
   ctx->device = device;
   ctx->num_sms = prop.multiProcessorCount;
+  // CLG_AUTOTUNE=0 keeps the default block size (reproducible profiling runs)
+  if (const char* t = std::getenv("CLG_AUTOTUNE")) ctx->tuning_enabled = t[0] != '0';
   if (stream) {
     ctx->stream = (cudaStream_t)stream;
   } else {
@@ -312,6 +315,10 @@ clg_status clg_lattice_create(clg_context ctx, const int dims[4], const int bc[4
     lat->g.L[k] = dims[k];
     lat->g.bc[k] = bc ? (bc[k] < 0 ? -1 : 1) : (k == 3 ? -1 : 1);
     V *= dims[k];
+  }
+  if (V >= ((int64_t)1 << 31)) {
+    delete lat;
+    return ctx->fail(CLG_ERR_UNSUPPORTED, "lattice volume must be below 2^31 sites (32-bit site indices)");
   }
   lat->g.V = V;
   lat->g.Vh = V / 2;

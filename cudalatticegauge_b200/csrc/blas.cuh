@@ -97,7 +97,10 @@ clg_status launch_sites(clg_context_s* ctx, const F& f, int first_parity, int np
   const int bs = 256;
   const int64_t nsites = (int64_t)nparity * Vh;
   int64_t nb = (nsites + bs - 1) / bs;
-  const int64_t cap = (int64_t)ctx->num_sms * 8 / (nrhs > 0 ? nrhs : 1) + 1;
+  // wide reductions use fewer, longer-running blocks: each block's shuffle tree
+  // and its NRED partials are then amortised over more sites
+  const int64_t per_sm = NRED > 4 ? 2 : 8;
+  const int64_t cap = (int64_t)ctx->num_sms * per_sm / (nrhs > 0 ? nrhs : 1) + 1;
   if (NRED > 0 && nb > cap) nb = cap;
   if (nb > 65535 * 64) nb = 65535 * 64;
   if (NRED > 0) {

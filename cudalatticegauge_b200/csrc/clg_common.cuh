@@ -57,18 +57,23 @@ template <typename T> __device__ __forceinline__ cpx<T> mul_i(cpx<T> a, int b) {
 
 // ---------------------------------------------------------------- geometry
 // Coordinates of the checkerboard site (parity p, index h).
+// 32-bit index arithmetic: lattices are limited to V < 2^31 sites (checked when
+// the lattice is created), and 64-bit integer division is emulated on the GPU.
 __device__ __forceinline__ void eo_coords(const Geom& g, int p, int64_t h, int c[4]) {
-  const int64_t s0 = 2 * h;
-  const int t0 = (int)(s0 % g.L[3]);
-  int64_t r = s0 / g.L[3];
-  c[2] = (int)(r % g.L[2]);
-  r /= g.L[2];
-  c[1] = (int)(r % g.L[1]);
-  c[0] = (int)(r / g.L[1]);
+  const unsigned s0 = 2u * (unsigned)h;
+  const unsigned Lt = (unsigned)g.L[3], Lz = (unsigned)g.L[2], Ly = (unsigned)g.L[1];
+  unsigned r = s0 / Lt;
+  const int t0 = (int)(s0 - r * Lt);
+  unsigned q = r / Lz;
+  c[2] = (int)(r - q * Lz);
+  r = q / Ly;
+  c[1] = (int)(q - r * Ly);
+  c[0] = (int)r;
   c[3] = t0 + ((c[0] + c[1] + c[2] + p) & 1);
 }
 __device__ __forceinline__ int64_t site_index(const Geom& g, const int c[4]) {
-  return (((int64_t)c[0] * g.L[1] + c[1]) * g.L[2] + c[2]) * g.L[3] + c[3];
+  return (int64_t)((((unsigned)c[0] * (unsigned)g.L[1] + (unsigned)c[1]) * (unsigned)g.L[2] + (unsigned)c[2]) *
+                       (unsigned)g.L[3] + (unsigned)c[3]);
 }
 
 // ---------------------------------------------------------------- errors

@@ -15,8 +15,21 @@ bool idempotent(const HopArgs& a) { return a.x == nullptr || a.x != a.out; }
 
 template <int P, int RECON>
 cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
-  auto go = [&](int bs) {
-    dim3 grid((unsigned)((a.g.Vh + bs - 1) / bs), (unsigned)nrhs);
+  // config = block size | (register-capped variant << 16)
+  auto go = [&](int cfg) {
+    const int bs = cfg & 0xffff;
+    const bool capped = (cfg >> 16) != 0;
+    dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
+    if constexpr (P != P64) {
+      if (capped) {
+        if (dagger)
+          wilson_hop_kernel<P, RECON, true, 3><<<grid, bs, 0, ctx->stream>>>(a);
+        else
+          wilson_hop_kernel<P, RECON, false, 3><<<grid, bs, 0, ctx->stream>>>(a);
+        ctx->kernels++;
+        return cudaGetLastError();
+      }
+    }
     if (dagger)
       wilson_hop_kernel<P, RECON, true><<<grid, bs, 0, ctx->stream>>>(a);
     else
@@ -24,13 +37,16 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
     ctx->kernels++;
     return cudaGetLastError();
   };
-  return go(tune_block(ctx, key, idempotent(a), go));
+  std::vector<int> cand = {64, 128, 256, 512};
+  if (P != P64)
+    for (int bs : {64, 128, 256}) cand.push_back(bs | (1 << 16));
+  return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 
 template <int P, int RECON>
 cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
   auto go = [&](int bs) {
-    dim3 grid((unsigned)((a.g.Vh + bs - 1) / bs), (unsigned)nrhs);
+    dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
     staggered_hop_kernel<P, RECON><<<grid, bs, 0, ctx->stream>>>(a);
     ctx->kernels++;
     return cudaGetLastError();
@@ -143,6 +159,7 @@ clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
   a.scale_stride = s.scale_stride;
   a.skip_dev = s.skip_dev;
   a.skip_stride = s.skip_stride;
+  a.nrhs = s.nrhs > 0 ? s.nrhs : 1;
   const bool wilson = s.kind == CLG_FERMION_WILSON;
   std::string key = std::string(wilson ? "wilson" : "ks") + "_p" + std::to_string(s.prec) + "_d" +
                     std::to_string((int)s.dagger) + "_V" + std::to_string((long long)a.g.Vh) + "_n" +

@@ -44,6 +44,7 @@ struct HopArgs {
   int scale_stride;
   const int* skip_dev;      // optional: rhs with skip_dev[rhs * skip_stride] != 0 are not computed
   int skip_stride;
+  int nrhs;                 // right-hand sides (interleaved in blockIdx.x)
 };
 
 // chiral gamma tables (GammaMatrix.h:447-478): row r -> column perm[r] with phase i^z4[r]
@@ -91,24 +92,24 @@ __device__ __forceinline__ void wilson_hop_dir(cpx<AT> acc[12], const cpx<AT> ps
 }
 
 struct NbrInfo {
-  int64_t hf[4], hb[4];
-  float sf[4], sb[4];
+  int hf[4], hb[4];   // checkerboard index of x+mu, x-mu (V < 2^31)
+  float sf[4], sb[4]; // boundary signs
 };
 
 __device__ __forceinline__ void neighbours(const Geom& g, int p, int64_t h, NbrInfo& nb, int c[4]) {
   eo_coords(g, p, h, c);
-  const int64_t s = site_index(g, c);
-  int64_t st[4];
+  const int s = (int)site_index(g, c);
+  int st[4];
   st[3] = 1;
   st[2] = g.L[3];
-  st[1] = (int64_t)g.L[2] * g.L[3];
-  st[0] = (int64_t)g.L[1] * st[1];
+  st[1] = g.L[2] * g.L[3];
+  st[0] = g.L[1] * st[1];
 #pragma unroll
   for (int mu = 0; mu < 4; ++mu) {
-    int64_t sf = s + st[mu], sb = s - st[mu];
+    int sf = s + st[mu], sb = s - st[mu];
     float bf = 1.f, bb = 1.f;
-    if (c[mu] == g.L[mu] - 1) { sf -= (int64_t)g.L[mu] * st[mu]; bf = (float)g.bc[mu]; }
-    if (c[mu] == 0) { sb += (int64_t)g.L[mu] * st[mu]; bb = (float)g.bc[mu]; }
+    if (c[mu] == g.L[mu] - 1) { sf -= g.L[mu] * st[mu]; bf = (float)g.bc[mu]; }
+    if (c[mu] == 0) { sb += g.L[mu] * st[mu]; bb = (float)g.bc[mu]; }
     nb.hf[mu] = sf >> 1;
     nb.hb[mu] = sb >> 1;
     nb.sf[mu] = bf;
@@ -116,12 +117,17 @@ __device__ __forceinline__ void neighbours(const Geom& g, int p, int64_t h, NbrI
   }
 }
 
-template <int P, int RECON, bool DAGGER>
-__global__ void __launch_bounds__(256) wilson_hop_kernel(HopArgs a) {
+// MINB = 3 caps registers at 85 per thread (24 resident warps per SM instead
+// of 16): the hop is latency-bound on its gathers, and the low-precision
+// variants fit in 80 registers without spilling.  The autotuner picks.
+template <int P, int RECON, bool DAGGER, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
   using AT = typename AccT<P>::T;
   const int64_t Vh = a.g.Vh;
-  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
+  // right-hand sides are interleaved in blockIdx.x so that the CTAs of all rhs
+  // for the same sites run back to back and share the links through L2
+  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
+  const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
   if (h >= Vh) return;
   if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
@@ -178,8 +184,10 @@ template <int P, int RECON>
 __global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
   using AT = typename AccT<P>::T;
   const int64_t Vh = a.g.Vh;
-  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
+  // right-hand sides are interleaved in blockIdx.x so that the CTAs of all rhs
+  // for the same sites run back to back and share the links through L2
+  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
+  const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
   if (h >= Vh) return;
   if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;

@@ -130,16 +130,16 @@ clg_status ensure_reduction(clg_context_s* ctx, int64_t doubles);
 
 // ------------------------------------------------------------ launch helpers
 bool stream_capturing(cudaStream_t s);
-// Autotuner: the block size for kernel variant `key`.  On first use (outside
-// stream capture, when the launch is idempotent) each candidate block size is
+// Autotuner: the launch configuration for kernel variant `key`.  On first use
+// (outside stream capture, when the launch is idempotent) each candidate
+// (a block size, optionally combined with a register-capped kernel variant) is
 // timed with CUDA events on the context stream and the fastest is cached.
 template <class Go>
-int tune_block(clg_context_s* ctx, const std::string& key, bool can_repeat, Go&& go) {
+int tune_block(clg_context_s* ctx, const std::string& key, bool can_repeat, Go&& go,
+               const std::vector<int>& cand = {64, 128, 256, 512}, int fallback = 128) {
   auto it = ctx->tuned.find(key);
   if (it != ctx->tuned.end()) return it->second;
-  const int fallback = 128;
   if (!ctx->tuning_enabled || !can_repeat || stream_capturing(ctx->stream)) return fallback;
-  const int cand[4] = {64, 128, 256, 512};
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return fallback;
   if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return fallback; }

@@ -414,21 +414,20 @@ struct GmStart {
   }
 };
 
-// h_ij = s_i <V'_i, w>, i <= j
-template <int P, int NC>
-struct GmDots {
+// h_ij = s_i <V'_i, w>, i <= J: J+1 dot products (2(J+1) reductions) in one pass;
+// J is a template argument so the reduction width matches the column
+template <int P, int NC, int J>
+struct GmDotsJ {
   VList V;
   DField w;
   KState* st;
-  int j;
   __device__ bool active(int q) const { return !st[q].skip; }
   __device__ void operator()(int rhs, int par, int64_t h, double* acc) const {
     using AT = typename AccT<P>::T;
     cpx<AT> vw[NC];
     ldv<P, NC, AT>(w, rhs, par, h, vw);
 #pragma unroll
-    for (int i = 0; i < GM_MAXK; ++i) {
-      if (i > j) break;
+    for (int i = 0; i <= J; ++i) {
       cpx<AT> vi[NC];
       ldv<P, NC, AT>(V.v[i], rhs, par, h, vi);
       acc_dot<NC, AT>(vi, vw, acc + 2 * i);
@@ -438,7 +437,7 @@ struct GmDots {
     KState& k = st[q];
     if (k.skip) return;
     k.iters += 1;
-    for (int i = 0; i <= j; ++i) k.H[i * GM_MAXK + j] = make_double2(k.s[i] * s[2 * i], k.s[i] * s[2 * i + 1]);
+    for (int i = 0; i <= J; ++i) k.H[i * GM_MAXK + J] = make_double2(k.s[i] * s[2 * i], k.s[i] * s[2 * i + 1]);
   }
 };
 

@@ -364,6 +364,18 @@ clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& bo
   return CLG_SUCCESS;
 }
 
+// GMRES multi-dot of column j with a reduction exactly 2(j+1) wide
+template <int PV, int NV, int J>
+clg_status launch_gm_dots(clg_context_s* ctx, const VList& vl, const FieldRef& wv, KState* st, int j, int fp, int np,
+                          int64_t Vh, int nrhs) {
+  if constexpr (J < GM_MAXK) {
+    if (j == J) return launch_sites<2 * (J + 1)>(ctx, GmDotsJ<PV, NV, J>{vl, dfield(wv), st}, fp, np, Vh, nrhs);
+    return launch_gm_dots<PV, NV, J + 1>(ctx, vl, wv, st, j, fp, np, Vh, nrhs);
+  } else {
+    return ctx->fail(CLG_ERR_BAD_ARG, "GMRES column index out of range");
+  }
+}
+
 // ------------------------------------------------------------------ Krylov methods
 // Solve K x = b (precision P, the subset of b) for every rhs not marked in outer_done.
 clg_status krylov(Work& w, int op, const FieldRef& x, const FieldRef& b, int slot_base) {
@@ -459,7 +471,7 @@ clg_status krylov(Work& w, int op, const FieldRef& x, const FieldRef& b, int slo
         for (int j = 0; j < k; ++j) {
           if ((e2 = kapply(w, op, wv.ref, V[j].ref, &w.st[0].s[j], (int)(sizeof(KState) / sizeof(double)), skip, ks)))
             return e2;
-          if ((e2 = launch_sites<2 * GM_MAXK>(ctx, GmDots<PV, NV>{vl, dfield(wv.ref), w.st, j}, fp, np, Vh, nrhs))) return e2;
+          if ((e2 = launch_gm_dots<PV, NV, 0>(ctx, vl, wv.ref, w.st, j, fp, np, Vh, nrhs))) return e2;
           if ((e2 = launch_sites<1>(ctx, GmOrtho<PV, NV>{vl, dfield(wv.ref), w.st, j}, fp, np, Vh, nrhs))) return e2;
         }
         gm_solve_y<<<(nrhs + 63) / 64, 64, 0, ctx->stream>>>(w.st, nrhs);
