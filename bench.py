@@ -39,6 +39,13 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "wilson_eo_32x32x32x16"
 TOL = 1e-10
+SOLVER_NAMES = {"cg": "CGNE on the Schur system (CG on M_ee M_ee^+)", "gmres": "GMRES(12)"}
+
+
+def make_solver(clg, ctx, kind, inner):
+    if kind == "cg":
+        return clg.CSLASolverCG(ctx, inner_precision=inner, tol_true_rel=TOL)
+    return clg.CSLASolverGMRES(ctx, inner_precision=inner, tol_true_rel=TOL, MaxDim=12)
 
 
 def peaks():
@@ -226,7 +233,7 @@ def ours(args, world, rank, local):
             b.InitialField(clg.SOURCE_GAUSS, seed, 2 + r, rhs=r)
     x = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
     inner = {"single": clg.SINGLE, "half": clg.HALF}[args.inner]
-    mixed = clg.CSLASolverGMRES(ctx, inner_precision=inner, tol_true_rel=TOL, MaxDim=12)
+    mixed = make_solver(clg, ctx, args.solver, inner)
 
     def check(infos):
         for i in infos:
@@ -314,10 +321,12 @@ def ours(args, world, rank, local):
         plain = {}
         for label, cls, prec in (("fp64_gmres12", clg.CSLASolverGMRES, clg.DOUBLE),
                                  ("fp64_bicgstab", clg.CSLASolverBiCGStab, clg.DOUBLE),
+                                 ("fp64_cgne", clg.CSLASolverCG, clg.DOUBLE),
                                  ("mixed_gmres12", clg.CSLASolverGMRES, clg.SINGLE),
-                                 ("mixed_bicgstab", clg.CSLASolverBiCGStab, clg.SINGLE),
-                                 ("half_bicgstab", clg.CSLASolverBiCGStab, clg.HALF)):
-            s = cls(ctx, inner_precision=prec, tol_true_rel=TOL, MaxDim=12)
+                                 ("half_gmres12", clg.CSLASolverGMRES, clg.HALF),
+                                 ("mixed_cgne", clg.CSLASolverCG, clg.SINGLE),
+                                 ("half_cgne", clg.CSLASolverCG, clg.HALF)):
+            s = cls(ctx, inner_precision=prec, tol_true_rel=TOL, MaxDim=12, max_iterations=60000, max_outer=20)
             xs = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -340,8 +349,8 @@ def ours(args, world, rank, local):
         "config": {"workload": args.workload, "dims": list(W["dims"]), "kappa": kappa, "links": f"exp(i eps H), eps={W['eps']}",
                    "source": ("12 spin-colour point sources + 16 Z2 noise sources" if W.get("sources") else
                               "complex Gaussian"),
-                   "solver": f"GMRES(12), {'FP32' if args.inner == 'single' else 'FP16'} inner, FP64 defect correction, "
-                             "even-odd, all rhs batched in one call",
+                   "solver": f"{SOLVER_NAMES[args.solver]}, {'FP32' if args.inner == 'single' else 'FP16'} inner, "
+                             "FP64 defect correction, even-odd, all rhs batched in one call",
                    "tol_true_rel": TOL, "rhs_per_gpu": nrhs, "parallelism": f"replicas x{world}",
                    "l2": "working set (links and spinors of the solve) larger than the 126 MB L2"},
         "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": launches,
@@ -435,6 +444,36 @@ def reference(args, world, rank):
     print(json.dumps(out))
 
 
+def profile_driver(args):
+    """A small, fixed launch sequence for ncu captures (run it under
+    `CLG_AUTOTUNE=0` so the captured launches use the default configuration)."""
+    import cudalatticegauge_b200 as clg
+
+    W = WORKLOADS[args.workload]
+    ctx = clg.Context(0)
+    lat = clg.Lattice(ctx, W["dims"])
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, W["seed"], 1, W["eps"])
+    if args.profile.startswith("hop"):
+        prec = {"hop-double": clg.DOUBLE, "hop-single": clg.SINGLE, "hop-half": clg.HALF}[args.profile]
+        a = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], precision=prec)
+        a.InitialField(clg.SOURCE_GAUSS, 5, 2)
+        o = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], precision=prec)
+        for _ in range(args.steps):
+            a.apply_to(clg.OP_DEO, o, U)
+    else:
+        b = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=W["nrhs"])
+        for r in range(W["nrhs"]):
+            b.InitialField(clg.SOURCE_GAUSS, W["seed"], 2 + r, rhs=r)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=W["nrhs"])
+        inner = {"single": clg.SINGLE, "half": clg.HALF}[args.inner]
+        s = make_solver(clg, ctx, args.solver, inner)
+        for _ in range(args.steps):
+            print(s.Solve(x, b, U, clg.EFO_F_D)[0], flush=True)
+    ctx.synchronize()
+    print("profile driver done, kernels", ctx.kernel_count())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -445,7 +484,14 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the per-precision and FP64 side measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--inner", default="single", choices=["single", "half"], help="inner Krylov precision")
+    ap.add_argument("--solver", default="gmres", choices=["gmres", "cg"], help="inner Krylov method")
+    ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve"],
+                    help="profiling driver (no JSON line): `--steps` hop launches on the workload lattice, "
+                         "or `--steps` solves without warm-up")
     args = ap.parse_args()
+    if args.profile:
+        profile_driver(args)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)
     try:

@@ -280,6 +280,7 @@ template <int P, int NC>
 struct CgAlpha {
   DField p, q;
   KState* st;
+  int weight;  // operator applications per Krylov-operator application (2 for M M^+)
   __device__ bool active(int r) const { return !st[r].skip; }
   __device__ void operator()(int rhs, int par, int64_t h, double* acc) const {
     using AT = typename AccT<P>::T;
@@ -291,7 +292,7 @@ struct CgAlpha {
   __device__ void finalize(int r, const double* s) const {
     KState& k = st[r];
     if (k.skip) return;
-    k.iters += 1;
+    k.iters += weight;
     if (!(s[0] > 0.0) || bad(s[0])) {
       k.status = ST_BREAKDOWN;
       k.done = k.skip = 1;

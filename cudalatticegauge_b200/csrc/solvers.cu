@@ -200,7 +200,14 @@ struct Owned {
   }
 };
 
-bool hermitian_op(int op) { return op == CLG_OP_DDDAG || op == CLG_OP_DDDAG_EE || op == CLG_OP_MEE_MEEDAG; }
+// internal Krylov operator M_ee^+ M_ee (CGNR for D^+ solves); not part of the C ABI
+constexpr int OP_MEEDAG_MEE = 100;
+
+bool hermitian_op(int op) {
+  return op == CLG_OP_DDDAG || op == CLG_OP_DDDAG_EE || op == CLG_OP_MEE_MEEDAG || op == OP_MEEDAG_MEE;
+}
+// operator applications one Krylov-operator application stands for
+int op_weight(int op) { return (op == CLG_OP_MEE_MEEDAG || op == OP_MEEDAG_MEE || op == CLG_OP_DDDAG) ? 2 : 1; }
 
 }  // namespace
 
@@ -278,12 +285,13 @@ clg_status read_summary(Work& w) {
 clg_status kapply_base(Work& w, int op, const FieldRef& out, const FieldRef& in, const double* scale, int sstride,
                        const int* skip, int kstride) {
   const double2 one = make_double2(1, 0);
-  if (op == CLG_OP_MEE_MEEDAG) {
-    clg_status s = apply_op(w.ctx, CLG_OP_MEE_DAG, w.U, w.kind, w.param, w.kt_even.ref, in, &w.kt_odd.ref, one, w.nrhs,
-                            nullptr, 0, skip, kstride);
+  if (op == CLG_OP_MEE_MEEDAG || op == OP_MEEDAG_MEE) {
+    const bool mdag_first = op == CLG_OP_MEE_MEEDAG;  // M (M^+ in)  or  M^+ (M in)
+    clg_status s = apply_op(w.ctx, mdag_first ? CLG_OP_MEE_DAG : CLG_OP_MEE, w.U, w.kind, w.param, w.kt_even.ref, in,
+                            &w.kt_odd.ref, one, w.nrhs, nullptr, 0, skip, kstride);
     if (s) return s;
-    return apply_op(w.ctx, CLG_OP_MEE, w.U, w.kind, w.param, out, w.kt_even.ref, &w.kt_odd.ref, one, w.nrhs, scale,
-                    sstride, skip, kstride);
+    return apply_op(w.ctx, mdag_first ? CLG_OP_MEE : CLG_OP_MEE_DAG, w.U, w.kind, w.param, out, w.kt_even.ref,
+                    &w.kt_odd.ref, one, w.nrhs, scale, sstride, skip, kstride);
   }
   const FieldRef* tmp = (op == CLG_OP_DDDAG || op == CLG_OP_DD) ? &w.kt_full.ref : &w.kt_odd.ref;
   return apply_op(w.ctx, op, w.U, w.kind, w.param, out, in, tmp, one, w.nrhs, scale, sstride, skip, kstride);
@@ -433,7 +441,8 @@ clg_status krylov(Work& w, int op, const FieldRef& x, const FieldRef& b, int slo
       auto body = [&]() -> clg_status {
         clg_status e2;
         if ((e2 = kapply(w, op, q.ref, p.ref, nullptr, 0, skip, ks))) return e2;
-        if ((e2 = launch_sites<2>(ctx, CgAlpha<PV, NV>{dfield(p.ref), dfield(q.ref), w.st}, fp, np, Vh, nrhs))) return e2;
+        CgAlpha<PV, NV> ca{dfield(p.ref), dfield(q.ref), w.st, op_weight(op)};
+        if ((e2 = launch_sites<2>(ctx, ca, fp, np, Vh, nrhs))) return e2;
         CgUpdate<PV, NV> up{dfield(x), dfield(r.ref), dfield(p.ref), dfield(q.ref), w.st};
         if ((e2 = launch_sites<1>(ctx, up, fp, np, Vh, nrhs))) return e2;
         return launch_sites<0>(ctx, CgP<PV, NV>{dfield(p.ref), dfield(r.ref), w.st}, fp, np, Vh, nrhs);
@@ -639,14 +648,18 @@ clg_status clg::solve_core(const SolveReq& q) {
     return s;
   if ((s = t64.alloc(ctx, 0, nc, full ? 2 : 1, full ? 0 : 1, nrhs, Vh))) return s;
   // inner-precision vectors
-  Owned rP, eP, yP, bS;
+  // CG on a Wilson D / D^+ solve: the Schur system through its normal equations
+  // (CGNE: M M^+ y = b, x = M^+ y; CGNR for D^+: M^+ M y = b, x = M y)
+  const bool cgne = schur && wilson && prm->kind == CLG_SOLVER_CG;
+  Owned rP, eP, yP, bS, yS;
   if ((s = rP.alloc(ctx, w.P, nc, npar, 0, nrhs, Vh)) || (s = eP.alloc(ctx, w.P, nc, npar, 0, nrhs, Vh))) return s;
   if (schur) {
     if ((s = bS.alloc(ctx, w.P, nc, 1, 0, nrhs, Vh))) return s;
     if (op == CLG_OP_DDDAG && (s = yP.alloc(ctx, w.P, nc, 2, 0, nrhs, Vh))) return s;
+    if (cgne && (s = yS.alloc(ctx, w.P, nc, 1, 0, nrhs, Vh))) return s;
   }
   if ((s = w.kt_odd.alloc(ctx, w.P, nc, 1, 1, nrhs, Vh))) return s;
-  if (op == CLG_OP_MEE_MEEDAG && (s = w.kt_even.alloc(ctx, w.P, nc, 1, 0, nrhs, Vh))) return s;
+  if ((op == CLG_OP_MEE_MEEDAG || cgne) && (s = w.kt_even.alloc(ctx, w.P, nc, 1, 0, nrhs, Vh))) return s;
   if (!schur && op == CLG_OP_DDDAG && (s = w.kt_full.alloc(ctx, w.P, nc, 2, 0, nrhs, Vh))) return s;
 
   // b64 = B, x64 = X0 or 0
@@ -757,7 +770,15 @@ clg_status clg::solve_core(const SolveReq& q) {
       h1.skip_stride = 1;
       h1.nrhs = nrhs;
       if ((q = hop(ctx, U, h1))) return q;
-      if ((q = krylov(w, dag ? kop_ddag : kop_d, sol_e, bS.ref, dag ? 10 : 0))) return q;
+      if (cgne) {
+        // M M^+ y = bS, sol_e = M^+ y   (D^+: M^+ M y = bS, sol_e = M y)
+        if ((q = krylov(w, dag ? OP_MEEDAG_MEE : CLG_OP_MEE_MEEDAG, yS.ref, bS.ref, dag ? 10 : 0))) return q;
+        if ((q = apply_op(ctx, dag ? CLG_OP_MEE : CLG_OP_MEE_DAG, U, w.kind, w.param, sol_e, yS.ref, &w.kt_odd.ref, one,
+                          nrhs, nullptr, 0, w.outer_done_d, 1)))
+          return q;
+      } else if ((q = krylov(w, dag ? kop_ddag : kop_d, sol_e, bS.ref, dag ? 10 : 0))) {
+        return q;
+      }
       // sol_o = rhs_o + kappa H_oe sol_e (Wilson) ; (rhs_o -/+ H_oe sol_e) / m (staggered)
       HopSpec h2 = h1;
       h2.out_parity = 1;

@@ -112,6 +112,21 @@ def test_multi_rhs_batch(ctx, clg, oracle):
         assert op.true_residual(b.to_numpy(r), x.to_numpy(r)) <= TOL
 
 
+@pytest.mark.parametrize("op,name", [(0, "WILSON_D"), (1, "WILSON_DDAG")])
+@pytest.mark.parametrize("prec", [1, 2])
+def test_wilson_cg_normal_equations(ctx, clg, oracle, op, name, prec):
+    """CG on a Wilson D (D^+) solve runs CGNE (CGNR) on the even-odd Schur system."""
+    lat = clg.Lattice(ctx, (8, 8, 8, 16))
+    U = gauge(clg, lat, "expH", 0xC1A60001)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    b.InitialField(clg.SOURCE_GAUSS, 6, 2)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    info = clg.CSLASolverCG(ctx, inner_precision=prec).Solve(x, b, U, op)[0]
+    o = oracle.Operator(name, lat.dims, U.CopyDataOut(), KAPPA)
+    assert info["status"] == 0
+    assert o.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
+
+
 def test_staggered_cg(ctx, clg, oracle):
     """Staggered D x = b through CG on (DD^+)_ee, and DD^+ x = b."""
     lat = clg.Lattice(ctx, (8, 8, 8, 8))
