@@ -100,6 +100,10 @@ __device__ __forceinline__ void store_site(void* __restrict__ base, float* __res
     float m = 0.f;
 #pragma unroll
     for (int k = 0; k < NC; ++k) m = fmaxf(m, fmaxf(fabsf((float)v[k].x), fabsf((float)v[k].y)));
+    // a site whose largest component is below 1e-30 is stored as exact zero:
+    // 1/m of a float denormal overflows to inf and would turn the site into NaN
+    // (point sources produce such sites after a few hops)
+    if (!(m > 1e-30f)) m = 0.f;
     const float inv = m > 0.f ? 1.0f / m : 0.f;
     nrm[h] = m;
     if constexpr (NC % 4 == 0) {

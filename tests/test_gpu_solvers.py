@@ -127,6 +127,25 @@ def test_wilson_cg_normal_equations(ctx, clg, oracle, op, name, prec):
     assert o.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
 
 
+def test_half_precision_point_source(ctx, clg, oracle):
+    """A point source makes sites with tiny (float-denormal) maxima after a few
+    hops; the FP16 per-site-norm storage must flush them instead of producing NaN."""
+    lat = clg.Lattice(ctx, (8, 8, 8, 32))
+    U = gauge(clg, lat, "expH", 0xC1A60003)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    b.InitialAsSource(lat.volume // 2 + 3, 0)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
+    info = clg.CSLASolverCG(ctx, inner_precision=clg.HALF).Solve(x, b, U, clg.EFO_F_D)[0]
+    o = oracle.Operator("WILSON_D", lat.dims, U.CopyDataOut(), KAPPA)
+    assert info["status"] == 0
+    assert o.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
+    e = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF)
+    e.InitialAsSource(0, 0)
+    for _ in range(6):
+        e.ApplyOperator(clg.OP_MEE_MEEDAG, U)
+    assert np.isfinite(e.to_numpy()).all()
+
+
 def test_staggered_cg(ctx, clg, oracle):
     """Staggered D x = b through CG on (DD^+)_ee, and DD^+ x = b."""
     lat = clg.Lattice(ctx, (8, 8, 8, 8))
