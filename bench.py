@@ -328,16 +328,22 @@ def ours(args, world, rank, local):
                                  ("half_cgne", clg.CSLASolverCG, clg.HALF)):
             s = cls(ctx, inner_precision=prec, tol_true_rel=TOL, MaxDim=12, max_iterations=60000, max_outer=20)
             xs = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            inf = s.Solve(xs, b1, U, clg.EFO_F_D, raise_on_fail=False)[0]
-            dt = time.perf_counter() - t0
+            inf = s.Solve(xs, b1, U, clg.EFO_F_D, raise_on_fail=False)[0]  # warm-up (tuning, graph capture)
+            if inf["status"] == 0:  # time a second solve when the first converged
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                inf = s.Solve(xs, b1, U, clg.EFO_F_D, raise_on_fail=False)[0]
+                dt = time.perf_counter() - t0
+            else:
+                dt = inf["seconds"]
             plain[label] = {"solves_per_s": round(1.0 / dt, 3), "seconds": round(dt, 4),
                             "applications": inf["iterations"], "outer": inf["outer"],
                             "true_rel_residual": inf["true_rel_residual"], "status": inf["status"]}
             s.close()
             xs.close()
         extra["solves"] = plain
+        if args.workload == DEFAULT_WORKLOAD and not args.no_batched:
+            extra["batched_config4"] = batched_config4(clg, ctx, stream, args)
         if world == 1 and not args.no_cpu:
             extra["cpu_baseline"] = cpu_baseline(U, lat, kappa, plain["fp64_gmres12"]["applications"])
     result = {
@@ -362,6 +368,58 @@ def ours(args, world, rank, local):
     if rank == 0:
         print(json.dumps(result))
     ctx.close()
+
+
+def batched_config4(clg, ctx, stream, args, steps=2):
+    """BASELINE config 4 measured beside the headline: 32^3x32, 12 spin-colour point
+    sources + 16 Z2 noise sources solved in one batched call (FP32-inner CGNE in
+    FP64 defect correction), against one FP64 CGNE solve of a single source."""
+    import torch
+
+    W = WORKLOADS["wilson_eo_batched_32x32x32x32"]
+    lat = clg.Lattice(ctx, W["dims"])
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, W["seed"], 1, W["eps"])
+    n = W["nrhs"]
+    b = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=n)
+    for r in range(12):
+        b.InitialAsSource(0, r, rhs=r)
+    for r in range(12, n):
+        b.InitialField(clg.SOURCE_Z2, W["seed"], 2 + r, rhs=r)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=n)
+    s = clg.CSLASolverCG(ctx, inner_precision=clg.SINGLE, tol_true_rel=TOL)
+    s.Solve(x, b, U, clg.EFO_F_D)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        infos = s.Solve(x, b, U, clg.EFO_F_D)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / steps
+    worst = max(i["true_rel_residual"] for i in infos)
+    b1 = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"])
+    b1.InitialField(clg.SOURCE_Z2, W["seed"], 2 + n - 1)
+    x1 = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"])
+    s64 = clg.CSLASolverCG(ctx, inner_precision=clg.DOUBLE, tol_true_rel=TOL)
+    s64.Solve(x1, b1, U, clg.EFO_F_D)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    i64 = s64.Solve(x1, b1, U, clg.EFO_F_D)[0]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t64 = e0.elapsed_time(e1) / 1e3
+    out = {"dims": list(W["dims"]), "rhs": n, "solver": "CGNE, FP32 inner, FP64 defect correction, batched",
+           "solves_per_s": round(n / t, 3), "ms_per_batch": round(t * 1e3, 2),
+           "max_applications": max(i["iterations"] for i in infos), "worst_true_rel_residual": worst,
+           "fp64_single_rhs_cgne_solves_per_s": round(1.0 / t64, 3), "fp64_single_rhs_applications": i64["iterations"],
+           "ratio_batched_mixed_vs_fp64": round(n / t * t64, 2)}
+    for f in (b, x, b1, x1):
+        f.close()
+    s.close()
+    s64.close()
+    U.close()
+    return out
 
 
 def cpu_baseline(U, lat, kappa, fp64_applications):
@@ -484,7 +542,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the per-precision and FP64 side measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--inner", default="single", choices=["single", "half"], help="inner Krylov precision")
-    ap.add_argument("--solver", default="gmres", choices=["gmres", "cg"], help="inner Krylov method")
+    ap.add_argument("--solver", default="cg", choices=["gmres", "cg"], help="inner Krylov method")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched config-4 side measurement")
     ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve"],
                     help="profiling driver (no JSON line): `--steps` hop launches on the workload lattice, "
                          "or `--steps` solves without warm-up")

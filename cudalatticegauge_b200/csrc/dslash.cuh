@@ -144,6 +144,31 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
   // D: forward (1 - g), backward (1 + g); D^+: swapped
   constexpr int SF = DAGGER ? 1 : -1;
   constexpr int SB = -SF;
+  if constexpr (P == P16) {
+    // FP16: both neighbours' packed data (19 registers each) are loaded before
+    // either is unpacked, so twice the bytes are in flight per thread
+#define CLG_WILSON_DIR16(MU)                                                            \
+  {                                                                                     \
+    Packed16 pf, pb;                                                                    \
+    PackedLink16 lf, lb;                                                                \
+    load_packed16(in, in_norm, Vh, nb.hf[MU], pf);                                      \
+    load_packed_link16(a.U_here, MU, Vh, h, lf);                                        \
+    load_packed16(in, in_norm, Vh, nb.hb[MU], pb);                                      \
+    load_packed_link16(a.U_there, MU, Vh, nb.hb[MU], lb);                               \
+    cpx<AT> psi[12], u[9];                                                              \
+    unpack16(pf, psi);                                                                  \
+    unpack_link16(lf, u);                                                               \
+    wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (AT)nb.sf[MU]);                      \
+    unpack16(pb, psi);                                                                  \
+    unpack_link16(lb, u);                                                               \
+    wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU]);                       \
+  }
+    CLG_WILSON_DIR16(0)
+    CLG_WILSON_DIR16(1)
+    CLG_WILSON_DIR16(2)
+    CLG_WILSON_DIR16(3)
+#undef CLG_WILSON_DIR16
+  } else {
 #define CLG_WILSON_DIR(MU)                                                              \
   {                                                                                     \
     cpx<AT> psi[12], u[9];                                                              \
@@ -154,11 +179,12 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
     load_link<P, RECON, AT>(a.U_there, MU, Vh, nb.hb[MU], u);                           \
     wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU]);                       \
   }
-  CLG_WILSON_DIR(0)
-  CLG_WILSON_DIR(1)
-  CLG_WILSON_DIR(2)
-  CLG_WILSON_DIR(3)
+    CLG_WILSON_DIR(0)
+    CLG_WILSON_DIR(1)
+    CLG_WILSON_DIR(2)
+    CLG_WILSON_DIR(3)
 #undef CLG_WILSON_DIR
+  }
 
   const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
 #pragma unroll

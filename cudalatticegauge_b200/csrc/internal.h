@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -198,9 +199,16 @@ clg_status blas_copy(clg_context_s* ctx, const FieldRef& dst, const FieldRef& sr
 clg_status blas_zero(clg_context_s* ctx, const FieldRef& y);
 
 // ------------------------------------------------------------ solves (solvers.cu)
+// Workspace a solver keeps between calls (buffers, pinned host memory, captured
+// CUDA graphs); rebuilt when the shape of the solve changes.
+struct SolveCacheBase {
+  virtual ~SolveCacheBase() {}
+};
+
 // One batched solve of (op + shift_r) x_r = b_r, r < nrhs, to prm->tol_true_rel
 // through the FP64 defect-correction loop.
 struct SolveReq {
+  std::unique_ptr<SolveCacheBase>* cache = nullptr;  // solver-owned workspace slot (nullable)
   clg_context_s* ctx = nullptr;
   const clg_solver_params* prm = nullptr;
   clg_gauge_s* U = nullptr;
@@ -224,4 +232,6 @@ clg_status solve_core(const SolveReq& q);
 struct clg_solver_s {
   clg_context_s* ctx = nullptr;
   clg_solver_params p;
+  std::unique_ptr<clg::SolveCacheBase> cache;        // single-shift solves
+  std::unique_ptr<clg::SolveCacheBase> cache_shift;  // multi-shift refinement
 };

@@ -374,6 +374,7 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
     prm.kind = hermitian ? CLG_SOLVER_CG : CLG_SOLVER_GMRES;
   }
   SolveReq q;
+  q.cache = &S->cache_shift;
   q.ctx = ctx;
   q.prm = &prm;
   q.U = g;

@@ -177,7 +177,9 @@ struct Owned {
     dfree(data);
     dfree(norm);
   }
+  // allocates once; a cached workspace calls it again with the same shape
   clg_status alloc(clg_context_s* ctx, int prec, int nc, int nparity, int first_parity, int nrhs, int64_t Vh) {
+    if (data) return CLG_SUCCESS;
     const int64_t blk = Vh * site_bytes_of(prec, nc);
     clg_status st = dalloc(ctx, &data, (size_t)blk * nparity * nrhs);
     if (st) return st;
@@ -218,13 +220,16 @@ using namespace clg;
 namespace {
 
 // Everything one solve needs, allocated per call.
-struct Work {
+struct Work : public SolveCacheBase {
+  std::string key;  // shape of the solve this workspace was built for
   clg_context_s* ctx;
   clg_gauge_s* U;
   int kind, op, P, nc, nrhs;
   double param;
   int64_t Vh;
   const clg_solver_params* prm;
+  // FP64 outer vectors and inner-precision Schur vectors (allocated on first use)
+  Owned x64, b64, r64, t64, tf, te, rP, eP, yP, bS, yS;
   // device state
   KState* st = nullptr;
   Summary* sum_d = nullptr;
@@ -563,6 +568,7 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
   if (S->p.kind == CLG_SOLVER_CGM || S->p.kind == CLG_SOLVER_FOM_MS)
     return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift solvers are called through clg_solve_multishift");
   SolveReq q;
+  q.cache = &S->cache;
   q.ctx = ctx;
   q.prm = &S->p;
   q.U = U;
@@ -603,12 +609,41 @@ clg_status clg::solve_core(const SolveReq& q) {
   if (q.shifts && (op == CLG_OP_D || op == CLG_OP_DDAG) && q.prm->kind == CLG_SOLVER_CG)
     return ctx->fail(CLG_ERR_BAD_ARG, "CG needs a Hermitian operator");
 
-  Work w;
+  clg_status s = CLG_SUCCESS;
+  const int P = q.prm->inner_precision;
+  if ((s = gauge_prepare(U, P))) return s;
+  // The workspace (buffers, pinned memory, captured graphs) lives in the solver
+  // and is reused while the shape of the solve and the gauge arrays stay the same.
+  const std::string key =
+      std::to_string((uintptr_t)q.lat) + "/" + std::to_string(q.kind) + "/" + std::to_string(q.subset) + "/" +
+      std::to_string(q.nrhs) + "/" + std::to_string(op) + "/" + std::to_string(P) + "/" + std::to_string(q.prm->kind) +
+      "/" + std::to_string(q.prm->max_dim) + "/" + std::to_string(q.prm->even_odd) + "/" +
+      std::to_string(q.prm->use_graphs) + "/" + std::to_string((uintptr_t)U) + "/" +
+      std::to_string((uintptr_t)U->u64[0]) + "/" + std::to_string((uintptr_t)U->u32[0]) + "/" +
+      std::to_string((uintptr_t)U->u16[0]) + "/" + std::to_string(q.shifts != nullptr) + "/" +
+      std::to_string(q.b_broadcast) + "/" + std::to_string(q.param);
+  std::unique_ptr<Work> local;
+  Work* wp = nullptr;
+  if (q.cache) {
+    Work* cw = dynamic_cast<Work*>(q.cache->get());
+    if (!cw || cw->key != key) {
+      cudaStreamSynchronize(ctx->stream);
+      q.cache->reset();
+      cw = new Work();
+      q.cache->reset(cw);
+    }
+    wp = cw;
+  } else {
+    local.reset(new Work());
+    wp = local.get();
+  }
+  Work& w = *wp;
+  w.key = key;
   w.ctx = ctx;
   w.U = U;
   w.kind = q.kind;
   w.op = op;
-  w.P = q.prm->inner_precision;
+  w.P = P;
   w.nc = q.kind == CLG_FERMION_WILSON ? 12 : 3;
   w.nrhs = q.nrhs;
   w.param = q.param;
@@ -616,23 +651,27 @@ clg_status clg::solve_core(const SolveReq& q) {
   w.prm = q.prm;
   const int nrhs = w.nrhs;
   const clg_solver_params* prm = q.prm;
-  clg_status s = CLG_SUCCESS;
-  if ((s = gauge_prepare(U, w.P))) return s;
-  if ((s = dalloc(ctx, (void**)&w.st, sizeof(KState) * nrhs)) || (s = dalloc(ctx, (void**)&w.sum_d, sizeof(Summary) * nrhs)) ||
-      (s = dalloc(ctx, (void**)&w.outer_done_d, sizeof(int) * nrhs)) ||
-      (s = dalloc(ctx, (void**)&w.tol_d, sizeof(double) * nrhs)) || (s = dalloc(ctx, (void**)&w.red_d, sizeof(double) * 2 * nrhs)))
-    return s;
-  if (cudaMallocHost((void**)&w.sum_h, sizeof(Summary) * nrhs) != cudaSuccess ||
-      cudaMallocHost((void**)&w.host_buf, sizeof(double) * 4 * nrhs + 64) != cudaSuccess)
-    return ctx->fail(CLG_ERR_OOM, "pinned host buffer");
+  if (!w.st) {
+    if ((s = dalloc(ctx, (void**)&w.st, sizeof(KState) * nrhs)) ||
+        (s = dalloc(ctx, (void**)&w.sum_d, sizeof(Summary) * nrhs)) ||
+        (s = dalloc(ctx, (void**)&w.outer_done_d, sizeof(int) * nrhs)) ||
+        (s = dalloc(ctx, (void**)&w.tol_d, sizeof(double) * nrhs)) ||
+        (s = dalloc(ctx, (void**)&w.red_d, sizeof(double) * 2 * nrhs)))
+      return s;
+    if (cudaMallocHost((void**)&w.sum_h, sizeof(Summary) * nrhs) != cudaSuccess ||
+        cudaMallocHost((void**)&w.host_buf, sizeof(double) * 4 * nrhs + 64) != cudaSuccess)
+      return ctx->fail(CLG_ERR_OOM, "pinned host buffer");
+  }
   cudaMemsetAsync(w.st, 0, sizeof(KState) * nrhs, ctx->stream);
 
   // Schur (even-odd) path for D / D^+ on full fields; Wilson DD^+ = two Schur solves
   const bool schur =
       full && prm->even_odd && !q.shifts && (op == CLG_OP_D || op == CLG_OP_DDAG || (op == CLG_OP_DDDAG && wilson));
   if (q.shifts) {
-    if ((s = dalloc(ctx, (void**)&w.shift_dev, sizeof(double2) * nrhs))) return s;
-    if (cudaMemcpy(w.shift_dev, q.shifts, sizeof(double2) * nrhs, cudaMemcpyHostToDevice) != cudaSuccess)
+    if (!w.shift_dev && (s = dalloc(ctx, (void**)&w.shift_dev, sizeof(double2) * nrhs))) return s;
+    if (cudaMemcpyAsync(w.shift_dev, q.shifts, sizeof(double2) * nrhs, cudaMemcpyHostToDevice, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
       return ctx->fail(CLG_ERR_CUDA, "solve: shifts upload");
   }
   const int kop_d = wilson ? CLG_OP_MEE : CLG_OP_DDDAG_EE;
@@ -641,7 +680,7 @@ clg_status clg::solve_core(const SolveReq& q) {
   const int nc = w.nc;
 
   // FP64 outer vectors
-  Owned x64, b64, r64, t64;
+  Owned &x64 = w.x64, &b64 = w.b64, &r64 = w.r64, &t64 = w.t64;
   const int npar = full ? 2 : 1;
   if ((s = x64.alloc(ctx, 0, nc, npar, 0, nrhs, Vh)) || (s = b64.alloc(ctx, 0, nc, npar, 0, nrhs, Vh)) ||
       (s = r64.alloc(ctx, 0, nc, npar, 0, nrhs, Vh)))
@@ -651,7 +690,7 @@ clg_status clg::solve_core(const SolveReq& q) {
   // CG on a Wilson D / D^+ solve: the Schur system through its normal equations
   // (CGNE: M M^+ y = b, x = M^+ y; CGNR for D^+: M^+ M y = b, x = M y)
   const bool cgne = schur && wilson && prm->kind == CLG_SOLVER_CG;
-  Owned rP, eP, yP, bS, yS;
+  Owned &rP = w.rP, &eP = w.eP, &yP = w.yP, &bS = w.bS, &yS = w.yS;
   if ((s = rP.alloc(ctx, w.P, nc, npar, 0, nrhs, Vh)) || (s = eP.alloc(ctx, w.P, nc, npar, 0, nrhs, Vh))) return s;
   if (schur) {
     if ((s = bS.alloc(ctx, w.P, nc, 1, 0, nrhs, Vh))) return s;
@@ -690,13 +729,13 @@ clg_status clg::solve_core(const SolveReq& q) {
   for (;; ++outer) {
     // r = b - A x  (FP64, true residual)
     const FieldRef* tmp = (op == CLG_OP_DDDAG) ? nullptr : &t64.ref;
-    Owned tf;
+    Owned& tf = w.tf;
     if (op == CLG_OP_DDDAG) {
       if ((s = tf.alloc(ctx, 0, nc, 2, 0, nrhs, Vh))) return s;
       tmp = &tf.ref;
     }
     if (op == CLG_OP_MEE_MEEDAG) {
-      Owned te;
+      Owned& te = w.te;
       if ((s = te.alloc(ctx, 0, nc, 1, 0, nrhs, Vh))) return s;
       if ((s = apply_op(ctx, CLG_OP_MEE_DAG, U, w.kind, w.param, te.ref, x64.ref, &t64.ref, one, nrhs))) return s;
       if ((s = apply_op(ctx, CLG_OP_MEE, U, w.kind, w.param, r64.ref, te.ref, &t64.ref, one, nrhs))) return s;
