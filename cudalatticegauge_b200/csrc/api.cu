@@ -41,6 +41,22 @@ void dfree(void* p) {
   if (p) cudaFree(p);
 }
 
+static clg_status staging_buffer(clg_context_s* ctx, size_t bytes, double** p) {
+  if (bytes > ctx->staging_bytes) {
+    if (ctx->staging) {
+      cudaStreamSynchronize(ctx->stream);
+      dfree(ctx->staging);
+      ctx->staging = nullptr;
+      ctx->staging_bytes = 0;
+    }
+    clg_status st = dalloc(ctx, &ctx->staging, bytes);
+    if (st) return st;
+    ctx->staging_bytes = bytes;
+  }
+  *p = static_cast<double*>(ctx->staging);
+  return CLG_SUCCESS;
+}
+
 clg_status ensure_reduction(clg_context_s* ctx, int64_t doubles) {
   if (doubles <= ctx->red_capacity) return CLG_SUCCESS;
   if (stream_capturing(ctx->stream))
@@ -205,6 +221,13 @@ clg_status sync_status(clg_context_s* ctx) {
   return CLG_SUCCESS;
 }
 
+// errors of the launches issued so far, without waiting for them
+clg_status launch_status(clg_context_s* ctx) {
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) return ctx->fail(cuda_status(e), cudaGetErrorString(e));
+  return CLG_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" {
@@ -268,6 +291,7 @@ clg_status clg_context_destroy(clg_context ctx) {
   cudaStreamSynchronize(ctx->stream);
   dfree(ctx->red_partials);
   dfree(ctx->red_counter);
+  dfree(ctx->staging);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return CLG_SUCCESS;
@@ -486,16 +510,14 @@ clg_status clg_field_import(clg_field f, int rhs, const double* data, int on_dev
   if (on_device) {
     buf = const_cast<double*>(data);
   } else {
-    st = dalloc(ctx, (void**)&buf, bytes);
+    st = staging_buffer(ctx, bytes, &buf);
     if (st) return st;
     cudaError_t e = cudaMemcpyAsync(buf, data, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) st = ctx->fail(cuda_status(e), cudaGetErrorString(e));
   }
   if (!st) st = field_reorder(f, rhs, buf, 1);
-  if (!on_device) {
-    if (!st) st = sync_status(ctx);
-    dfree(buf);
-  }
+  // the caller may reuse or free its buffer once this returns
+  if (!st) st = sync_status(ctx);
   return st;
 }
 
@@ -508,18 +530,16 @@ clg_status clg_field_export(clg_field f, int rhs, double* data, int on_device) {
   if (on_device) {
     buf = data;
   } else {
-    st = dalloc(ctx, (void**)&buf, bytes);
+    st = staging_buffer(ctx, bytes, &buf);
     if (st) return st;
   }
   st = field_reorder(f, rhs, buf, 0);
-  if (!on_device) {
-    if (!st) {
-      cudaError_t e = cudaMemcpyAsync(data, buf, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-      if (e != cudaSuccess) st = ctx->fail(cuda_status(e), cudaGetErrorString(e));
-    }
-    if (!st) st = sync_status(ctx);
-    dfree(buf);
+  if (!on_device && !st) {
+    cudaError_t e = cudaMemcpyAsync(data, buf, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) st = ctx->fail(cuda_status(e), cudaGetErrorString(e));
   }
+  // the data is complete (and readable from any stream) once this returns
+  if (!st) st = sync_status(ctx);
   return st;
 }
 
@@ -607,7 +627,10 @@ clg_status clg_apply_to(int op, clg_field out, clg_field in, clg_gauge g, int co
       st = apply_op(ctx, op, g, in->kind, in->param, o, i, nullptr, coeff, in->nrhs);
     }
   }
-  if (!st) st = sync_status(ctx);
+  // Operators that needed scratch fields wait for their kernels before the
+  // scratch is released; the others return once launched, like any stream
+  // operation, and can be captured into a CUDA graph.
+  if (!st) st = (t1.data || t2.data) ? sync_status(ctx) : launch_status(ctx);
   free_scratch(t1);
   free_scratch(t2);
   return st;

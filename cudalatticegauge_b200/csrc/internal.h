@@ -67,6 +67,11 @@ struct clg_context_s {
   double* red_partials = nullptr;
   int64_t red_capacity = 0;  // doubles
   unsigned int* red_counter = nullptr;
+  // device staging buffer of host field imports/exports (grow-only; one FP64
+  // lexicographic field).  Kept across calls so that a host round trip costs
+  // two copies and a reorder, not a cudaMalloc/cudaFree pair.
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
   // block size chosen per kernel variant by the autotuner
   std::map<std::string, int> tuned;
   bool tuning_enabled = true;
