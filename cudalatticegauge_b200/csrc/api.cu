@@ -1,6 +1,7 @@
 // api.cu -- the C ABI (include/clg_b200.h): contexts, lattices, gauge and
 // fermion fields, operator application (CField::ApplyOperator,
 // Data/Field/CField.h:203) and field BLAS.
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -266,6 +267,12 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   ctx->num_sms = prop.multiProcessorCount;
   // CLG_AUTOTUNE=0 keeps the default block size (reproducible profiling runs)
   if (const char* t = std::getenv("CLG_AUTOTUNE")) ctx->tuning_enabled = t[0] != '0';
+  if (const char* t = std::getenv("CLG_HOP_CONFIG")) {
+    int variant = -1, bs = 0;
+    if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && variant >= 0 && variant <= 1 &&
+        (bs == 64 || bs == 128 || bs == 256 || bs == 512))
+      ctx->hop_config = bs | (variant << 16);
+  }
   if (stream) {
     ctx->stream = (cudaStream_t)stream;
   } else {

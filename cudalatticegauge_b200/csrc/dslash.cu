@@ -15,13 +15,13 @@ bool idempotent(const HopArgs& a) { return a.x == nullptr || a.x != a.out; }
 
 template <int P, int RECON>
 cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
-  // config = block size | (register-capped variant << 16)
+  // config = block size | (variant << 16): 0 plain, 1 register-capped
   auto go = [&](int cfg) {
     const int bs = cfg & 0xffff;
-    const bool capped = (cfg >> 16) != 0;
+    const int variant = cfg >> 16;
     dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
     if constexpr (P != P64) {
-      if (capped) {
+      if (variant == 1) {
         if (dagger)
           wilson_hop_kernel<P, RECON, true, 3><<<grid, bs, 0, ctx->stream>>>(a);
         else
@@ -37,6 +37,7 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
     ctx->kernels++;
     return cudaGetLastError();
   };
+  if (ctx->hop_config >= 0) return go(ctx->hop_config);
   std::vector<int> cand = {64, 128, 256, 512};
   if (P != P64)
     for (int bs : {64, 128, 256}) cand.push_back(bs | (1 << 16));
@@ -163,7 +164,7 @@ clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
   const bool wilson = s.kind == CLG_FERMION_WILSON;
   std::string key = std::string(wilson ? "wilson" : "ks") + "_p" + std::to_string(s.prec) + "_d" +
                     std::to_string((int)s.dagger) + "_V" + std::to_string((long long)a.g.Vh) + "_n" +
-                    std::to_string(s.nrhs);
+                    std::to_string(s.nrhs) + "_r" + std::to_string(s.prec == CLG_PREC_SINGLE ? U->recon32 : 0);
   cudaError_t e = cudaSuccess;
   if (s.prec == CLG_PREC_DOUBLE) {
     a.U_here = U->u64[p];

@@ -117,6 +117,30 @@ __device__ __forceinline__ void neighbours(const Geom& g, int p, int64_t h, NbrI
   }
 }
 
+// out = [scale_dev[rhs] *] (a * acc + xa * x), stored at (rhs, h)
+template <int P, typename AT>
+__device__ __forceinline__ void wilson_hop_store(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
+  const int64_t Vh = a.g.Vh;
+  const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = ca * acc[k];
+  if (a.x) {
+    cpx<AT> xv[12];
+    const char* xp = reinterpret_cast<const char*>(a.x) + rhs * a.x_stride;
+    load_site<P, 12, AT>(xp, a.x_norm ? a.x_norm + rhs * a.x_nstride : nullptr, Vh, h, xv);
+    const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = acc[k] + cx * xv[k];
+  }
+  if (a.scale_dev) {
+    const AT sc = (AT)a.scale_dev[rhs * a.scale_stride];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];
+  }
+  store_site<P, 12, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
+                        a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
+}
+
 // MINB = 3 caps registers at 85 per thread (24 resident warps per SM instead
 // of 16): the hop is latency-bound on its gathers, and the low-precision
 // variants fit in 80 registers without spilling.  The autotuner picks.
@@ -186,24 +210,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
 #undef CLG_WILSON_DIR
   }
 
-  const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = ca * acc[k];
-  if (a.x) {
-    cpx<AT> xv[12];
-    const char* xp = reinterpret_cast<const char*>(a.x) + rhs * a.x_stride;
-    load_site<P, 12, AT>(xp, a.x_norm ? a.x_norm + rhs * a.x_nstride : nullptr, Vh, h, xv);
-    const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
-#pragma unroll
-    for (int k = 0; k < 12; ++k) acc[k] = acc[k] + cx * xv[k];
-  }
-  if (a.scale_dev) {
-    const AT sc = (AT)a.scale_dev[rhs * a.scale_stride];
-#pragma unroll
-    for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];
-  }
-  store_site<P, 12, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
-                        a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
+  wilson_hop_store<P>(a, rhs, h, acc);
 }
 
 template <int P, int RECON>

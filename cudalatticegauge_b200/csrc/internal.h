@@ -75,6 +75,9 @@ struct clg_context_s {
   // block size chosen per kernel variant by the autotuner
   std::map<std::string, int> tuned;
   bool tuning_enabled = true;
+  // CLG_HOP_CONFIG="<variant>:<block>" pins the Wilson hop launch (variant
+  // 0 plain, 1 register-capped; block 64..512); -1 lets the autotuner choose
+  int hop_config = -1;
   clg_status fail(clg_status s, const std::string& msg) {
     last_error = msg;
     return s;
