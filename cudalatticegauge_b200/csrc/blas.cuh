@@ -13,6 +13,7 @@
 
 #include "field_io.cuh"
 #include "internal.h"
+#include "reduce.cuh"
 
 namespace clg {
 
@@ -30,65 +31,8 @@ __global__ void __launch_bounds__(256)
       f(rhs, first_parity + pi, h, acc);
     }
   }
-  if constexpr (NRED > 0) {
-    __shared__ double sm[NRED][8];
-    __shared__ bool last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < NRED; ++k) {
-      double v = acc[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lane == 0) sm[k][warp] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < NRED) {
-      double v = 0.0;
-      const int nw = (blockDim.x + 31) >> 5;
-      for (int w = 0; w < nw; ++w) v += sm[threadIdx.x][w];
-      partials[((int64_t)rhs * gridDim.x + blockIdx.x) * NRED + threadIdx.x] = v;
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const unsigned t = atomicAdd(counter, 1u);
-      last = (t == gridDim.x * gridDim.y - 1);
-    }
-    __syncthreads();
-    if (last) {
-      // every thread of the last block sums a fixed strided subset of the block
-      // partials, then a fixed shuffle / shared-memory tree: parallel and
-      // deterministic (independent of which block arrived last)
-      __shared__ double tot[NRED];
-      __threadfence();
-      for (int r = 0; r < (int)gridDim.y; ++r) {
-        double s[NRED];
-#pragma unroll
-        for (int k = 0; k < NRED; ++k) s[k] = 0.0;
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-#pragma unroll
-          for (int k = 0; k < NRED; ++k) s[k] += __ldcg(partials + ((int64_t)r * gridDim.x + b) * NRED + k);
-#pragma unroll
-        for (int k = 0; k < NRED; ++k) {
-          double v = s[k];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-          if (lane == 0) sm[k][warp] = v;
-        }
-        __syncthreads();
-        if (threadIdx.x < NRED) {
-          double v = 0.0;
-          const int nw = (blockDim.x + 31) >> 5;
-          for (int w = 0; w < nw; ++w) v += sm[threadIdx.x][w];
-          tot[threadIdx.x] = v;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) f.finalize(r, tot);
-        __syncthreads();
-      }
-      if (threadIdx.x == 0) *counter = 0u;
-    }
-  }
+  if constexpr (NRED > 0)
+    grid_reduce_finalize<NRED>(acc, f, rhs, blockIdx.x, gridDim.x, (int)gridDim.y, partials, counter);
 }
 
 // Launch F over the checkerboards [first_parity, first_parity + nparity) of all nrhs.

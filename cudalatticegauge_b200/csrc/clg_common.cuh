@@ -41,6 +41,13 @@ template <typename T> __device__ __forceinline__ cpx<T> operator*(cpx<T> a, cpx<
 }
 template <typename T> __device__ __forceinline__ cpx<T> operator*(T s, cpx<T> a) { return mk<T>(s * a.x, s * a.y); }
 template <typename T> __device__ __forceinline__ cpx<T> cj(cpx<T> a) { return mk<T>(a.x, -a.y); }
+// acc + s * a, one fused multiply-add per real component
+template <typename T> __device__ __forceinline__ cpx<T> cfma(T s, cpx<T> a, cpx<T> acc) {
+  if constexpr (sizeof(T) == 4)
+    return mk<T>(fmaf(s, a.x, acc.x), fmaf(s, a.y, acc.y));
+  else
+    return mk<T>(fma(s, a.x, acc.x), fma(s, a.y, acc.y));
+}
 // conj(a) * b
 template <typename T> __device__ __forceinline__ cpx<T> cjmul(cpx<T> a, cpx<T> b) {
   return mk<T>(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);

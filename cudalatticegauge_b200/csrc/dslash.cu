@@ -15,7 +15,8 @@ bool idempotent(const HopArgs& a) { return a.x == nullptr || a.x != a.out; }
 
 template <int P, int RECON>
 cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
-  // config = block size | (variant << 16): 0 plain, 1 register-capped
+  // config = block size | (variant << 16): 0 plain, 1 capped at 80 registers,
+  // 2 capped at 72 registers (64-thread blocks only)
   auto go = [&](int cfg) {
     const int bs = cfg & 0xffff;
     const int variant = cfg >> 16;
@@ -23,9 +24,17 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
     if constexpr (P != P64) {
       if (variant == 1) {
         if (dagger)
-          wilson_hop_kernel<P, RECON, true, 3><<<grid, bs, 0, ctx->stream>>>(a);
+          wilson_hop_kernel<P, RECON, true, 256, 3><<<grid, bs, 0, ctx->stream>>>(a);
         else
-          wilson_hop_kernel<P, RECON, false, 3><<<grid, bs, 0, ctx->stream>>>(a);
+          wilson_hop_kernel<P, RECON, false, 256, 3><<<grid, bs, 0, ctx->stream>>>(a);
+        ctx->kernels++;
+        return cudaGetLastError();
+      }
+      if (variant == 2 && bs == 64) {
+        if (dagger)
+          wilson_hop_kernel<P, RECON, true, 64, 14><<<grid, bs, 0, ctx->stream>>>(a);
+        else
+          wilson_hop_kernel<P, RECON, false, 64, 14><<<grid, bs, 0, ctx->stream>>>(a);
         ctx->kernels++;
         return cudaGetLastError();
       }
@@ -38,9 +47,11 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
     return cudaGetLastError();
   };
   if (ctx->hop_config >= 0) return go(ctx->hop_config);
-  std::vector<int> cand = {64, 128, 256, 512};
+  // __launch_bounds__(256, ...) caps the block at 256 threads
+  std::vector<int> cand = {64, 128, 256};
   if (P != P64)
     for (int bs : {64, 128, 256}) cand.push_back(bs | (1 << 16));
+  if (P != P64) cand.push_back(64 | (2 << 16));
   return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 
@@ -133,13 +144,12 @@ clg_status gauge_prepare(clg_gauge_s* U, int prec) {
   return CLG_SUCCESS;
 }
 
-clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
+clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, HopArgs& a) {
   const int p = s.out_parity;
   if (!s.in.has_parity(1 - p) || !s.out.has_parity(p) || (s.x && !s.x->has_parity(p)))
     return ctx->fail(CLG_ERR_BAD_ARG, "hop: field does not hold the required checkerboard");
   if (s.in.prec != s.prec || s.out.prec != s.prec || (s.x && s.x->prec != s.prec))
     return ctx->fail(CLG_ERR_BAD_ARG, "hop: precision mismatch");
-  HopArgs a;
   a.g = U->lat->g;
   a.out_parity = p;
   a.in = s.in.base(0, 1 - p);
@@ -161,27 +171,48 @@ clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
   a.skip_dev = s.skip_dev;
   a.skip_stride = s.skip_stride;
   a.nrhs = s.nrhs > 0 ? s.nrhs : 1;
-  const bool wilson = s.kind == CLG_FERMION_WILSON;
-  std::string key = std::string(wilson ? "wilson" : "ks") + "_p" + std::to_string(s.prec) + "_d" +
-                    std::to_string((int)s.dagger) + "_V" + std::to_string((long long)a.g.Vh) + "_n" +
-                    std::to_string(s.nrhs) + "_r" + std::to_string(s.prec == CLG_PREC_SINGLE ? U->recon32 : 0);
-  cudaError_t e = cudaSuccess;
   if (s.prec == CLG_PREC_DOUBLE) {
     a.U_here = U->u64[p];
     a.U_there = U->u64[1 - p];
-    e = wilson ? launch_wilson<P64, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P64, 18>(ctx, a, s.nrhs, key);
   } else if (s.prec == CLG_PREC_SINGLE) {
     a.U_here = U->u32[p];
     a.U_there = U->u32[1 - p];
     if (!a.U_here || !a.U_there) return ctx->fail(CLG_ERR_BAD_ARG, "hop: FP32 links not prepared");
+  } else {
+    a.U_here = U->u16[p];
+    a.U_there = U->u16[1 - p];
+    if (!a.U_here || !a.U_there) return ctx->fail(CLG_ERR_BAD_ARG, "hop: FP16 links not prepared");
+  }
+  return CLG_SUCCESS;
+}
+
+static std::string hop_key(const clg_gauge_s* U, const HopSpec& s) {
+  const bool wilson = s.kind == CLG_FERMION_WILSON;
+  return std::string(wilson ? "wilson" : "ks") + "_p" + std::to_string(s.prec) + "_d" + std::to_string((int)s.dagger) +
+         "_V" + std::to_string((long long)U->lat->g.Vh) + "_n" + std::to_string(s.nrhs) + "_r" +
+         std::to_string(s.prec == CLG_PREC_SINGLE ? U->recon32 : 0);
+}
+
+int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback) {
+  auto it = ctx->tuned.find(hop_key(U, s));
+  if (it == ctx->tuned.end()) return fallback;
+  return it->second & 0xffff;
+}
+
+clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
+  HopArgs a;
+  if (clg_status st = make_hop_args(ctx, U, s, a)) return st;
+  const bool wilson = s.kind == CLG_FERMION_WILSON;
+  const std::string key = hop_key(U, s);
+  cudaError_t e = cudaSuccess;
+  if (s.prec == CLG_PREC_DOUBLE) {
+    e = wilson ? launch_wilson<P64, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P64, 18>(ctx, a, s.nrhs, key);
+  } else if (s.prec == CLG_PREC_SINGLE) {
     if (U->recon32 == 12)
       e = wilson ? launch_wilson<P32, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 12>(ctx, a, s.nrhs, key);
     else
       e = wilson ? launch_wilson<P32, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 18>(ctx, a, s.nrhs, key);
   } else {
-    a.U_here = U->u16[p];
-    a.U_there = U->u16[1 - p];
-    if (!a.U_here || !a.U_there) return ctx->fail(CLG_ERR_BAD_ARG, "hop: FP16 links not prepared");
     e = wilson ? launch_wilson<P16, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P16, 12>(ctx, a, s.nrhs, key);
   }
   if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("hop launch: ") + cudaGetErrorString(e));

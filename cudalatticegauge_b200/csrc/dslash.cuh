@@ -18,6 +18,7 @@
 // device-resident scalar (used for lazily normalised Krylov vectors).
 #pragma once
 #include "field_io.cuh"
+#include "reduce.cuh"
 
 namespace clg {
 
@@ -79,15 +80,16 @@ __device__ __forceinline__ void wilson_hop_dir(cpx<AT> acc[12], const cpx<AT> ps
   }
   su3_mv<AT, UDAG>(u, h0, g0);
   su3_mv<AT, UDAG>(u, h1, g1);
+  // each accumulator row takes s * (phase * g) as one fused multiply-add per
+  // real component: the phase is a swap / negation (operand modifiers), and s
+  // is never applied to g separately
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    g0[c] = s * g0[c];
-    g1[c] = s * g1[c];
-    acc[c] = acc[c] + g0[c];
-    acc[3 + c] = acc[3 + c] + g1[c];
+    acc[c] = cfma(s, g0[c], acc[c]);
+    acc[3 + c] = cfma(s, g1[c], acc[3 + c]);
     // rows 2,3: coefficient SGN*i^z4[r] times the projected row perm[r] (in {0,1})
-    acc[6 + c] = acc[6 + c] + mul_i(gperm(MU, 2) == 0 ? g0[c] : g1[c], gz4(MU, 2) + add);
-    acc[9 + c] = acc[9 + c] + mul_i(gperm(MU, 3) == 0 ? g0[c] : g1[c], gz4(MU, 3) + add);
+    acc[6 + c] = cfma(s, mul_i(gperm(MU, 2) == 0 ? g0[c] : g1[c], gz4(MU, 2) + add), acc[6 + c]);
+    acc[9 + c] = cfma(s, mul_i(gperm(MU, 3) == 0 ? g0[c] : g1[c], gz4(MU, 3) + add), acc[9 + c]);
   }
 }
 
@@ -117,9 +119,9 @@ __device__ __forceinline__ void neighbours(const Geom& g, int p, int64_t h, NbrI
   }
 }
 
-// out = [scale_dev[rhs] *] (a * acc + xa * x), stored at (rhs, h)
+// acc <- [scale_dev[rhs] *] (a * acc + xa * x) at (rhs, h)
 template <int P, typename AT>
-__device__ __forceinline__ void wilson_hop_store(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
+__device__ __forceinline__ void wilson_hop_finish(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
   const int64_t Vh = a.g.Vh;
   const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
 #pragma unroll
@@ -137,23 +139,18 @@ __device__ __forceinline__ void wilson_hop_store(const HopArgs& a, int rhs, int6
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];
   }
-  store_site<P, 12, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
-                        a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
 }
 
-// MINB = 3 caps registers at 85 per thread (24 resident warps per SM instead
-// of 16): the hop is latency-bound on its gathers, and the low-precision
-// variants fit in 80 registers without spilling.  The autotuner picks.
-template <int P, int RECON, bool DAGGER, int MINB = 1>
-__global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
-  using AT = typename AccT<P>::T;
+template <int P, typename AT>
+__device__ __forceinline__ void wilson_hop_store(const HopArgs& a, int rhs, int64_t h, const cpx<AT> acc[12]) {
+  store_site<P, 12, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
+                        a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, a.g.Vh, h, acc);
+}
+
+// The whole stencil for output site (rhs, h): acc = [scale *] (a H in + xa x)
+template <int P, int RECON, bool DAGGER, typename AT>
+__device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
   const int64_t Vh = a.g.Vh;
-  // right-hand sides are interleaved in blockIdx.x so that the CTAs of all rhs
-  // for the same sites run back to back and share the links through L2
-  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
-  const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
-  if (h >= Vh) return;
-  if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
   const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
 
@@ -161,7 +158,6 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
   int c[4];
   neighbours(a.g, a.out_parity, h, nb, c);
 
-  cpx<AT> acc[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) acc[k] = mk<AT>(0, 0);
 
@@ -170,7 +166,10 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
   constexpr int SB = -SF;
   if constexpr (P == P16) {
     // FP16: both neighbours' packed data (19 registers each) are loaded before
-    // either is unpacked, so twice the bytes are in flight per thread
+    // either is unpacked, so twice the bytes are in flight per thread.  The
+    // projection and the link product are linear, so the neighbour's site norm
+    // is applied with the boundary sign to the 6 projected products instead of
+    // to the 24 unpacked components.
 #define CLG_WILSON_DIR16(MU)                                                            \
   {                                                                                     \
     Packed16 pf, pb;                                                                    \
@@ -180,12 +179,12 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
     load_packed16(in, in_norm, Vh, nb.hb[MU], pb);                                      \
     load_packed_link16(a.U_there, MU, Vh, nb.hb[MU], lb);                               \
     cpx<AT> psi[12], u[9];                                                              \
-    unpack16(pf, psi);                                                                  \
+    unpack16_raw(pf, psi);                                                              \
     unpack_link16(lf, u);                                                               \
-    wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (AT)nb.sf[MU]);                      \
-    unpack16(pb, psi);                                                                  \
+    wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (AT)nb.sf[MU] * pf.n);               \
+    unpack16_raw(pb, psi);                                                              \
     unpack_link16(lb, u);                                                               \
-    wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU]);                       \
+    wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU] * pb.n);                \
   }
     CLG_WILSON_DIR16(0)
     CLG_WILSON_DIR16(1)
@@ -209,8 +208,54 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_kernel(HopArgs a) {
     CLG_WILSON_DIR(3)
 #undef CLG_WILSON_DIR
   }
+  wilson_hop_finish<P>(a, rhs, h, acc);
+}
 
+// Register caps through the launch bounds (the autotuner picks per operator):
+// (256, 3) caps at 80 registers (24 resident warps per SM instead of 16): the
+// hop is latency-bound on its gathers, and the low-precision variants fit in
+// 80 registers without spilling.  (64, 14) caps at 72 registers, 28 warps per
+// SM: one rhs of a 32^3 x 16 checkerboard (262144 threads) then runs in two
+// full waves instead of 2.3.
+template <int P, int RECON, bool DAGGER, int MAXT = 256, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) wilson_hop_kernel(HopArgs a) {
+  using AT = typename AccT<P>::T;
+  // right-hand sides are interleaved in blockIdx.x so that the CTAs of all rhs
+  // for the same sites run back to back and share the links through L2
+  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
+  const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
+  if (h >= a.g.Vh) return;
+  if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
+  cpx<AT> acc[12];
+  wilson_hop_site<P, RECON, DAGGER>(a, rhs, h, acc);
   wilson_hop_store<P>(a, rhs, h, acc);
+}
+
+// The hop with a fused epilogue E (used by the Krylov solvers):
+//   E::STORE      the result is stored to a.out (else it only feeds E::site)
+//   E::NRED       doubles reduced over the grid per rhs, E::finalize(rhs, tot)
+//                 runs on the device in the last block (grid_reduce_finalize)
+//   E::site(rhs, h, acc, red)   per-site work on the result in registers
+// Every thread reaches the block reduction: out-of-range sites and skipped
+// right-hand sides contribute zero.
+template <int P, int RECON, bool DAGGER, int MAXT, int MINB, class E>
+__global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E e, double* partials,
+                                                                    unsigned* counter) {
+  using AT = typename AccT<P>::T;
+  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
+  const unsigned slot = blockIdx.x / (unsigned)a.nrhs;
+  const int64_t h = (int64_t)slot * blockDim.x + threadIdx.x;
+  const bool live = h < a.g.Vh && !(a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]);
+  double red[E::NRED];
+#pragma unroll
+  for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
+  if (live) {
+    cpx<AT> acc[12];
+    wilson_hop_site<P, RECON, DAGGER>(a, rhs, h, acc);
+    if constexpr (E::STORE) wilson_hop_store<P>(a, rhs, h, acc);
+    e.site(rhs, h, acc, red);
+  }
+  grid_reduce_finalize<E::NRED>(red, e, rhs, slot, gridDim.x / (unsigned)a.nrhs, a.nrhs, partials, counter);
 }
 
 template <int P, int RECON>

@@ -218,6 +218,17 @@ __device__ __forceinline__ void unpack16(const Packed16& p, cpx<float> v[12]) {
     f = h2f(p.c[k].w); v[4 * k + 3] = mk<float>(p.n * f.x, p.n * f.y);
   }
 }
+// the stored halves without the site norm (callers fold p.n into a later scale)
+__device__ __forceinline__ void unpack16_raw(const Packed16& p, cpx<float> v[12]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float2 f;
+    f = h2f(p.c[k].x); v[4 * k + 0] = mk<float>(f.x, f.y);
+    f = h2f(p.c[k].y); v[4 * k + 1] = mk<float>(f.x, f.y);
+    f = h2f(p.c[k].z); v[4 * k + 2] = mk<float>(f.x, f.y);
+    f = h2f(p.c[k].w); v[4 * k + 3] = mk<float>(f.x, f.y);
+  }
+}
 __device__ __forceinline__ void load_packed_link16(const void* __restrict__ base, int mu, int64_t Vh, int64_t h,
                                                    PackedLink16& l) {
   const uint4* b4 = reinterpret_cast<const uint4*>(base);

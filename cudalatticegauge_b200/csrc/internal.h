@@ -76,8 +76,11 @@ struct clg_context_s {
   std::map<std::string, int> tuned;
   bool tuning_enabled = true;
   // CLG_HOP_CONFIG="<variant>:<block>" pins the Wilson hop launch (variant
-  // 0 plain, 1 register-capped; block 64..512); -1 lets the autotuner choose
+  // 0 plain, 1 register-capped; block 64, 128 or 256); -1 lets the autotuner choose
   int hop_config = -1;
+  // CG on the Wilson normal equations fuses its vector work into the Schur
+  // hops; CLG_FUSED_CG=0 runs the separate kernels instead
+  bool fused_cg = true;
   clg_status fail(clg_status s, const std::string& msg) {
     last_error = msg;
     return s;
@@ -189,6 +192,12 @@ struct HopSpec {
   int nrhs;
 };
 clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s);
+// the kernel arguments of a hop (checked as hop() checks them), for callers
+// that launch a fused variant themselves
+struct HopArgs;
+clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, HopArgs& a);
+// block size the autotuner chose for this hop (fallback if not tuned yet)
+int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
 clg_status gauge_prepare(clg_gauge_s* U, int prec);  // builds the FP32 / FP16 copies on first use
 
 // ------------------------------------------------------------ operator composition (api.cu)

@@ -275,6 +275,33 @@ struct CgInit {
     }
   }
 };
+// pAp = (p, A p) -> alpha = rr / pAp; counts `weight` operator applications
+__device__ __forceinline__ void cg_alpha_finalize(KState& k, double pAp, int weight) {
+  if (k.skip) return;
+  k.iters += weight;
+  if (!(pAp > 0.0) || bad(pAp)) {
+    k.status = ST_BREAKDOWN;
+    k.done = k.skip = 1;
+    return;
+  }
+  k.alpha = make_double2(k.rr / pAp, 0.0);
+}
+// rr_new = |r|^2 after the update -> beta, convergence
+__device__ __forceinline__ void cg_update_finalize(KState& k, double rr_new) {
+  if (k.skip) return;
+  if (bad(rr_new)) {
+    k.status = ST_BREAKDOWN;
+    k.done = k.skip = 1;
+    return;
+  }
+  k.beta = make_double2(rr_new / k.rr, 0.0);
+  k.rr = rr_new;
+  if (rr_new <= k.tol2 * k.rr0) {
+    k.status = ST_CONVERGED;
+    k.done = k.skip = 1;
+  }
+}
+
 // (p, q) -> alpha = rr / (p, q)
 template <int P, int NC>
 struct CgAlpha {
@@ -289,17 +316,7 @@ struct CgAlpha {
     ldv<P, NC, AT>(q, rhs, par, h, b);
     acc_dot<NC, AT>(a, b, acc);
   }
-  __device__ void finalize(int r, const double* s) const {
-    KState& k = st[r];
-    if (k.skip) return;
-    k.iters += weight;
-    if (!(s[0] > 0.0) || bad(s[0])) {
-      k.status = ST_BREAKDOWN;
-      k.done = k.skip = 1;
-      return;
-    }
-    k.alpha = make_double2(k.rr / s[0], 0.0);
-  }
+  __device__ void finalize(int r, const double* s) const { cg_alpha_finalize(st[r], s[0], weight); }
 };
 // x += alpha p ; r -= alpha q ; rr_new -> beta
 template <int P, int NC>
@@ -324,21 +341,51 @@ struct CgUpdate {
     stv<P, NC, AT>(r, rhs, par, h, vr);
     acc[0] += site_norm2<NC, AT>(vr);
   }
-  __device__ void finalize(int w, const double* s) const {
-    KState& k = st[w];
-    if (k.skip) return;
-    if (bad(s[0])) {
-      k.status = ST_BREAKDOWN;
-      k.done = k.skip = 1;
-      return;
-    }
-    k.beta = make_double2(s[0] / k.rr, 0.0);
-    k.rr = s[0];
-    if (s[0] <= k.tol2 * k.rr0) {
-      k.status = ST_CONVERGED;
-      k.done = k.skip = 1;
-    }
+  __device__ void finalize(int w, const double* s) const { cg_update_finalize(st[w], s[0]); }
+};
+
+// CG on A = M M^+ (or M^+ M) with the vector work fused into the Schur hops
+// (wilson_hop_epi_kernel).  The second hop of the first factor produces
+// q = M^+ p (or M p), stores it and reduces |q|^2 = (p, A p) -> alpha; the
+// second hop of the second factor produces A p in registers only and applies
+//   x += alpha p,  r -= alpha A p,  |r|^2 -> beta
+// at its own site, so A p is never written and the separate (p, A p) and
+// update passes disappear.  Both act on the even checkerboard (parity 0).
+template <int P>
+struct CgHopAlpha {
+  static constexpr int NRED = 1;
+  static constexpr bool STORE = true;
+  KState* st;
+  int weight;
+  template <typename AT>
+  __device__ void site(int, int64_t, const cpx<AT> q[12], double* red) const {
+    red[0] += site_norm2<12, AT>(q);
   }
+  __device__ void finalize(int r, const double* s) const { cg_alpha_finalize(st[r], s[0], weight); }
+};
+template <int P>
+struct CgHopUpdate {
+  static constexpr int NRED = 1;
+  static constexpr bool STORE = false;
+  DField x, r, p;
+  KState* st;
+  template <typename AT>
+  __device__ void site(int rhs, int64_t h, const cpx<AT> ap[12], double* red) const {
+    const AT al = (AT)st[rhs].alpha.x;
+    cpx<AT> vx[12], vr[12], vp[12];
+    ldv<P, 12, AT>(x, rhs, 0, h, vx);
+    ldv<P, 12, AT>(r, rhs, 0, h, vr);
+    ldv<P, 12, AT>(p, rhs, 0, h, vp);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      vx[i] = vx[i] + al * vp[i];
+      vr[i] = vr[i] - al * ap[i];
+    }
+    stv<P, 12, AT>(x, rhs, 0, h, vx);
+    stv<P, 12, AT>(r, rhs, 0, h, vr);
+    red[0] += site_norm2<12, AT>(vr);
+  }
+  __device__ void finalize(int w, const double* s) const { cg_update_finalize(st[w], s[0]); }
 };
 // p = r + beta p
 template <int P, int NC>

@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "dslash.cuh"
 #include "krylov.cuh"
 
 namespace clg {
@@ -391,6 +392,105 @@ clg_status launch_gm_dots(clg_context_s* ctx, const VList& vl, const FieldRef& w
 
 // ------------------------------------------------------------------ Krylov methods
 // Solve K x = b (precision P, the subset of b) for every rhs not marked in outer_done.
+// ------------------------------------------------------------------ fused CG on the Wilson normal equations
+// CG on A = M_ee M_ee^+ (CLG_OP_MEE_MEEDAG) or M_ee^+ M_ee (OP_MEEDAG_MEE)
+// without a shift: one iteration is the four Schur hops of A p with the CG
+// vector work in the epilogues of the second and fourth (CgHopAlpha,
+// CgHopUpdate), then p = r + beta p.
+bool fused_cg(const Work& w, int op) {
+  return w.ctx->fused_cg && w.kind == CLG_FERMION_WILSON && !w.shift_dev &&
+         (op == CLG_OP_MEE_MEEDAG || op == OP_MEEDAG_MEE);
+}
+
+template <int P, int RECON, bool DAG, class E>
+cudaError_t launch_hop_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int bs) {
+  dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * a.nrhs));
+  constexpr int MINB = P == P64 ? 1 : 3;
+  wilson_hop_epi_kernel<P, RECON, DAG, 256, MINB, E>
+      <<<grid, bs, 0, ctx->stream>>>(a, e, ctx->red_partials, ctx->red_counter);
+  ctx->kernels++;
+  return cudaGetLastError();
+}
+
+// out_e = in_e - kappa^2 H_eo^(dag) t_o with epilogue e (E::STORE decides
+// whether out_e is written)
+template <int P, class E>
+clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRef& in_even, const FieldRef& out_even,
+                         const E& e, const int* skip, int ks) {
+  clg_context_s* ctx = w.ctx;
+  HopSpec s;
+  s.kind = CLG_FERMION_WILSON;
+  s.prec = P;
+  s.dagger = dag;
+  s.out_parity = 0;
+  s.in = t_odd;
+  s.out = out_even;
+  s.x = &in_even;
+  s.a = make_double2(-w.param * w.param, 0.0);
+  s.xa = make_double2(1.0, 0.0);
+  s.scale_dev = nullptr;
+  s.scale_stride = 0;
+  s.skip_dev = skip;
+  s.skip_stride = ks;
+  s.nrhs = w.nrhs;
+  HopArgs a;
+  if (clg_status st = make_hop_args(ctx, w.U, s, a)) return st;
+  // the block size tuned for the plain hop of the same kind (the hops on the
+  // odd checkerboard of each iteration run first and are tuned)
+  HopSpec plain = s;
+  plain.x = nullptr;
+  const int bs = tuned_hop_block(ctx, w.U, plain, P == P64 ? 64 : 128);
+  const int64_t nblk = ((w.Vh + bs - 1) / bs) * w.nrhs;
+  if (clg_status st = ensure_reduction(ctx, nblk * E::NRED)) return st;
+  cudaError_t err;
+  if constexpr (P == P64) {
+    err = dag ? launch_hop_epi<P, 18, true>(ctx, a, e, bs) : launch_hop_epi<P, 18, false>(ctx, a, e, bs);
+  } else if constexpr (P == P32) {
+    if (w.U->recon32 == 12)
+      err = dag ? launch_hop_epi<P, 12, true>(ctx, a, e, bs) : launch_hop_epi<P, 12, false>(ctx, a, e, bs);
+    else
+      err = dag ? launch_hop_epi<P, 18, true>(ctx, a, e, bs) : launch_hop_epi<P, 18, false>(ctx, a, e, bs);
+  } else {
+    err = dag ? launch_hop_epi<P, 12, true>(ctx, a, e, bs) : launch_hop_epi<P, 12, false>(ctx, a, e, bs);
+  }
+  if (err != cudaSuccess) return ctx->fail(cuda_status(err), std::string("fused hop: ") + cudaGetErrorString(err));
+  return CLG_SUCCESS;
+}
+
+// t_o = H_oe^(dag) in_e
+clg_status schur_hop_odd(Work& w, bool dag, const FieldRef& in_even, const FieldRef& t_odd, const int* skip, int ks) {
+  HopSpec s;
+  s.kind = CLG_FERMION_WILSON;
+  s.prec = t_odd.prec;
+  s.dagger = dag;
+  s.out_parity = 1;
+  s.in = in_even;
+  s.out = t_odd;
+  s.x = nullptr;
+  s.a = make_double2(1.0, 0.0);
+  s.xa = make_double2(0.0, 0.0);
+  s.scale_dev = nullptr;
+  s.scale_stride = 0;
+  s.skip_dev = skip;
+  s.skip_stride = ks;
+  s.nrhs = w.nrhs;
+  return hop(w.ctx, w.U, s);
+}
+
+// one CG iteration on A = M M^+ (m_dag_first) or M^+ M, fused as described above
+template <int P>
+clg_status cg_fused_iteration(Work& w, int op, const FieldRef& x, const FieldRef& r, const FieldRef& p,
+                              const int* skip, int ks) {
+  const bool d1 = op == CLG_OP_MEE_MEEDAG;  // the factor applied first is M^+
+  const FieldRef& to = w.kt_odd.ref;
+  const FieldRef& te = w.kt_even.ref;
+  clg_status s;
+  if ((s = schur_hop_odd(w, d1, p, to, skip, ks))) return s;
+  if ((s = schur_hop_epi<P>(w, d1, to, p, te, CgHopAlpha<P>{w.st, op_weight(op)}, skip, ks))) return s;
+  if ((s = schur_hop_odd(w, !d1, te, to, skip, ks))) return s;
+  return schur_hop_epi<P>(w, !d1, to, te, te, CgHopUpdate<P>{dfield(x), dfield(r), dfield(p), w.st}, skip, ks);
+}
+
 clg_status krylov(Work& w, int op, const FieldRef& x, const FieldRef& b, int slot_base) {
   clg_context_s* ctx = w.ctx;
   const int nrhs = w.nrhs;
@@ -443,13 +543,19 @@ clg_status krylov(Work& w, int op, const FieldRef& x, const FieldRef& b, int slo
       CgInit<PV, NV> init{dfield(b), dfield(x), dfield(r.ref), dfield(p.ref), w.st, w.tol_d};
       clg_status e = launch_sites<1>(ctx, init, fp, np, Vh, nrhs);
       if (e) return e;
+      const bool fused = NV == 12 && fused_cg(w, op);
       auto body = [&]() -> clg_status {
         clg_status e2;
-        if ((e2 = kapply(w, op, q.ref, p.ref, nullptr, 0, skip, ks))) return e2;
-        CgAlpha<PV, NV> ca{dfield(p.ref), dfield(q.ref), w.st, op_weight(op)};
-        if ((e2 = launch_sites<2>(ctx, ca, fp, np, Vh, nrhs))) return e2;
-        CgUpdate<PV, NV> up{dfield(x), dfield(r.ref), dfield(p.ref), dfield(q.ref), w.st};
-        if ((e2 = launch_sites<1>(ctx, up, fp, np, Vh, nrhs))) return e2;
+        if (fused) {
+          if constexpr (NV == 12)
+            if ((e2 = cg_fused_iteration<PV>(w, op, x, r.ref, p.ref, skip, ks))) return e2;
+        } else {
+          if ((e2 = kapply(w, op, q.ref, p.ref, nullptr, 0, skip, ks))) return e2;
+          CgAlpha<PV, NV> ca{dfield(p.ref), dfield(q.ref), w.st, op_weight(op)};
+          if ((e2 = launch_sites<2>(ctx, ca, fp, np, Vh, nrhs))) return e2;
+          CgUpdate<PV, NV> up{dfield(x), dfield(r.ref), dfield(p.ref), dfield(q.ref), w.st};
+          if ((e2 = launch_sites<1>(ctx, up, fp, np, Vh, nrhs))) return e2;
+        }
         return launch_sites<0>(ctx, CgP<PV, NV>{dfield(p.ref), dfield(r.ref), w.st}, fp, np, Vh, nrhs);
       };
       const int chunk = 16;

@@ -127,6 +127,39 @@ def test_wilson_cg_normal_equations(ctx, clg, oracle, op, name, prec):
     assert o.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
 
 
+@pytest.mark.parametrize("op,name", [(0, "WILSON_D"), (1, "WILSON_DDAG")])
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_wilson_cg_fused_matches_unfused(clg, oracle, op, name, prec, monkeypatch):
+    """The CG iteration whose vector updates run in the Schur hops' epilogues
+    (the default) against the one with separate (p, Ap) / update kernels
+    (CLG_FUSED_CG=0): both reach the FP64 true residual, on two right-hand
+    sides, with iteration counts that agree to within a few percent (they
+    differ only in rounding: the fused form never stores A p)."""
+    infos, sols = {}, {}
+    for fused in ("1", "0"):
+        monkeypatch.setenv("CLG_FUSED_CG", fused)
+        c = clg.Context(0)
+        lat = clg.Lattice(c, (8, 8, 8, 16))
+        U = gauge(clg, lat, "expH", 0xC1A60001)
+        b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=2)
+        for r in range(2):
+            b.InitialField(clg.SOURCE_GAUSS, 16 + r, 2, rhs=r)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=2)
+        infos[fused] = clg.CSLASolverCG(c, inner_precision=prec).Solve(x, b, U, op)
+        o = oracle.Operator(name, lat.dims, U.CopyDataOut(), KAPPA)
+        for r in range(2):
+            assert infos[fused][r]["status"] == 0
+            assert o.true_residual(b.to_numpy(r), x.to_numpy(r)) <= TOL
+        sols[fused] = [x.to_numpy(r) for r in range(2)]
+        c.close()
+    for r in range(2):
+        n1, n0 = infos["1"][r]["iterations"], infos["0"][r]["iterations"]
+        assert abs(n1 - n0) <= max(4, 0.05 * n0), (n1, n0)
+        # both solutions have residual <= 1e-10; their distance is bounded by
+        # that times the condition number of D
+        assert np.linalg.norm(sols["1"][r] - sols["0"][r]) <= 1e-7 * np.linalg.norm(sols["0"][r])
+
+
 def test_half_precision_point_source(ctx, clg, oracle):
     """A point source makes sites with tiny (float-denormal) maxima after a few
     hops; the FP16 per-site-norm storage must flush them instead of producing NaN."""
