@@ -307,21 +307,23 @@ def ours(args, world, rank, local):
     b1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
     b1.from_numpy(src[nrhs - 1])
 
-    # ---------------- roofline of the dominant kernel (FP32 checkerboard hop)
+    # ---------------- roofline of the dominant kernel (the checkerboard hop in
+    # the inner precision)
     peak, peak_kind = peaks()
-    t_hop, hop_launches = time_hops(clg, ctx, lat, U, clg.SINGLE, stream)
-    hop_alg = hop_bytes_per_site(1) * Vh
+    pname = {"single": "fp32", "half": "fp16"}[args.inner]
+    t_hop, hop_launches = time_hops(clg, ctx, lat, U, inner, stream)
+    hop_alg = hop_bytes_per_site(inner) * Vh
     achieved = hop_alg / t_hop / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "hop_fp32_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "hop_traffic.json")
     if os.path.exists(tp):
         d = json.load(open(tp))
         if tuple(d.get("dims", ())) == tuple(W["dims"]):
-            traffic = d.get("bytes_per_launch")
+            traffic = d.get(pname, {}).get("bytes_per_launch")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic,
-            "kernel": "wilson_hop_kernel<P32,12-real>", "bytes_per_launch": hop_alg,
-            "launch_us": round(t_hop * 1e6, 2), "peak_source": peak_kind}
+            "kernel": f"wilson_hop_kernel<{'P32' if inner == clg.SINGLE else 'P16'},12-real>",
+            "bytes_per_launch": hop_alg, "launch_us": round(t_hop * 1e6, 2), "peak_source": peak_kind}
 
     extra = {}
     if rank == 0 and not args.quick:
@@ -358,6 +360,10 @@ def ours(args, world, rank, local):
         extra["solves"] = plain
         if args.workload == DEFAULT_WORKLOAD and not args.no_batched:
             extra["batched_config4"] = batched_config4(clg, ctx, stream, args)
+            extra["uneven_lattices_config4"] = uneven_lattices(clg, ctx, stream, args)
+        if args.workload == DEFAULT_WORKLOAD and not args.no_side:
+            extra["dslash_config3"] = dslash_config3(clg, ctx, stream)
+            extra["staggered_multishift_config5"] = staggered_config5(clg, ctx, stream)
         if world == 1 and not args.no_cpu:
             extra["cpu_baseline"] = cpu_baseline(U, lat, kappa, plain["fp64_gmres12"]["applications"])
     result = {
@@ -386,8 +392,9 @@ def ours(args, world, rank, local):
 
 def batched_config4(clg, ctx, stream, args, steps=2):
     """BASELINE config 4 measured beside the headline: 32^3x32, 12 spin-colour point
-    sources + 16 Z2 noise sources solved in one batched call (FP32-inner CGNE in
-    FP64 defect correction), against one FP64 CGNE solve of a single source."""
+    sources + 16 Z2 noise sources solved in one batched call (CGNE in the
+    `--inner` precision inside FP64 defect correction), against one FP64 CGNE
+    solve of a single source."""
     import torch
 
     W = WORKLOADS["wilson_eo_batched_32x32x32x32"]
@@ -401,7 +408,8 @@ def batched_config4(clg, ctx, stream, args, steps=2):
     for r in range(12, n):
         b.InitialField(clg.SOURCE_Z2, W["seed"], 2 + r, rhs=r)
     x = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=n)
-    s = clg.CSLASolverCG(ctx, inner_precision=clg.SINGLE, tol_true_rel=TOL)
+    inner = {"single": clg.SINGLE, "half": clg.HALF}[args.inner]
+    s = clg.CSLASolverCG(ctx, inner_precision=inner, tol_true_rel=TOL)
     s.Solve(x, b, U, clg.EFO_F_D)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -423,7 +431,8 @@ def batched_config4(clg, ctx, stream, args, steps=2):
     e1.record(stream)
     torch.cuda.synchronize()
     t64 = e0.elapsed_time(e1) / 1e3
-    out = {"dims": list(W["dims"]), "rhs": n, "solver": "CGNE, FP32 inner, FP64 defect correction, batched",
+    label = {"single": "FP32", "half": "FP16"}[args.inner]
+    out = {"dims": list(W["dims"]), "rhs": n, "solver": f"CGNE, {label} inner, FP64 defect correction, batched",
            "solves_per_s": round(n / t, 3), "ms_per_batch": round(t * 1e3, 2),
            "max_applications": max(i["iterations"] for i in infos), "worst_true_rel_residual": worst,
            "fp64_single_rhs_cgne_solves_per_s": round(1.0 / t64, 3), "fp64_single_rhs_applications": i64["iterations"],
@@ -434,6 +443,113 @@ def batched_config4(clg, ctx, stream, args, steps=2):
     s64.close()
     U.close()
     return out
+
+
+def uneven_lattices(clg, ctx, stream, args, steps=2):
+    """BASELINE config 4, second part: the uneven set 8^4, 12^4, 16^4, 16^3x32,
+    24^3x16 (442,624 sites), 4 complex Gaussian sources each.  Each lattice's
+    sources are one batched call (CGNE in the `--inner` precision, FP64 defect
+    correction); the five calls are issued back to back on the context stream.
+    Unit: one source solved to the true relative residual 1e-10."""
+    import torch
+
+    dims_set = [(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (16, 16, 16, 32), (24, 24, 24, 16)]
+    kappa, eps, seed, n = 0.1355, 0.25, 0xC1A60003, 4
+    inner = {"single": clg.SINGLE, "half": clg.HALF}[args.inner]
+    jobs = []
+    for d in dims_set:
+        lat = clg.Lattice(ctx, d)
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, seed, 1, eps)
+        b = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=n)
+        for r in range(n):
+            b.InitialField(clg.SOURCE_GAUSS, seed, 100 + r, rhs=r)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=n)
+        s = clg.CSLASolverCG(ctx, inner_precision=inner, tol_true_rel=TOL)
+        s.Solve(x, b, U, clg.EFO_F_D)  # warm-up (tuning, workspace, graphs)
+        jobs.append((lat, U, b, x, s))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    infos = []
+    for _ in range(steps):
+        infos = []
+        for lat, U, b, x, s in jobs:
+            infos += s.Solve(x, b, U, clg.EFO_F_D)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / steps
+    out = {"lattices": [list(d) for d in dims_set], "sites": sum(int(np.prod(d)) for d in dims_set),
+           "rhs_per_lattice": n, "solves_per_s": round(len(infos) / t, 3), "ms_per_set": round(t * 1e3, 2),
+           "worst_true_rel_residual": max(i["true_rel_residual"] for i in infos),
+           "max_applications": max(i["iterations"] for i in infos)}
+    for lat, U, b, x, s in jobs:
+        for f in (b, x):
+            f.close()
+        s.close()
+        U.close()
+    return out
+
+
+def dslash_config3(clg, ctx, stream):
+    """checkerboard Wilson hop on 48^3x24 (V = 2,654,208) in
+    FP64 (18-real links), FP32 (12-real) and FP16 (12-real FP16 links, FP16
+    spinors with a per-site FP32 norm); compulsory bytes per output site as in
+    hop_bytes_per_site, against the measured copy peak."""
+    peak, _ = peaks()
+    lat = clg.Lattice(ctx, (48, 48, 48, 24))
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60002, 1, 0.25)
+    Vh = lat.volume // 2
+    out = {"dims": [48, 48, 48, 24]}
+    for name, prec in (("fp64", clg.DOUBLE), ("fp32", clg.SINGLE), ("fp16", clg.HALF)):
+        t, _ = time_hops(clg, ctx, lat, U, prec, stream, reps=24)
+        gbs = hop_bytes_per_site(prec) * Vh / t / 1e9
+        out[name] = {"GB/s": round(gbs, 1), "frac": round(gbs / peak, 4), "GFLOP/s": round(1320 * Vh / t / 1e9, 1),
+                     "launch_us": round(t * 1e6, 2)}
+    U.close()
+    return out
+
+
+def staggered_config5(clg, ctx, stream, steps=2):
+    """32^3x16 staggered fermions, 2am = 0.02 (the reference's
+    `Mass` parameter is 2am), BC (+,+,+,-), 12 shifts sigma_k = 10^(-4 + 5k/11),
+    complex Gaussian source on the even sites; multi-shift CG on (DD^+)_ee + sigma_k
+    in FP32 with every shift refined to the FP64 true residual 1e-10.  Unit: all
+    12 shifts solved.  Baseline: the same multi-shift solve in FP64."""
+    import torch
+
+    lat = clg.Lattice(ctx, (32, 32, 32, 16))
+    m = 0.02
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60004, 1, 0.25)
+    b = clg.CFieldFermionKSSU3(lat, m, subset=clg.EVEN)
+    b.InitialField(clg.SOURCE_GAUSS, 0xC1A60004, 2)
+    shifts = [10.0 ** (-4 + 5 * k / 11) for k in range(12)]
+    xs = [clg.CFieldFermionKSSU3(lat, m, subset=clg.EVEN) for _ in shifts]
+    res = {}
+    for name, prec in (("mixed", clg.SINGLE), ("fp64", clg.DOUBLE)):
+        S = clg.CMultiShiftCG(ctx, inner_precision=prec, tol_true_rel=TOL)
+        S.Solve(xs, shifts, b, U, clg.OP_DDDAG_EE)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = steps if name == "mixed" else 1
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            infos = S.Solve(xs, shifts, b, U, clg.OP_DDDAG_EE)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        res[name] = {"units_per_s": round(1.0 / t, 3), "ms_per_unit": round(t * 1e3, 2),
+                     "worst_true_rel_residual": max(i["true_rel_residual"] for i in infos),
+                     "max_iterations": max(i["iterations"] for i in infos)}
+        S.close()
+    for f in xs + [b]:
+        f.close()
+    U.close()
+    return {"dims": [32, 32, 32, 16], "mass_2am": m, "shifts": len(shifts),
+            "solver": "multi-shift CG (Jegerlehner) FP32, per-shift FP64 refinement", **res,
+            "ratio_mixed_vs_fp64": round(res["fp64"]["ms_per_unit"] / res["mixed"]["ms_per_unit"], 2)}
 
 
 def cpu_baseline(U, lat, kappa, fp64_applications):
@@ -558,9 +674,12 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--quick", action="store_true", help="skip the per-precision and FP64 side measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--inner", default="single", choices=["single", "half"], help="inner Krylov precision")
+    ap.add_argument("--inner", default="half", choices=["single", "half"],
+                    help="inner Krylov precision (half: FP16 storage with a per-site FP32 norm, FP32 arithmetic)")
     ap.add_argument("--solver", default="cg", choices=["gmres", "cg"], help="inner Krylov method")
-    ap.add_argument("--no-batched", action="store_true", help="skip the batched config-4 side measurement")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched config-4 side measurements")
+    ap.add_argument("--no-side", action="store_true",
+                    help="skip the config-3 Dslash and config-5 staggered multi-shift side measurements")
     ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve"],
                     help="profiling driver (no JSON line): `--steps` hop launches on the workload lattice, "
                          "or `--steps` solves without warm-up")

@@ -251,4 +251,5 @@ struct clg_solver_s {
   clg_solver_params p;
   std::unique_ptr<clg::SolveCacheBase> cache;        // single-shift solves
   std::unique_ptr<clg::SolveCacheBase> cache_shift;  // multi-shift refinement
+  std::unique_ptr<clg::SolveCacheBase> cache_cgm;    // multi-shift CG vectors, state, graph
 };

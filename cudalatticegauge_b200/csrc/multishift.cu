@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "krylov.cuh"
@@ -31,6 +32,7 @@ struct CgmState {
   double zeta[CGM_MAXSHIFT], zeta_old[CGM_MAXSHIFT], zeta_new[CGM_MAXSHIFT];
   double alpha_k[CGM_MAXSHIFT], beta_k[CGM_MAXSHIFT];
   int active[CGM_MAXSHIFT];
+  int upd_x[CGM_MAXSHIFT];  // x_k takes alpha_k p_k in this iteration (active when alpha_k was formed)
 };
 
 namespace {
@@ -53,6 +55,9 @@ struct CgmAlpha {
   }
   __device__ void finalize(int, const double* s) const {
     CgmState& c = *st;
+    // runs on every replayed iteration, also once all shifts are done, so a
+    // finished solve never repeats its last x update
+    for (int k = 0; k < c.nshift; ++k) c.upd_x[k] = 0;
     if (c.done) return;
     c.iters += 1;
     if (!(s[0] > 0.0) || bad(s[0])) {
@@ -61,6 +66,7 @@ struct CgmAlpha {
     }
     const double alpha = c.rr / s[0];
     for (int k = 0; k < c.nshift; ++k) {
+      c.upd_x[k] = c.active[k];
       if (!c.active[k]) continue;
       const double zn = c.zeta[k], zo = c.zeta_old[k];
       const double den = alpha * c.beta * (zo - zn) + zo * c.alpha_old * (1.0 + c.shift[k] * alpha);
@@ -70,25 +76,6 @@ struct CgmAlpha {
     }
     c.alpha = alpha;
   }
-};
-
-// x_k += alpha_k p_k   (grid.y = shift)
-template <int P, int NC>
-struct CgmX {
-  DField x, pk;
-  CgmState* st;
-  __device__ bool active(int k) const { return !st->done && st->active[k]; }
-  __device__ void operator()(int k, int par, int64_t h, double*) const {
-    using AT = typename AccT<P>::T;
-    cpx<AT> vx[NC], vp[NC];
-    ldv<P, NC, AT>(x, k, par, h, vx);
-    ldv<P, NC, AT>(pk, k, par, h, vp);
-    const AT a = (AT)st->alpha_k[k];
-#pragma unroll
-    for (int i = 0; i < NC; ++i) vx[i] = vx[i] + a * vp[i];
-    stv<P, NC, AT>(x, k, par, h, vx);
-  }
-  __device__ void finalize(int, const double*) const {}
 };
 
 // r -= alpha q ; |r|^2 -> beta, beta_k, convergence per shift
@@ -135,40 +122,47 @@ struct CgmR {
   }
 };
 
-// p_k = zeta_k r + beta_k p_k   (grid.y = shift)
+// One pass after the residual update, grid.y = nshift + 1:
+//   shift k < nshift:  x_k += alpha_k p_k ; p_k = zeta_k r + beta_k p_k
+//                      (both from the same, old p_k: the x update of the
+//                      shift loop deferred past r's update, as the algebra allows)
+//   y = nshift:        p = r + beta p
 template <int P, int NC>
-struct CgmPk {
-  DField pk, r;
+struct CgmUpdate {
+  DField x, pk, p, r;
   CgmState* st;
-  __device__ bool active(int k) const { return !st->done && st->active[k]; }
+  int nshift;
+  __device__ bool active(int k) const {
+    if (k == nshift) return !st->done;
+    return st->upd_x[k] || (!st->done && st->active[k]);
+  }
   __device__ void operator()(int k, int par, int64_t h, double*) const {
     using AT = typename AccT<P>::T;
     cpx<AT> vp[NC], vr[NC];
+    ldv<P, NC, AT>(r, 0, par, h, vr);
+    if (k == nshift) {
+      ldv<P, NC, AT>(p, 0, par, h, vp);
+      const AT b = (AT)st->beta;
+#pragma unroll
+      for (int i = 0; i < NC; ++i) vp[i] = vr[i] + b * vp[i];
+      stv<P, NC, AT>(p, 0, par, h, vp);
+      return;
+    }
     ldv<P, NC, AT>(pk, k, par, h, vp);
-    ldv<P, NC, AT>(r, 0, par, h, vr);
-    const AT z = (AT)st->zeta[k], b = (AT)st->beta_k[k];
+    if (st->upd_x[k]) {
+      cpx<AT> vx[NC];
+      ldv<P, NC, AT>(x, k, par, h, vx);
+      const AT a = (AT)st->alpha_k[k];
 #pragma unroll
-    for (int i = 0; i < NC; ++i) vp[i] = z * vr[i] + b * vp[i];
-    stv<P, NC, AT>(pk, k, par, h, vp);
-  }
-  __device__ void finalize(int, const double*) const {}
-};
-
-// p = r + beta p
-template <int P, int NC>
-struct CgmP {
-  DField p, r;
-  CgmState* st;
-  __device__ bool active(int) const { return !st->done; }
-  __device__ void operator()(int, int par, int64_t h, double*) const {
-    using AT = typename AccT<P>::T;
-    cpx<AT> vp[NC], vr[NC];
-    ldv<P, NC, AT>(p, 0, par, h, vp);
-    ldv<P, NC, AT>(r, 0, par, h, vr);
-    const AT b = (AT)st->beta;
+      for (int i = 0; i < NC; ++i) vx[i] = vx[i] + a * vp[i];
+      stv<P, NC, AT>(x, k, par, h, vx);
+    }
+    if (!st->done && st->active[k]) {
+      const AT z = (AT)st->zeta[k], b = (AT)st->beta_k[k];
 #pragma unroll
-    for (int i = 0; i < NC; ++i) vp[i] = vr[i] + b * vp[i];
-    stv<P, NC, AT>(p, 0, par, h, vp);
+      for (int i = 0; i < NC; ++i) vp[i] = z * vr[i] + b * vp[i];
+      stv<P, NC, AT>(pk, k, par, h, vp);
+    }
   }
   __device__ void finalize(int, const double*) const {}
 };
@@ -204,6 +198,7 @@ struct CgmInit {
     for (int k = 0; k < c.nshift; ++k) {
       c.zeta[k] = c.zeta_old[k] = 1.0;
       c.active[k] = c.done ? 0 : 1;
+      c.upd_x[k] = 0;
     }
   }
 };
@@ -236,93 +231,115 @@ struct OwnedF {
   }
 };
 
-// Multi-shift CG in precision P on a Hermitian positive operator; X holds nshift rhs.
-clg_status cgm_run(clg_context_s* ctx, clg_gauge_s* U, int kind, double param, int op, const FieldRef& b,
-                   const FieldRef& X, const std::vector<double>& shifts, double tol, int max_iter, int* iters_out) {
+// Buffers, device state, pinned summary and the captured iteration graph of a
+// multi-shift CG, kept in the solver between calls with the same shape and
+// gauge arrays (a call then costs the solve, not cudaMalloc/cudaFree, pinned
+// allocations and a graph capture).
+struct CgmWork : SolveCacheBase {
+  std::string key;
+  OwnedF X, bP, r, p, q, pk, t_odd, t_full;
+  CgmState* st = nullptr;
+  CgmState* hs = nullptr;  // pinned copy read per chunk
+  cudaGraphExec_t exec = nullptr;
+  int64_t graph_kernels = 0;
+  ~CgmWork() {
+    if (exec) cudaGraphExecDestroy(exec);
+    dfree(st);
+    if (hs) cudaFreeHost(hs);
+  }
+  clg_status alloc(clg_context_s* ctx, int P, int nc, int np, int fp, int ns, int64_t Vh, int op) {
+    clg_status s;
+    if ((s = X.alloc(ctx, P, nc, np, fp, ns, Vh)) || (s = bP.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
+        (s = r.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = p.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
+        (s = q.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = pk.alloc(ctx, P, nc, np, fp, ns, Vh)) ||
+        (s = t_odd.alloc(ctx, P, nc, 1, 1, 1, Vh)))
+      return s;
+    if (op == CLG_OP_DDDAG && (s = t_full.alloc(ctx, P, nc, 2, 0, 1, Vh))) return s;
+    if ((s = dalloc(ctx, (void**)&st, sizeof(CgmState)))) return s;
+    if (cudaMallocHost((void**)&hs, sizeof(CgmState)) != cudaSuccess) {
+      hs = nullptr;
+      return ctx->fail(CLG_ERR_OOM, "multi-shift: pinned state");
+    }
+    return CLG_SUCCESS;
+  }
+};
+
+// Multi-shift CG in precision P on a Hermitian positive operator; W.X receives
+// the nshift solutions.
+clg_status cgm_run(clg_context_s* ctx, CgmWork& W, clg_gauge_s* U, int kind, double param, int op, const FieldRef& b,
+                   const std::vector<double>& shifts, double tol, int max_iter, int* iters_out) {
+  const FieldRef& X = W.X.ref;
   const int P = X.prec, nc = X.nc, np = b.nparity, fp = b.first_parity;
   const int64_t Vh = b.Vh;
   const int ns = (int)shifts.size();
-  OwnedF bP, r, p, q, pk, t_odd, t_full;
   clg_status s;
-  if ((s = bP.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = r.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
-      (s = p.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = q.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
-      (s = pk.alloc(ctx, P, nc, np, fp, ns, Vh)) || (s = t_odd.alloc(ctx, P, nc, 1, 1, 1, Vh)))
-    return s;
-  if (op == CLG_OP_DDDAG && (s = t_full.alloc(ctx, P, nc, 2, 0, 1, Vh))) return s;
-  if ((s = blas_copy(ctx, bP.ref, b))) return s;
-  CgmState* st = nullptr;
-  if ((s = dalloc(ctx, (void**)&st, sizeof(CgmState)))) return s;
+  if ((s = blas_copy(ctx, W.bP.ref, b))) return s;
+  CgmState* st = W.st;
   CgmState h;
   std::memset(&h, 0, sizeof(h));
   h.nshift = ns;
   h.tol2 = tol * tol;
   for (int k = 0; k < ns; ++k) h.shift[k] = shifts[k];
-  cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
+  if (cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+    return ctx->fail(CLG_ERR_CUDA, "multi-shift: state upload");
   const double2 one = make_double2(1, 0);
   const int* skip = &st->done;
-  s = with_pn(P, nc, [&](auto PP, auto NN) -> clg_status {
+  return with_pn(P, nc, [&](auto PP, auto NN) -> clg_status {
     constexpr int PV = PP.value, NV = NN.value;
-    clg_status e = launch_sites<1>(ctx, CgmInit<PV, NV>{dfield(bP.ref), dfield(r.ref), dfield(p.ref), dfield(X),
-                                                         dfield(pk.ref), st, ns},
+    clg_status e = launch_sites<1>(ctx, CgmInit<PV, NV>{dfield(W.bP.ref), dfield(W.r.ref), dfield(W.p.ref), dfield(X),
+                                                         dfield(W.pk.ref), st, ns},
                                    fp, np, Vh, 1);
     if (e) return e;
     const int chunk = 16;
-    cudaGraphExec_t exec = nullptr;
     auto body = [&]() -> clg_status {
       clg_status e2;
-      const FieldRef* tmp = (op == CLG_OP_DDDAG) ? &t_full.ref : &t_odd.ref;
-      if ((e2 = apply_op(ctx, op, U, kind, param, q.ref, p.ref, tmp, one, 1, nullptr, 0, skip, 0))) return e2;
-      if ((e2 = launch_sites<1>(ctx, CgmAlpha<PV, NV>{dfield(p.ref), dfield(q.ref), st}, fp, np, Vh, 1))) return e2;
-      if ((e2 = launch_sites<0>(ctx, CgmX<PV, NV>{dfield(X), dfield(pk.ref), st}, fp, np, Vh, ns))) return e2;
-      if ((e2 = launch_sites<1>(ctx, CgmR<PV, NV>{dfield(r.ref), dfield(q.ref), st}, fp, np, Vh, 1))) return e2;
-      if ((e2 = launch_sites<0>(ctx, CgmPk<PV, NV>{dfield(pk.ref), dfield(r.ref), st}, fp, np, Vh, ns))) return e2;
-      return launch_sites<0>(ctx, CgmP<PV, NV>{dfield(p.ref), dfield(r.ref), st}, fp, np, Vh, 1);
+      const FieldRef* tmp = (op == CLG_OP_DDDAG) ? &W.t_full.ref : &W.t_odd.ref;
+      if ((e2 = apply_op(ctx, op, U, kind, param, W.q.ref, W.p.ref, tmp, one, 1, nullptr, 0, skip, 0))) return e2;
+      if ((e2 = launch_sites<1>(ctx, CgmAlpha<PV, NV>{dfield(W.p.ref), dfield(W.q.ref), st}, fp, np, Vh, 1))) return e2;
+      if ((e2 = launch_sites<1>(ctx, CgmR<PV, NV>{dfield(W.r.ref), dfield(W.q.ref), st}, fp, np, Vh, 1))) return e2;
+      CgmUpdate<PV, NV> up{dfield(X), dfield(W.pk.ref), dfield(W.p.ref), dfield(W.r.ref), st, ns};
+      return launch_sites<0>(ctx, up, fp, np, Vh, ns + 1);
     };
     int done = 0, it = 0;
-    CgmState* hs = nullptr;
-    int64_t graph_kernels = 0;
-    if (cudaMallocHost((void**)&hs, sizeof(CgmState)) != cudaSuccess) return ctx->fail(CLG_ERR_OOM, "pinned");
     e = CLG_SUCCESS;
     for (int c = 0; c * chunk < max_iter + chunk; ++c) {
-      if (c == 1 && ctx->stream) {
+      // the first chunk of the first call runs eagerly (it tunes the launches);
+      // the second captures the chunk, later chunks and calls replay it
+      if (c == 1 && !W.exec && ctx->stream) {
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
           const int64_t k0 = ctx->kernels;  // captured launches are counted per replay
           for (int i = 0; i < chunk && !e; ++i) e = body();
-          graph_kernels = ctx->kernels - k0;
+          W.graph_kernels = ctx->kernels - k0;
           ctx->kernels = k0;
-          if (cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && g && !e) cudaGraphInstantiate(&exec, g, 0);
+          if (cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && g && !e) cudaGraphInstantiate(&W.exec, g, 0);
           if (g) cudaGraphDestroy(g);
           cudaGetLastError();
         }
       }
       if (e) break;
-      if (exec) {
-        if (cudaGraphLaunch(exec, ctx->stream) != cudaSuccess) {
+      if (W.exec) {
+        if (cudaGraphLaunch(W.exec, ctx->stream) != cudaSuccess) {
           e = ctx->fail(CLG_ERR_CUDA, "multi-shift graph launch");
           break;
         }
-        ctx->kernels += graph_kernels;
+        ctx->kernels += W.graph_kernels;
       } else {
         for (int i = 0; i < chunk && !e; ++i) e = body();
         if (e) break;
       }
-      if (cudaMemcpyAsync(hs, st, sizeof(CgmState), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+      if (cudaMemcpyAsync(W.hs, st, sizeof(CgmState), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
           cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         e = ctx->fail(CLG_ERR_CUDA, "multi-shift sync");
         break;
       }
-      done = hs->done;
-      it = hs->iters;
+      done = W.hs->done;
+      it = W.hs->iters;
       if (done || it >= max_iter) break;
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    cudaFreeHost(hs);
     *iters_out = it;
     return e;
   });
-  dfree(st);
-  return s;
 }
 
 }  // namespace
@@ -353,7 +370,7 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
   const int P = prm.inner_precision;
   const int nc = b->nc();
   const int64_t Vh = b->lat->g.Vh;
-  OwnedF X;
+  CgmWork* W = nullptr;
   int cgm_iters = 0;
   const bool use_cgm = S->p.kind == CLG_SOLVER_CGM;
   if (use_cgm) {
@@ -365,9 +382,31 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
     }
     if ((s = gauge_prepare(g, P))) return s;
     if (op == CLG_OP_MEE_MEEDAG) return ctx->fail(CLG_ERR_UNSUPPORTED, "CG-M on MEE_MEEDAG: use FOM_MS");
-    if ((s = X.alloc(ctx, P, nc, b->nparity(), 0, nshift, Vh))) return s;
-    const double itol = P == CLG_PREC_DOUBLE ? prm.tol_true_rel * 0.5 : std::max(prm.inner_tol, 1e-6);
-    if ((s = cgm_run(ctx, g, b->kind, b->param, op, b->ref(), X.ref, real, itol, prm.max_iterations, &cgm_iters)))
+    // workspace reused while lattice, kind, parity layout, precision, shift
+    // count, operator and the gauge arrays stay the same
+    const std::string key = std::to_string((uintptr_t)b->lat) + "/" + std::to_string(b->kind) + "/" +
+                            std::to_string(b->subset) + "/" + std::to_string(P) + "/" + std::to_string(nshift) + "/" +
+                            std::to_string(op) + "/" + std::to_string((uintptr_t)g) + "/" +
+                            std::to_string((uintptr_t)g->u64[0]) + "/" + std::to_string((uintptr_t)g->u32[0]) + "/" +
+                            std::to_string((uintptr_t)g->u16[0]) + "/" + std::to_string(b->param);
+    W = dynamic_cast<CgmWork*>(S->cache_cgm.get());
+    if (!W || W->key != key) {
+      cudaStreamSynchronize(ctx->stream);
+      S->cache_cgm.reset();
+      W = new CgmWork();
+      S->cache_cgm.reset(W);
+      if ((s = W->alloc(ctx, P, nc, b->nparity(), 0, nshift, Vh, op))) {
+        S->cache_cgm.reset();
+        return s;
+      }
+      W->key = key;
+    }
+    // recursive-residual target of the multi-shift phase: the FP64 tolerance
+    // itself in FP64; inner_tol (floored where the precision's recurrences
+    // stop tracking the true residual) in FP32 / FP16
+    const double itol = P == CLG_PREC_DOUBLE ? prm.tol_true_rel * 0.5
+                                             : std::max(prm.inner_tol, P == CLG_PREC_SINGLE ? 1e-9 : 1e-4);
+    if ((s = cgm_run(ctx, *W, g, b->kind, b->param, op, b->ref(), real, itol, prm.max_iterations, &cgm_iters)))
       return s;
     prm.kind = CLG_SOLVER_CG;  // per-shift refinement
   } else {
@@ -386,7 +425,7 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
   q.nrhs = nshift;
   q.b = b->ref();
   q.b_broadcast = true;
-  if (use_cgm) q.x0 = &X.ref;
+  if (use_cgm) q.x0 = &W->X.ref;
   q.shifts = sh.data();
   for (int k = 0; k < nshift; ++k) q.xout.push_back(x[k]->ref());
   q.info = info;
