@@ -21,6 +21,8 @@ template <int NRED, class F>
 __global__ void __launch_bounds__(256)
     site_reduce_kernel(F f, int64_t nsites, int first_parity, int64_t Vh, double* partials, unsigned* counter) {
   const int rhs = blockIdx.y;
+  pdl_launch_dependents();
+  pdl_wait();
   double acc[NRED > 0 ? NRED : 1];
 #pragma unroll
   for (int k = 0; k < (NRED > 0 ? NRED : 1); ++k) acc[k] = 0.0;
@@ -52,10 +54,8 @@ clg_status launch_sites(clg_context_s* ctx, const F& f, int first_parity, int np
     if (st) return st;
   }
   dim3 grid((unsigned)nb, (unsigned)nrhs);
-  site_reduce_kernel<NRED, F><<<grid, bs, 0, ctx->stream>>>(f, nsites, first_parity, Vh, ctx->red_partials,
-                                                           ctx->red_counter);
-  ctx->kernels++;
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(ctx, site_reduce_kernel<NRED, F>, grid, dim3(bs), 0, f, nsites, first_parity, Vh,
+                             ctx->red_partials, ctx->red_counter);
   if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("site kernel: ") + cudaGetErrorString(e));
   return CLG_SUCCESS;
 }

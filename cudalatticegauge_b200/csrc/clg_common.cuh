@@ -83,6 +83,20 @@ __device__ __forceinline__ int64_t site_index(const Geom& g, const int c[4]) {
                        (unsigned)g.L[3] + (unsigned)c[3]);
 }
 
+// ---------------------------------------------------------------- programmatic dependent launch
+// A kernel launched with programmatic stream serialization may start while
+// the previous kernel in the stream is still draining.  The hot kernels
+// (hops, site functors) therefore
+//   1. let their own dependents launch as soon as every one of their blocks
+//      has started (pdl_launch_dependents at block start), and
+//   2. call pdl_wait() -- a hardware wait for the previous grid's completion
+//      and memory flush -- before reading or writing anything that kernel
+//      may touch; only index arithmetic and reads of constant data (links,
+//      geometry) come before it.
+// Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------- errors
 #define CLG_CUDA_OK(expr)                                   \
   do {                                                      \

@@ -22,29 +22,15 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
     const int variant = cfg >> 16;
     dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
     if constexpr (P != P64) {
-      if (variant == 1) {
-        if (dagger)
-          wilson_hop_kernel<P, RECON, true, 256, 3><<<grid, bs, 0, ctx->stream>>>(a);
-        else
-          wilson_hop_kernel<P, RECON, false, 256, 3><<<grid, bs, 0, ctx->stream>>>(a);
-        ctx->kernels++;
-        return cudaGetLastError();
-      }
-      if (variant == 2 && bs == 64) {
-        if (dagger)
-          wilson_hop_kernel<P, RECON, true, 64, 14><<<grid, bs, 0, ctx->stream>>>(a);
-        else
-          wilson_hop_kernel<P, RECON, false, 64, 14><<<grid, bs, 0, ctx->stream>>>(a);
-        ctx->kernels++;
-        return cudaGetLastError();
-      }
+      if (variant == 1)
+        return dagger ? launch_pdl(ctx, wilson_hop_kernel<P, RECON, true, 256, 3>, grid, dim3(bs), 0, a)
+                      : launch_pdl(ctx, wilson_hop_kernel<P, RECON, false, 256, 3>, grid, dim3(bs), 0, a);
+      if (variant == 2 && bs == 64)
+        return dagger ? launch_pdl(ctx, wilson_hop_kernel<P, RECON, true, 64, 14>, grid, dim3(bs), 0, a)
+                      : launch_pdl(ctx, wilson_hop_kernel<P, RECON, false, 64, 14>, grid, dim3(bs), 0, a);
     }
-    if (dagger)
-      wilson_hop_kernel<P, RECON, true><<<grid, bs, 0, ctx->stream>>>(a);
-    else
-      wilson_hop_kernel<P, RECON, false><<<grid, bs, 0, ctx->stream>>>(a);
-    ctx->kernels++;
-    return cudaGetLastError();
+    return dagger ? launch_pdl(ctx, wilson_hop_kernel<P, RECON, true>, grid, dim3(bs), 0, a)
+                  : launch_pdl(ctx, wilson_hop_kernel<P, RECON, false>, grid, dim3(bs), 0, a);
   };
   if (ctx->hop_config >= 0) return go(ctx->hop_config);
   // __launch_bounds__(256, ...) caps the block at 256 threads
@@ -59,9 +45,7 @@ template <int P, int RECON>
 cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
   auto go = [&](int bs) {
     dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
-    staggered_hop_kernel<P, RECON><<<grid, bs, 0, ctx->stream>>>(a);
-    ctx->kernels++;
-    return cudaGetLastError();
+    return launch_pdl(ctx, staggered_hop_kernel<P, RECON>, grid, dim3(bs), 0, a);
   };
   return go(tune_block(ctx, key, idempotent(a), go));
 }

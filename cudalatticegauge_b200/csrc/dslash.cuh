@@ -93,6 +93,85 @@ __device__ __forceinline__ void wilson_hop_dir(cpx<AT> acc[12], const cpx<AT> ps
   }
 }
 
+// ---------------------------------------------------------------- FP16 arithmetic in half2 words
+// A word holds one complex number, real part in the low half.  Multiplying by
+// a phase i^Z is a swap of the halves and/or a sign-bit flip.
+__device__ __forceinline__ uint32_t h2_swap(uint32_t a) { return __byte_perm(a, 0, 0x1032); }
+template <int Z>
+__device__ __forceinline__ uint32_t h2_mul_i(uint32_t a) {
+  if constexpr ((Z & 3) == 0) return a;
+  if constexpr ((Z & 3) == 1) return h2_swap(a) ^ 0x00008000u;  // (-im, re)
+  if constexpr ((Z & 3) == 2) return a ^ 0x80008000u;           // (-re, -im)
+  return h2_swap(a) ^ 0x80000000u;                               // (im, -re)
+}
+__device__ __forceinline__ __half2 as_h2(uint32_t a) { return *reinterpret_cast<__half2*>(&a); }
+__device__ __forceinline__ uint32_t as_u32(__half2 a) { return *reinterpret_cast<uint32_t*>(&a); }
+// o + u * v   (UDAG: o + conj(u) * v), u given as its broadcast real / imaginary parts
+template <bool UDAG>
+__device__ __forceinline__ __half2 h2_cmac(__half2 ur, __half2 ui, uint32_t v, __half2 o) {
+  o = __hfma2(ur, as_h2(v), o);
+  return __hfma2(ui, as_h2(UDAG ? h2_mul_i<3>(v) : h2_mul_i<1>(v)), o);
+}
+
+// The FP16 counterpart of wilson_hop_dir: the spin projection, the third link
+// row (conj(row0 x row1)) and the two colour mat-vecs run on half2 words;
+// only the 6 projected products are converted, and they are accumulated in
+// FP32 with the factor s (boundary sign times the neighbour's site norm).
+template <int MU, int SGN, bool UDAG>
+__device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packed16& p, const PackedLink16& l,
+                                                 float s) {
+  constexpr int add = SGN < 0 ? 2 : 0;
+  uint32_t w[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    w[4 * k + 0] = p.c[k].x;
+    w[4 * k + 1] = p.c[k].y;
+    w[4 * k + 2] = p.c[k].z;
+    w[4 * k + 3] = p.c[k].w;
+  }
+  uint32_t h0[3], h1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    h0[c] = as_u32(__hadd2(as_h2(w[c]), as_h2(h2_mul_i<gz4(MU, 0) + add>(w[3 * gperm(MU, 0) + c]))));
+    h1[c] = as_u32(__hadd2(as_h2(w[3 + c]), as_h2(h2_mul_i<gz4(MU, 1) + add>(w[3 * gperm(MU, 1) + c]))));
+  }
+  uint32_t u[9] = {l.a.x, l.a.y, l.a.z, l.a.w, l.b.x, l.b.y, 0u, 0u, 0u};
+  {
+    // row2 = conj(row0 x row1): u6 = conj(u1 u5 - u2 u4), u7 = conj(u2 u3 - u0 u5), u8 = conj(u0 u4 - u1 u3)
+    const __half2 zero = __float2half2_rn(0.f);
+    auto cross = [&](int a, int b, int c, int d) -> uint32_t {
+      __half2 t = h2_cmac<false>(__low2half2(as_h2(u[a])), __high2half2(as_h2(u[a])), u[b], zero);
+      const uint32_t nd = u[d] ^ 0x80008000u;  // -u[d]
+      t = h2_cmac<false>(__low2half2(as_h2(u[c])), __high2half2(as_h2(u[c])), nd, t);
+      return as_u32(t) ^ 0x80000000u;  // conjugate
+    };
+    u[6] = cross(1, 5, 2, 4);
+    u[7] = cross(2, 3, 0, 5);
+    u[8] = cross(0, 4, 1, 3);
+  }
+  const __half2 zero = __float2half2_rn(0.f);
+  __half2 g0[3] = {zero, zero, zero}, g1[3] = {zero, zero, zero};
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      // U: row r, column k;  U^+: conj of row k, column r
+      const uint32_t e = UDAG ? u[3 * k + r] : u[3 * r + k];
+      const __half2 er = __low2half2(as_h2(e)), ei = __high2half2(as_h2(e));
+      g0[r] = h2_cmac<UDAG>(er, ei, h0[k], g0[r]);
+      g1[r] = h2_cmac<UDAG>(er, ei, h1[k], g1[r]);
+    }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float2 f0 = __half22float2(g0[c]), f1 = __half22float2(g1[c]);
+    const cpx<float> a0 = mk<float>(f0.x, f0.y), a1 = mk<float>(f1.x, f1.y);
+    acc[c] = cfma(s, a0, acc[c]);
+    acc[3 + c] = cfma(s, a1, acc[3 + c]);
+    acc[6 + c] = cfma(s, mul_i(gperm(MU, 2) == 0 ? a0 : a1, gz4(MU, 2) + add), acc[6 + c]);
+    acc[9 + c] = cfma(s, mul_i(gperm(MU, 3) == 0 ? a0 : a1, gz4(MU, 3) + add), acc[9 + c]);
+  }
+}
+
 struct NbrInfo {
   int hf[4], hb[4];   // checkerboard index of x+mu, x-mu (V < 2^31)
   float sf[4], sb[4]; // boundary signs
@@ -166,10 +245,11 @@ __device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64
   constexpr int SB = -SF;
   if constexpr (P == P16) {
     // FP16: both neighbours' packed data (19 registers each) are loaded before
-    // either is unpacked, so twice the bytes are in flight per thread.  The
-    // projection and the link product are linear, so the neighbour's site norm
-    // is applied with the boundary sign to the 6 projected products instead of
-    // to the 24 unpacked components.
+    // either is used, so twice the bytes are in flight per thread.  The spin
+    // projection, the third link row and the link products run on half2 words
+    // (wilson_hop_dir16); the projection and the link product are linear, so
+    // the neighbour's site norm is applied with the boundary sign to the 6
+    // projected products when they are accumulated in FP32.
 #define CLG_WILSON_DIR16(MU)                                                            \
   {                                                                                     \
     Packed16 pf, pb;                                                                    \
@@ -178,13 +258,8 @@ __device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64
     load_packed_link16(a.U_here, MU, Vh, h, lf);                                        \
     load_packed16(in, in_norm, Vh, nb.hb[MU], pb);                                      \
     load_packed_link16(a.U_there, MU, Vh, nb.hb[MU], lb);                               \
-    cpx<AT> psi[12], u[9];                                                              \
-    unpack16_raw(pf, psi);                                                              \
-    unpack_link16(lf, u);                                                               \
-    wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (AT)nb.sf[MU] * pf.n);               \
-    unpack16_raw(pb, psi);                                                              \
-    unpack_link16(lb, u);                                                               \
-    wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU] * pb.n);                \
+    wilson_hop_dir16<MU, SF, false>(acc, pf, lf, nb.sf[MU] * pf.n);                     \
+    wilson_hop_dir16<MU, SB, true>(acc, pb, lb, nb.sb[MU] * pb.n);                      \
   }
     CLG_WILSON_DIR16(0)
     CLG_WILSON_DIR16(1)
@@ -224,6 +299,8 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_kernel(HopArgs a) {
   // for the same sites run back to back and share the links through L2
   const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
   const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait();
   if (h >= a.g.Vh) return;
   if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
   cpx<AT> acc[12];
@@ -236,8 +313,9 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_kernel(HopArgs a) {
 //   E::NRED       doubles reduced over the grid per rhs, E::finalize(rhs, tot)
 //                 runs on the device in the last block (grid_reduce_finalize)
 //   E::site(rhs, h, acc, red)   per-site work on the result in registers
-// Every thread reaches the block reduction: out-of-range sites and skipped
-// right-hand sides contribute zero.
+// Every thread reaches the block reduction: out-of-range sites contribute
+// zero; a block of a skipped (finished) right-hand side only takes its ticket,
+// and E::finalize ignores such right-hand sides.
 template <int P, int RECON, bool DAGGER, int MAXT, int MINB, class E>
 __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E e, double* partials,
                                                                     unsigned* counter) {
@@ -245,17 +323,20 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E
   const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
   const unsigned slot = blockIdx.x / (unsigned)a.nrhs;
   const int64_t h = (int64_t)slot * blockDim.x + threadIdx.x;
-  const bool live = h < a.g.Vh && !(a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]);
+  pdl_launch_dependents();
+  pdl_wait();
+  const bool skipped = a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride];
   double red[E::NRED];
 #pragma unroll
   for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
-  if (live) {
+  if (!skipped && h < a.g.Vh) {
     cpx<AT> acc[12];
     wilson_hop_site<P, RECON, DAGGER>(a, rhs, h, acc);
     if constexpr (E::STORE) wilson_hop_store<P>(a, rhs, h, acc);
     e.site(rhs, h, acc, red);
   }
-  grid_reduce_finalize<E::NRED>(red, e, rhs, slot, gridDim.x / (unsigned)a.nrhs, a.nrhs, partials, counter);
+  grid_reduce_finalize<E::NRED>(red, e, rhs, slot, gridDim.x / (unsigned)a.nrhs, a.nrhs, partials, counter,
+                                !skipped);
 }
 
 template <int P, int RECON>
@@ -266,6 +347,8 @@ __global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
   // for the same sites run back to back and share the links through L2
   const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
   const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait();
   if (h >= Vh) return;
   if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;

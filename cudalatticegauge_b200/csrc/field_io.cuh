@@ -208,43 +208,12 @@ __device__ __forceinline__ void load_packed16(const void* __restrict__ base, con
   p.c[2] = __ldg(b + 2 * Vh + h);
   p.n = __ldg(nrm + h);
 }
-__device__ __forceinline__ void unpack16(const Packed16& p, cpx<float> v[12]) {
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    float2 f;
-    f = h2f(p.c[k].x); v[4 * k + 0] = mk<float>(p.n * f.x, p.n * f.y);
-    f = h2f(p.c[k].y); v[4 * k + 1] = mk<float>(p.n * f.x, p.n * f.y);
-    f = h2f(p.c[k].z); v[4 * k + 2] = mk<float>(p.n * f.x, p.n * f.y);
-    f = h2f(p.c[k].w); v[4 * k + 3] = mk<float>(p.n * f.x, p.n * f.y);
-  }
-}
-// the stored halves without the site norm (callers fold p.n into a later scale)
-__device__ __forceinline__ void unpack16_raw(const Packed16& p, cpx<float> v[12]) {
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    float2 f;
-    f = h2f(p.c[k].x); v[4 * k + 0] = mk<float>(f.x, f.y);
-    f = h2f(p.c[k].y); v[4 * k + 1] = mk<float>(f.x, f.y);
-    f = h2f(p.c[k].z); v[4 * k + 2] = mk<float>(f.x, f.y);
-    f = h2f(p.c[k].w); v[4 * k + 3] = mk<float>(f.x, f.y);
-  }
-}
 __device__ __forceinline__ void load_packed_link16(const void* __restrict__ base, int mu, int64_t Vh, int64_t h,
                                                    PackedLink16& l) {
   const uint4* b4 = reinterpret_cast<const uint4*>(base);
   const uint2* b2 = reinterpret_cast<const uint2*>(b4 + 4 * Vh);
   l.a = __ldg(b4 + (int64_t)mu * Vh + h);
   l.b = __ldg(b2 + (int64_t)mu * Vh + h);
-}
-__device__ __forceinline__ void unpack_link16(const PackedLink16& l, cpx<float> u[9]) {
-  float2 f;
-  f = h2f(l.a.x); u[0] = mk<float>(f.x, f.y);
-  f = h2f(l.a.y); u[1] = mk<float>(f.x, f.y);
-  f = h2f(l.a.z); u[2] = mk<float>(f.x, f.y);
-  f = h2f(l.a.w); u[3] = mk<float>(f.x, f.y);
-  f = h2f(l.b.x); u[4] = mk<float>(f.x, f.y);
-  f = h2f(l.b.y); u[5] = mk<float>(f.x, f.y);
-  reconstruct_row2(u);
 }
 
 // bytes of one parity's link array

@@ -6,6 +6,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/clg_b200.h"
@@ -81,6 +82,9 @@ struct clg_context_s {
   // CG on the Wilson normal equations fuses its vector work into the Schur
   // hops; CLG_FUSED_CG=0 runs the separate kernels instead
   bool fused_cg = true;
+  // hops and site kernels are launched with programmatic stream serialization
+  // (they overlap the previous kernel's drain); CLG_PDL=0 launches them plainly
+  bool pdl = true;
   clg_status fail(clg_status s, const std::string& msg) {
     last_error = msg;
     return s;
@@ -142,6 +146,30 @@ clg_status ensure_reduction(clg_context_s* ctx, int64_t doubles);
 
 // ------------------------------------------------------------ launch helpers
 bool stream_capturing(cudaStream_t s);
+
+// Launch a kernel that follows the pdl_launch_dependents / pdl_wait protocol
+// (clg_common.cuh) on the context stream, with programmatic stream
+// serialization when the context allows it.  Counts the launch.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(clg_context_s* ctx, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       Args&&... args) {
+  ctx->kernels++;
+  if (!ctx->pdl) {
+    kernel<<<grid, block, smem, ctx->stream>>>(std::forward<Args>(args)...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 // Autotuner: the launch configuration for kernel variant `key`.  On first use
 // (outside stream capture, when the launch is idempotent) each candidate
 // (a block size, optionally combined with a register-capped kernel variant) is

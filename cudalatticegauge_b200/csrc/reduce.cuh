@@ -13,38 +13,15 @@
 
 namespace clg {
 
-// blocks of at most 256 threads (8 warps)
+// The last block's part: totals per right-hand side -> f.finalize.  Called by
+// every thread of that block (at most 256 threads, 8 warps).
 template <int NRED, class F>
-__device__ __forceinline__ void grid_reduce_finalize(double (&acc)[NRED], const F& f, int rhs, unsigned slot,
-                                                     unsigned nslots, int nrhs, double* partials, unsigned* counter) {
+__device__ __forceinline__ void grid_final_reduce(const F& f, unsigned nslots, int nrhs, const double* partials,
+                                                  unsigned* counter) {
   __shared__ double sm[NRED][8];
   __shared__ double tot[NRED];
-  __shared__ bool last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-  for (int k = 0; k < NRED; ++k) {
-    double v = acc[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) sm[k][warp] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < NRED) {
-    double v = 0.0;
-    for (int w = 0; w < nw; ++w) v += sm[threadIdx.x][w];
-    partials[((int64_t)rhs * nslots + slot) * NRED + threadIdx.x] = v;
-    // only the partials must be visible to the last block before the ticket
-    __threadfence();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned t = atomicAdd(counter, 1u);
-    last = (t == nslots * (unsigned)nrhs - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
   // U independent partial loads in flight per thread and step (fixed order)
   constexpr int U = NRED >= 8 ? 1 : 8 / NRED;
   for (int r = 0; r < nrhs; ++r) {
@@ -83,6 +60,46 @@ __device__ __forceinline__ void grid_reduce_finalize(double (&acc)[NRED], const 
     __syncthreads();
   }
   if (threadIdx.x == 0) *counter = 0u;
+}
+
+// Block partials + ticket + (last block) final reduction.  `contribute` must be
+// uniform over the block: a block that does not contribute (its right-hand
+// side is finished) writes no partial and only takes its ticket, so the caller's
+// finalize must ignore the totals of such right-hand sides.
+template <int NRED, class F>
+__device__ __forceinline__ void grid_reduce_finalize(double (&acc)[NRED], const F& f, int rhs, unsigned slot,
+                                                     unsigned nslots, int nrhs, double* partials, unsigned* counter,
+                                                     bool contribute = true) {
+  __shared__ double sm[NRED][8];
+  __shared__ bool last;
+  if (contribute) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) {
+      double v = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) sm[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NRED) {
+      double v = 0.0;
+      for (int w = 0; w < nw; ++w) v += sm[threadIdx.x][w];
+      partials[((int64_t)rhs * nslots + slot) * NRED + threadIdx.x] = v;
+      // only the partials must be visible to the last block before the ticket
+      __threadfence();
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(counter, 1u);
+    last = (t == nslots * (unsigned)nrhs - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  grid_final_reduce<NRED>(f, nslots, nrhs, partials, counter);
 }
 
 }  // namespace clg

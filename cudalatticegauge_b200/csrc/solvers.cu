@@ -406,10 +406,8 @@ template <int P, int RECON, bool DAG, class E>
 cudaError_t launch_hop_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int bs) {
   dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * a.nrhs));
   constexpr int MINB = P == P64 ? 1 : 3;
-  wilson_hop_epi_kernel<P, RECON, DAG, 256, MINB, E>
-      <<<grid, bs, 0, ctx->stream>>>(a, e, ctx->red_partials, ctx->red_counter);
-  ctx->kernels++;
-  return cudaGetLastError();
+  return launch_pdl(ctx, wilson_hop_epi_kernel<P, RECON, DAG, 256, MINB, E>, grid, dim3(bs), 0, a, e,
+                    ctx->red_partials, ctx->red_counter);
 }
 
 // out_e = in_e - kappa^2 H_eo^(dag) t_o with epilogue e (E::STORE decides
