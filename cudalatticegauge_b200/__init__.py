@@ -90,6 +90,9 @@ SIGNATURES = [
     ("clg_field_set_param", _S, [_P, _D]),
     ("clg_field_import", _S, [_P, _I, _P, _I]),
     ("clg_field_export", _S, [_P, _I, _P, _I]),
+    ("clg_field_import_async", _S, [_P, _I, _P]),
+    ("clg_field_export_async", _S, [_P, _I, _P]),
+    ("clg_field_wait", _S, [_P]),
     ("clg_field_random", _S, [_P, _I, _I, _U64, _U32, _I64, _I]),
     ("clg_field_copy", _S, [_P, _P]),
     ("clg_apply", _S, [_I, _P, _P, _I, _D, _D]),
@@ -251,6 +254,25 @@ class _FermionField:
             raise CLGError(ERR_BAD_ARG, "export buffer has the wrong size or type")
         self.ctx.check(self.ctx.lib.clg_field_export(self.h, rhs, _ptr(out), 0), "clg_field_export")
         return out
+
+    # asynchronous transfers (clg_field_import_async / export_async / wait): the
+    # arrays should be pinned (e.g. torch.empty(..., pin_memory=True).numpy())
+    # and are kept alive here until wait()
+    def from_numpy_async(self, data: np.ndarray, rhs: int = 0):
+        if data.dtype != np.complex128 or data.size != self.lat.volume * self.NC or not data.flags["C_CONTIGUOUS"]:
+            raise CLGError(ERR_BAD_ARG, "import buffer has the wrong size or type")
+        self.ctx.check(self.ctx.lib.clg_field_import_async(self.h, rhs, _ptr(data)), "clg_field_import_async")
+        self._inflight = getattr(self, "_inflight", []) + [data]
+
+    def to_numpy_async(self, out: np.ndarray, rhs: int = 0):
+        if out.dtype != np.complex128 or out.size != self.lat.volume * self.NC or not out.flags["C_CONTIGUOUS"]:
+            raise CLGError(ERR_BAD_ARG, "export buffer has the wrong size or type")
+        self.ctx.check(self.ctx.lib.clg_field_export_async(self.h, rhs, _ptr(out)), "clg_field_export_async")
+        self._inflight = getattr(self, "_inflight", []) + [out]
+
+    def wait(self):
+        self.ctx.check(self.ctx.lib.clg_field_wait(self.h), "clg_field_wait")
+        self._inflight = []
 
     def InitialField(self, kind: int, seed: int = 0, field_id: int = 2, rhs: int = 0, site: int = 0, comp: int = 0):
         self.ctx.check(self.ctx.lib.clg_field_random(self.h, rhs, kind, seed, field_id, site, comp), "clg_field_random")

@@ -42,6 +42,47 @@ void dfree(void* p) {
   if (p) cudaFree(p);
 }
 
+// bytes of one right-hand side of a host (FP64 lexicographic) field array
+static size_t host_rhs_bytes(const clg_field_s* f) { return (size_t)f->lat->g.V * f->nc() * 2 * sizeof(double); }
+
+// copy stream, staging slots and events of the asynchronous transfers
+static clg_status xfer_prepare(clg_field_s* f, bool import) {
+  clg_context_s* ctx = f->lat->ctx;
+  if (!ctx->copy_stream && cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    ctx->copy_stream = nullptr;
+    return ctx->fail(CLG_ERR_CUDA, "copy stream");
+  }
+  void*& buf = import ? f->xin : f->xout;
+  if (!buf)
+    if (clg_status st = dalloc(ctx, &buf, host_rhs_bytes(f) * f->nrhs)) return st;
+  auto make = [&](std::vector<cudaEvent_t>& v) -> bool {
+    if (!v.empty()) return true;
+    v.assign(f->nrhs, nullptr);
+    for (auto& e : v)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+    return true;
+  };
+  const bool ok = import ? (make(f->in_copied) && make(f->in_consumed)) : (make(f->out_ready) && make(f->out_copied));
+  if (!ok) return ctx->fail(CLG_ERR_CUDA, "transfer events");
+  if (import && f->in_pending.empty()) f->in_pending.assign(f->nrhs, 0);
+  return CLG_SUCCESS;
+}
+
+clg_status settle(clg_field_s* f) {
+  if (f->in_pending.empty()) return CLG_SUCCESS;
+  clg_context_s* ctx = f->lat->ctx;
+  for (int r = 0; r < f->nrhs; ++r) {
+    if (!f->in_pending[r]) continue;
+    f->in_pending[r] = 0;
+    if (cudaStreamWaitEvent(ctx->stream, f->in_copied[r], 0) != cudaSuccess)
+      return ctx->fail(CLG_ERR_CUDA, "import: wait for the copy");
+    double* slot = reinterpret_cast<double*>(static_cast<char*>(f->xin) + r * host_rhs_bytes(f));
+    if (clg_status st = field_reorder(f, r, slot, 1)) return st;
+    if (cudaEventRecord(f->in_consumed[r], ctx->stream) != cudaSuccess) return ctx->fail(CLG_ERR_CUDA, "import event");
+  }
+  return CLG_SUCCESS;
+}
+
 static clg_status staging_buffer(clg_context_s* ctx, size_t bytes, double** p) {
   if (bytes > ctx->staging_bytes) {
     if (ctx->staging) {
@@ -298,6 +339,10 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
 clg_status clg_context_destroy(clg_context ctx) {
   if (!ctx) return CLG_ERR_BAD_ARG;
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
   dfree(ctx->red_partials);
   dfree(ctx->red_counter);
   dfree(ctx->staging);
@@ -497,7 +542,14 @@ clg_status clg_field_create(clg_lattice lat, int kind, int subset, int precision
 
 clg_status clg_field_destroy(clg_field f) {
   if (!f) return CLG_ERR_BAD_ARG;
-  cudaStreamSynchronize(f->lat->ctx->stream);
+  clg_context_s* ctx = f->lat->ctx;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  for (auto* v : {&f->in_copied, &f->in_consumed, &f->out_ready, &f->out_copied})
+    for (cudaEvent_t e : *v)
+      if (e) cudaEventDestroy(e);
+  dfree(f->xin);
+  dfree(f->xout);
   dfree(f->data);
   dfree(f->norm);
   delete f;
@@ -512,6 +564,7 @@ clg_status clg_field_set_param(clg_field f, double param) {
 
 clg_status clg_field_import(clg_field f, int rhs, const double* data, int on_device) {
   if (!f || !data || rhs < 0 || rhs >= f->nrhs) return CLG_ERR_BAD_ARG;
+  if (clg_status st = settle(f)) return st;
   clg_context_s* ctx = f->lat->ctx;
   const size_t bytes = (size_t)f->lat->g.V * f->nc() * 2 * sizeof(double);
   double* buf = nullptr;
@@ -532,6 +585,7 @@ clg_status clg_field_import(clg_field f, int rhs, const double* data, int on_dev
 
 clg_status clg_field_export(clg_field f, int rhs, double* data, int on_device) {
   if (!f || !data || rhs < 0 || rhs >= f->nrhs) return CLG_ERR_BAD_ARG;
+  if (clg_status st = settle(f)) return st;
   clg_context_s* ctx = f->lat->ctx;
   const size_t bytes = (size_t)f->lat->g.V * f->nc() * 2 * sizeof(double);
   double* buf = nullptr;
@@ -555,13 +609,61 @@ clg_status clg_field_export(clg_field f, int rhs, double* data, int on_device) {
 clg_status clg_field_random(clg_field f, int rhs, int kind, uint64_t seed, uint32_t field_id, int64_t site, int comp) {
   if (!f || rhs < 0 || rhs >= f->nrhs || kind < 0 || kind > 3) return CLG_ERR_BAD_ARG;
   if (kind == CLG_SOURCE_POINT && (site < 0 || site >= f->lat->g.V || comp < 0 || comp >= f->nc())) return CLG_ERR_BAD_ARG;
+  if (clg_status st = settle(f)) return st;
   return field_source(f, rhs, kind, seed, field_id, site, comp);
+}
+
+clg_status clg_field_import_async(clg_field f, int rhs, const double* data) {
+  if (!f || !data || rhs < 0 || rhs >= f->nrhs) return CLG_ERR_BAD_ARG;
+  clg_context_s* ctx = f->lat->ctx;
+  if (clg_status st = xfer_prepare(f, true)) return st;
+  const size_t bytes = host_rhs_bytes(f);
+  char* slot = static_cast<char*>(f->xin) + rhs * bytes;
+  // the slot is overwritten only after the last reorder out of it
+  cudaError_t e = cudaStreamWaitEvent(ctx->copy_stream, f->in_consumed[rhs], 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(slot, data, bytes, cudaMemcpyHostToDevice, ctx->copy_stream);
+  if (e == cudaSuccess) e = cudaEventRecord(f->in_copied[rhs], ctx->copy_stream);
+  if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("import_async: ") + cudaGetErrorString(e));
+  f->in_pending[rhs] = 1;
+  return CLG_SUCCESS;
+}
+
+clg_status clg_field_export_async(clg_field f, int rhs, double* data) {
+  if (!f || !data || rhs < 0 || rhs >= f->nrhs) return CLG_ERR_BAD_ARG;
+  clg_context_s* ctx = f->lat->ctx;
+  if (clg_status st = settle(f)) return st;
+  if (clg_status st = xfer_prepare(f, false)) return st;
+  const size_t bytes = host_rhs_bytes(f);
+  double* slot = reinterpret_cast<double*>(static_cast<char*>(f->xout) + rhs * bytes);
+  // the slot is refilled only after its last copy to the host
+  cudaError_t e = cudaStreamWaitEvent(ctx->stream, f->out_copied[rhs], 0);
+  if (e != cudaSuccess) return ctx->fail(cuda_status(e), "export_async: wait");
+  if (clg_status st = field_reorder(f, rhs, slot, 0)) return st;
+  e = cudaEventRecord(f->out_ready[rhs], ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, f->out_ready[rhs], 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(data, slot, bytes, cudaMemcpyDeviceToHost, ctx->copy_stream);
+  if (e == cudaSuccess) e = cudaEventRecord(f->out_copied[rhs], ctx->copy_stream);
+  if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("export_async: ") + cudaGetErrorString(e));
+  return CLG_SUCCESS;
+}
+
+clg_status clg_field_wait(clg_field f) {
+  if (!f) return CLG_ERR_BAD_ARG;
+  clg_context_s* ctx = f->lat->ctx;
+  for (auto* v : {&f->in_copied, &f->out_copied})
+    for (cudaEvent_t ev : *v) {
+      const cudaError_t e = cudaEventSynchronize(ev);
+      if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("field wait: ") + cudaGetErrorString(e));
+    }
+  return CLG_SUCCESS;
 }
 
 clg_status clg_field_copy(clg_field dst, clg_field src) {
   if (!dst || !src || dst->lat != src->lat || dst->kind != src->kind || dst->subset != src->subset ||
       dst->nrhs != src->nrhs)
     return CLG_ERR_BAD_ARG;
+  if (clg_status st = settle(dst)) return st;
+  if (clg_status st = settle(src)) return st;
   return blas_copy(dst->lat->ctx, dst->ref(), src->ref());
 }
 
@@ -588,6 +690,7 @@ static bool op_on_even(int op) { return op == CLG_OP_MEE || op == CLG_OP_MEE_DAG
 clg_status clg_apply_to(int op, clg_field out, clg_field in, clg_gauge g, int coeff_type, double cre, double cim) {
   clg_status st = check_pair(out, in, g);
   if (st) return st;
+  if ((st = settle(out)) || (st = settle(in))) return st;
   clg_context_s* ctx = in->lat->ctx;
   if (op < 0 || op > CLG_OP_DDDAG_EE) return ctx->fail(CLG_ERR_BAD_ARG, "unknown operator");
   if (op_on_even(op)) {
@@ -661,6 +764,8 @@ clg_status clg_dot(clg_field a, clg_field b, double* re_im) {
   if (!a || !b || !re_im || a->lat != b->lat || a->kind != b->kind || a->subset != b->subset || a->nrhs != b->nrhs ||
       a->prec != b->prec)
     return CLG_ERR_BAD_ARG;
+  if (clg_status st = settle(a)) return st;
+  if (clg_status st = settle(b)) return st;
   clg_context_s* ctx = a->lat->ctx;
   double* d = nullptr;
   clg_status st = dalloc(ctx, (void**)&d, sizeof(double) * 2 * a->nrhs);
@@ -685,19 +790,24 @@ clg_status clg_axpy(clg_field y, double are, double aim, clg_field x) {
   if (!y || !x || y->lat != x->lat || y->kind != x->kind || y->subset != x->subset || y->nrhs != x->nrhs ||
       y->prec != x->prec)
     return CLG_ERR_BAD_ARG;
-  clg_status st = blas_axpby(y->lat->ctx, y->ref(), make_double2(are, aim), x->ref(), make_double2(1, 0));
+  clg_status st = settle(y);
+  if (!st) st = settle(x);
+  if (st) return st;
+  st = blas_axpby(y->lat->ctx, y->ref(), make_double2(are, aim), x->ref(), make_double2(1, 0));
   return st ? st : sync_status(y->lat->ctx);
 }
 
 clg_status clg_scale(clg_field y, double are, double aim) {
   if (!y) return CLG_ERR_BAD_ARG;
-  clg_status st = blas_axpby(y->lat->ctx, y->ref(), make_double2(0, 0), y->ref(), make_double2(are, aim));
+  clg_status st = settle(y);
+  if (!st) st = blas_axpby(y->lat->ctx, y->ref(), make_double2(0, 0), y->ref(), make_double2(are, aim));
   return st ? st : sync_status(y->lat->ctx);
 }
 
 clg_status clg_zero(clg_field y) {
   if (!y) return CLG_ERR_BAD_ARG;
-  clg_status st = blas_zero(y->lat->ctx, y->ref());
+  clg_status st = settle(y);
+  if (!st) st = blas_zero(y->lat->ctx, y->ref());
   return st ? st : sync_status(y->lat->ctx);
 }
 

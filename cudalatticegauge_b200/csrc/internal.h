@@ -73,6 +73,8 @@ struct clg_context_s {
   // two copies and a reorder, not a cudaMalloc/cudaFree pair.
   void* staging = nullptr;
   size_t staging_bytes = 0;
+  // stream of the asynchronous host transfers (created on first use)
+  cudaStream_t copy_stream = nullptr;
   // block size chosen per kernel variant by the autotuner
   std::map<std::string, int> tuned;
   bool tuning_enabled = true;
@@ -118,6 +120,15 @@ struct clg_field_s {
   char* data = nullptr;
   float* norm = nullptr;
   int64_t blk = 0;
+  // asynchronous host transfers: FP64 lexicographic staging per rhs, and per
+  // rhs the events that order the copy stream against the context stream
+  void* xin = nullptr;                       // import staging (nrhs slots)
+  void* xout = nullptr;                      // export staging (nrhs slots)
+  std::vector<cudaEvent_t> in_copied;        // H2D of a slot finished (copy stream)
+  std::vector<cudaEvent_t> in_consumed;      // reorder out of a slot finished (context stream)
+  std::vector<cudaEvent_t> out_ready;        // reorder into a slot finished (context stream)
+  std::vector<cudaEvent_t> out_copied;       // D2H of a slot finished (copy stream)
+  std::vector<char> in_pending;              // slot copied but not yet reordered into the field
   int nparity() const { return subset == CLG_SUBSET_FULL ? 2 : 1; }
   int nc() const { return kind == CLG_FERMION_WILSON ? 12 : 3; }
   clg::FieldRef ref() const {
@@ -138,6 +149,10 @@ struct clg_field_s {
 };
 
 namespace clg {
+
+// Queue the pending asynchronous imports of f on the context stream (every
+// entry point that takes a field calls it before using the field).
+clg_status settle(clg_field_s* f);
 
 // ------------------------------------------------------------ device allocation
 clg_status dalloc(clg_context_s* ctx, void** p, size_t bytes);

@@ -360,6 +360,9 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
       return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift: solution fields must match b");
     if (x[k]->data == b->data) return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift: x must not alias b (CMultiShiftSolver.h:35)");
   }
+  if (clg_status st = settle(b)) return st;
+  for (int k = 0; k < nshift; ++k)
+    if (clg_status st = settle(x[k])) return st;
   if (S->p.kind != CLG_SOLVER_CGM && S->p.kind != CLG_SOLVER_FOM_MS)
     return ctx->fail(CLG_ERR_BAD_ARG, "clg_solve_multishift needs a CGM or FOM_MS solver");
   std::vector<double2> sh(nshift);
@@ -439,6 +442,7 @@ clg_status clg_rational_apply(clg_solver S, clg_field f, clg_gauge g, int op, in
   if (!S || !f || !g || !a || !bsh || !info || degree < 1) return CLG_ERR_BAD_ARG;
   clg_context_s* ctx = S->ctx;
   if (f->nrhs != 1) return ctx->fail(CLG_ERR_BAD_ARG, "rational approximation acts on one field");
+  if (clg_status st = settle(f)) return st;
   std::vector<clg_field> xs(degree, nullptr);
   clg_status s = CLG_SUCCESS;
   for (int i = 0; i < degree && !s; ++i) s = clg_field_create(f->lat, f->kind, f->subset, f->prec, 1, f->param, &xs[i]);

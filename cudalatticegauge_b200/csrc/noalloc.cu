@@ -88,6 +88,9 @@ extern "C" clg_status clg_dot_noalloc(clg_field a, clg_field b, double* re_im) {
   if (!a || !b || !re_im || a->lat != b->lat || a->kind != b->kind || a->subset != b->subset || a->nrhs != b->nrhs ||
       a->prec != b->prec)
     return CLG_ERR_BAD_ARG;
+  // pending asynchronous imports are reordered from their own staging (no allocation)
+  if (clg_status st = clg::settle(a)) return st;
+  if (clg_status st = clg::settle(b)) return st;
   clg_context_s* ctx = a->lat->ctx;
   const int nrhs = a->nrhs;
   if (nrhs > kMaxRhs)

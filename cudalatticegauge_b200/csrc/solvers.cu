@@ -677,6 +677,9 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
     return ctx->fail(CLG_ERR_BAD_ARG, "solve: field shapes differ");
   if (S->p.kind == CLG_SOLVER_CGM || S->p.kind == CLG_SOLVER_FOM_MS)
     return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift solvers are called through clg_solve_multishift");
+  for (clg_field f : {X, B, X0})
+    if (f)
+      if (clg_status st = settle(f)) return st;
   SolveReq q;
   q.cache = &S->cache;
   q.ctx = ctx;

@@ -131,6 +131,24 @@ clg_status clg_field_destroy(clg_field f);
 clg_status clg_field_set_param(clg_field f, double param);
 clg_status clg_field_import(clg_field f, int rhs, const double* data, int on_device);
 clg_status clg_field_export(clg_field f, int rhs, double* data, int on_device);
+/* Asynchronous host transfers (no reference counterpart: the reference copies
+ * synchronously, CFieldFermionWilsonSquareSU3.cu InitialFieldWithFile /
+ * CopyDataOut).  They let a caller overlap the PCIe copies of one solve's
+ * source and solution with the next solve; `data` should be pinned host memory.
+ *
+ * clg_field_import_async: the host-to-device copy starts at once on the
+ * context's copy stream; the field takes the data before the next operation
+ * that uses it (any call taking the field), which waits for the copy.  `data`
+ * must stay unchanged until clg_field_wait(f) or that operation returns.
+ *
+ * clg_field_export_async: queued on the context stream after the work issued
+ * so far (the field's current value), copied to `data` on the copy stream;
+ * `data` is complete once clg_field_wait(f) returns.
+ *
+ * clg_field_wait: waits for every asynchronous transfer of f issued so far. */
+clg_status clg_field_import_async(clg_field f, int rhs, const double* data);
+clg_status clg_field_export_async(clg_field f, int rhs, double* data);
+clg_status clg_field_wait(clg_field f);
 /* InitialField / InitialAsSource (CFieldFermionWilsonSquareSU3.cu:1102-1136, :521-566):
  * GAUSS (E|z|^2 = 1), Z2 ((+-1 +- i)/sqrt 2), POINT (site, spin*3+colour), ZERO. */
 clg_status clg_field_random(clg_field f, int rhs, int kind, uint64_t seed, uint32_t field_id, int64_t site, int comp);
