@@ -139,7 +139,7 @@ clg_status clg_field_export(clg_field f, int rhs, double* data, int on_device);
  * clg_field_import_async: the host-to-device copy starts at once on the
  * context's copy stream; the field takes the data before the next operation
  * that uses it (any call taking the field), which waits for the copy.  `data`
- * must stay unchanged until clg_field_wait(f) or that operation returns.
+ * must stay unchanged until clg_field_wait(f) returns.
  *
  * clg_field_export_async: queued on the context stream after the work issued
  * so far (the field's current value), copied to `data` on the copy stream;
