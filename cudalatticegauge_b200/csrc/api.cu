@@ -306,6 +306,10 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   clg_context_s* ctx = new clg_context_s();
   ctx->device = device;
   ctx->num_sms = prop.multiProcessorCount;
+  ctx->max_window = prop.accessPolicyMaxWindowSize > 0 ? (size_t)prop.accessPolicyMaxWindowSize : 0;
+  ctx->max_persist = prop.persistingL2CacheMaxSize > 0 ? (size_t)prop.persistingL2CacheMaxSize : 0;
+  ctx->l2_bytes = prop.l2CacheSize > 0 ? (size_t)prop.l2CacheSize : 0;
+  if (const char* t = std::getenv("CLG_L2_WINDOW")) ctx->l2_window = t[0] != '0';
   // CLG_AUTOTUNE=0 keeps the default block size (reproducible profiling runs)
   if (const char* t = std::getenv("CLG_AUTOTUNE")) ctx->tuning_enabled = t[0] != '0';
   if (const char* t = std::getenv("CLG_FUSED_CG")) ctx->fused_cg = t[0] != '0';
@@ -342,6 +346,11 @@ clg_status clg_context_destroy(clg_context ctx) {
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);
+  }
+  if (ctx->persist_set) {  // give the persisting L2 carve-out back
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    cudaGetLastError();
   }
   dfree(ctx->red_partials);
   dfree(ctx->red_counter);
@@ -437,11 +446,9 @@ clg_status clg_gauge_create(clg_lattice lat, clg_gauge* out) {
 clg_status clg_gauge_destroy(clg_gauge g) {
   if (!g) return CLG_ERR_BAD_ARG;
   cudaStreamSynchronize(g->lat->ctx->stream);
-  for (int p = 0; p < 2; ++p) {
-    dfree(g->u64[p]);
-    dfree(g->u32[p]);
-    dfree(g->u16[p]);
-  }
+  for (int p = 0; p < 2; ++p) dfree(g->u64[p]);
+  dfree(g->u32[0]);  // one allocation holds both parities of a low-precision copy
+  dfree(g->u16[0]);
   delete g;
   return CLG_SUCCESS;
 }

@@ -87,6 +87,10 @@ struct clg_context_s {
   // hops and site kernels are launched with programmatic stream serialization
   // (they overlap the previous kernel's drain); CLG_PDL=0 launches them plainly
   bool pdl = true;
+  // solves keep the low-precision link copy in a persisting L2 window
+  // (CLG_L2_WINDOW=0 turns it off); device limits queried at creation
+  bool l2_window = true;
+  size_t max_window = 0, max_persist = 0, persist_set = 0, l2_bytes = 0;
   clg_status fail(clg_status s, const std::string& msg) {
     last_error = msg;
     return s;
@@ -242,6 +246,20 @@ clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec
 // block size the autotuner chose for this hop (fallback if not tuned yet)
 int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
 clg_status gauge_prepare(clg_gauge_s* U, int prec);  // builds the FP32 / FP16 copies on first use
+// address range of the link copy the hops of precision `prec` read (nullptr, 0 if none)
+void gauge_link_range(const clg_gauge_s* U, int prec, const void** base, size_t* bytes);
+
+// While alive, the link copy of precision `prec` is a persisting L2 access
+// window on the context stream (kernels and captured graph nodes launched on
+// it keep those lines resident), so streaming traffic -- the solve's own
+// vectors, or copy-engine transfers of neighbouring steps -- does not evict
+// the links every hop reads.
+struct L2LinkWindow {
+  clg_context_s* ctx;
+  bool set = false;
+  L2LinkWindow(clg_context_s* c, const clg_gauge_s* U, int prec);
+  ~L2LinkWindow();
+};
 
 // ------------------------------------------------------------ operator composition (api.cu)
 // out = coeff * op(in) on fields of one precision. tmp: scratch with at least

@@ -384,6 +384,7 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
       real[k] = sh[k].x;
     }
     if ((s = gauge_prepare(g, P))) return s;
+    const L2LinkWindow l2(ctx, g, P);
     if (op == CLG_OP_MEE_MEEDAG) return ctx->fail(CLG_ERR_UNSUPPORTED, "CG-M on MEE_MEEDAG: use FOM_MS");
     // workspace reused while lattice, kind, parity layout, precision, shift
     // count, operator and the gauge arrays stay the same

@@ -725,6 +725,7 @@ clg_status clg::solve_core(const SolveReq& q) {
   clg_status s = CLG_SUCCESS;
   const int P = q.prm->inner_precision;
   if ((s = gauge_prepare(U, P))) return s;
+  const L2LinkWindow l2(ctx, U, P);
   // The workspace (buffers, pinned memory, captured graphs) lives in the solver
   // and is reused while the shape of the solve and the gauge arrays stay the same.
   const std::string key =
