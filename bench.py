@@ -292,21 +292,26 @@ def ours(args, world, rank, local):
         b.to_numpy(r, out=src[r])
     bh = [clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs) for _ in range(2)]
     xh = [clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs) for _ in range(2)]
+
+    def pipeline(steps):
+        for r in range(nrhs):
+            bh[0].from_numpy_async(src[r], r)
+        for k in range(steps):
+            if k + 1 < steps:
+                for r in range(nrhs):
+                    bh[(k + 1) % 2].from_numpy_async(src[r], r)
+            check(mixed.Solve(xh[k % 2], bh[k % 2], U, clg.EFO_F_D))
+            for r in range(nrhs):
+                xh[k % 2].to_numpy_async(dst[k % 2][r], r)
+        for f in xh + bh:
+            f.wait()
+
+    pipeline(2)  # untimed: allocates the fields' transfer staging and events
     barrier(world)
     torch.cuda.synchronize()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
-    for r in range(nrhs):
-        bh[0].from_numpy_async(src[r], r)
-    for k in range(args.steps):
-        if k + 1 < args.steps:
-            for r in range(nrhs):
-                bh[(k + 1) % 2].from_numpy_async(src[r], r)
-        check(mixed.Solve(xh[k % 2], bh[k % 2], U, clg.EFO_F_D))
-        for r in range(nrhs):
-            xh[k % 2].to_numpy_async(dst[k % 2][r], r)
-    for f in xh + bh:
-        f.wait()
+    pipeline(args.steps)
     e3.record(stream)  # after the last copy to the host has landed
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3, world)
