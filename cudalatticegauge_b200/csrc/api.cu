@@ -310,6 +310,7 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   ctx->max_persist = prop.persistingL2CacheMaxSize > 0 ? (size_t)prop.persistingL2CacheMaxSize : 0;
   ctx->l2_bytes = prop.l2CacheSize > 0 ? (size_t)prop.l2CacheSize : 0;
   if (const char* t = std::getenv("CLG_L2_WINDOW")) ctx->l2_window = t[0] != '0';
+  if (const char* t = std::getenv("CLG_DEVICE_LOOP")) ctx->device_loops = t[0] == '1';
   // CLG_AUTOTUNE=0 keeps the default block size (reproducible profiling runs)
   if (const char* t = std::getenv("CLG_AUTOTUNE")) ctx->tuning_enabled = t[0] != '0';
   if (const char* t = std::getenv("CLG_FUSED_CG")) ctx->fused_cg = t[0] != '0';

@@ -90,6 +90,11 @@ struct clg_context_s {
   // solves keep the low-precision link copy in a persisting L2 window
   // (CLG_L2_WINDOW=0 turns it off); device limits queried at creation
   bool l2_window = true;
+  // CLG_DEVICE_LOOP=1: CG inner solves loop on the device (CUDA-graph WHILE
+  // node) after their first chunk, instead of one host check per chunk.  Off
+  // by default: on the 32^3x16 FP16-inner solve it measured no faster
+  // (70.2 / 71.7 against 71.2 / 74.5 solves/s), the host checks being cheap
+  bool device_loops = false;
   size_t max_window = 0, max_persist = 0, persist_set = 0, l2_bytes = 0;
   clg_status fail(clg_status s, const std::string& msg) {
     last_error = msg;

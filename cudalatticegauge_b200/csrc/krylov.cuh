@@ -23,7 +23,8 @@ struct KState {
   int status;
   int iters;     // operator applications
   int j;         // GMRES: columns built in this cycle
-  int pad[2];
+  int since;     // device-side inner loop: chunks without improving `best`
+  int pad;
   // GMRES cycle
   double2 H[(GM_MAXK + 1) * GM_MAXK];  // H[i*GM_MAXK + j]
   double2 cs[GM_MAXK], sn[GM_MAXK];
@@ -32,6 +33,7 @@ struct KState {
   double s[GM_MAXK + 1];   // lazy normalisation: v_i = s_i * V'_i
   double beta0;            // |r| at the start of the cycle
   double resid_est;        // |g_(j+1)| estimate
+  double best;             // device-side inner loop: smallest residual seen (stagnation guard)
 };
 
 __device__ __forceinline__ bool bad(double v) { return !(v == v) || isinf(v); }

@@ -69,6 +69,41 @@ __global__ void kstate_reset(KState* st, const int* outer_done, int nrhs) {
   k.iters = 0;
   k.j = 0;
   k.rr = k.rr0 = 0.0;
+  k.best = 1e300;
+  k.since = 0;
+}
+
+// Control of the device-side inner loop (a CUDA-graph WHILE node whose body is
+// one chunk of iterations followed by loop_cond).
+struct LoopCtl {
+  int cap;         // operator applications allowed per rhs in this inner solve
+  int max_chunks;  // hard bound on the chunks of one inner solve
+  int chunks;      // chunks run so far
+  int pad;
+};
+
+// Keeps looping while some right-hand side is unfinished, under its budget
+// and has improved its residual within the last `patience` chunks -- the
+// host-side rules of iterate(), evaluated on the device.
+__global__ void loop_cond(KState* st, int nrhs, LoopCtl* ctl, int patience, cudaGraphConditionalHandle h) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  ctl->chunks += 1;
+  unsigned go = 0;
+  if (ctl->chunks < ctl->max_chunks) {
+    for (int r = 0; r < nrhs; ++r) {
+      KState& k = st[r];
+      if (k.done || k.iters >= ctl->cap) continue;
+      const double cur = k.rr > 0 ? k.rr : k.resid_est * k.resid_est;
+      if (cur < 0.9 * k.best) {
+        k.best = cur;
+        k.since = 0;
+      } else if (++k.since >= patience) {
+        continue;
+      }
+      go = 1;
+    }
+  }
+  cudaGraphSetConditional(h, go);
 }
 
 struct Summary {
@@ -248,6 +283,12 @@ struct Work : public SolveCacheBase {
   // graphs
   std::vector<cudaGraphExec_t> graphs;
   std::vector<int64_t> graph_kernels;  // kernel nodes per graph (for the launch count)
+  // device-side inner loops (WHILE node around one chunk + loop_cond) per slot
+  std::vector<cudaGraphExec_t> loops;
+  std::vector<int64_t> loop_kernels;  // kernel nodes per loop body
+  std::vector<char> loop_failed;      // building the loop failed once: host-driven chunks
+  LoopCtl* ctl_d = nullptr;
+  LoopCtl* ctl_h = nullptr;           // pinned
   int total_iters = 0;
   int inner_cap = 1 << 30;  // operator applications allowed in the current inner solve
   clg_status kvec(int slot, int idx, int np, int fp, FieldRef& out) {
@@ -267,6 +308,10 @@ struct Work : public SolveCacheBase {
   ~Work() {
     for (auto g : graphs)
       if (g) cudaGraphExecDestroy(g);
+    for (auto g : loops)
+      if (g) cudaGraphExecDestroy(g);
+    dfree(ctl_d);
+    if (ctl_h) cudaFreeHost(ctl_h);
     dfree(st);
     dfree(sum_d);
     dfree(outer_done_d);
@@ -315,8 +360,85 @@ clg_status kapply(Work& w, int op, const FieldRef& out, const FieldRef& in, cons
 
 // Run `body` (one iteration or one cycle) repeatedly until every rhs is done
 // or the budget runs out.  Chunks after the first are replayed from a CUDA graph.
+// The rest of an inner solve as one graph launch: a WHILE node whose body is
+// `chunk` iterations and loop_cond.  Built on first use per graph slot (the
+// body is captured into the node's body graph); afterwards one launch and one
+// host read per inner solve.  CLG_ERR_UNSUPPORTED: the loop could not be built
+// (the caller falls back to host-driven chunks).
 template <class Body>
-clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& body) {
+clg_status run_device_loop(Work& w, int slot, int chunk, int max_chunks, int patience, Body& body) {
+  clg_context_s* ctx = w.ctx;
+  while ((int)w.loops.size() <= slot) {
+    w.loops.push_back(nullptr);
+    w.loop_kernels.push_back(0);
+    w.loop_failed.push_back(0);
+  }
+  if (w.loop_failed[slot]) return CLG_ERR_UNSUPPORTED;
+  if (!w.ctl_d) {
+    if (clg_status s = dalloc(ctx, (void**)&w.ctl_d, sizeof(LoopCtl))) return s;
+    if (cudaMallocHost((void**)&w.ctl_h, sizeof(LoopCtl)) != cudaSuccess) {
+      w.ctl_h = nullptr;
+      return ctx->fail(CLG_ERR_OOM, "loop control (pinned)");
+    }
+  }
+  if (!w.loops[slot]) {
+    cudaGraph_t g = nullptr;
+    cudaGraphConditionalHandle h;
+    cudaGraphNodeParams np = {};
+    cudaGraphNode_t node;
+    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      ok = cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess;
+    }
+    clg_status s = CLG_SUCCESS;
+    if (ok) ok = cudaStreamBeginCaptureToGraph(ctx->stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      // captured launches run per loop pass: count them from the passes run
+      const int64_t k0 = ctx->kernels;
+      const bool pdl = ctx->pdl;
+      ctx->pdl = false;  // plain stream order inside the loop body
+      for (int i = 0; i < chunk && !s; ++i) s = body();
+      if (!s) {
+        loop_cond<<<1, 32, 0, ctx->stream>>>(w.st, w.nrhs, w.ctl_d, patience, h);
+        ctx->kernels++;
+      }
+      ctx->pdl = pdl;
+      w.loop_kernels[slot] = ctx->kernels - k0;
+      ctx->kernels = k0;
+      cudaGraph_t out = nullptr;
+      ok = cudaStreamEndCapture(ctx->stream, &out) == cudaSuccess && !s;
+      cudaGraphExec_t ex = nullptr;
+      if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+      if (ok) w.loops[slot] = ex;
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (s) return s;
+    if (!ok) {
+      w.loop_failed[slot] = 1;
+      return CLG_ERR_UNSUPPORTED;
+    }
+  }
+  w.ctl_h->cap = w.inner_cap;
+  w.ctl_h->max_chunks = max_chunks;
+  w.ctl_h->chunks = 0;
+  cudaError_t e = cudaMemcpyAsync(w.ctl_d, w.ctl_h, sizeof(LoopCtl), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaGraphLaunch(w.loops[slot], ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w.ctl_h, w.ctl_d, sizeof(LoopCtl), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("device loop: ") + cudaGetErrorString(e));
+  if (clg_status s = read_summary(w)) return s;  // synchronises the stream
+  ctx->kernels += (int64_t)w.ctl_h->chunks * w.loop_kernels[slot];
+  return CLG_SUCCESS;
+}
+
+template <class Body>
+clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& body, bool device_loop = false) {
   const bool graphs = w.prm->use_graphs && w.ctx->stream != nullptr;
   while ((int)w.graphs.size() <= graph_slot) w.graphs.push_back(nullptr);
   while ((int)w.graph_kernels.size() <= graph_slot) w.graph_kernels.push_back(0);
@@ -327,6 +449,12 @@ clg_status iterate(Work& w, int graph_slot, int chunk, int max_chunks, Body&& bo
   const int patience = std::max(8, 400 / std::max(chunk, 1));
   for (int c = 0; c < max_chunks; ++c) {
     clg_status s = CLG_SUCCESS;
+    // after the first (eager) chunk, the rest of the inner solve on the device
+    if (device_loop && graphs && w.ctx->device_loops && c > 0) {
+      s = run_device_loop(w, graph_slot, chunk, max_chunks - c, patience, body);
+      if (s != CLG_ERR_UNSUPPORTED) return s;
+      s = CLG_SUCCESS;
+    }
     if (graphs && c > 0 && !w.graphs[graph_slot]) {
       cudaGraph_t g = nullptr;
       if (cudaStreamBeginCapture(w.ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -560,7 +688,7 @@ clg_status krylov(Work& w, int op, const FieldRef& x, const FieldRef& b, int slo
       // fewer (skipped) iterations; measured on the 32^3x16 FP16-inner solve
       // against chunks of 4, 12 and 16 (65.5, 66.0, 67.2 -> 69.8 solves/s)
       const int chunk = 8;
-      return iterate(w, slot_base + 1, chunk, w.prm->max_iterations / chunk + 2, body);
+      return iterate(w, slot_base + 1, chunk, w.prm->max_iterations / chunk + 2, body, true);
     });
   }
 

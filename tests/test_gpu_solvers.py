@@ -127,6 +127,36 @@ def test_wilson_cg_normal_equations(ctx, clg, oracle, op, name, prec):
     assert o.true_residual(b.to_numpy(), x.to_numpy()) <= TOL
 
 
+@pytest.mark.parametrize("prec", [1, 2])
+def test_cg_device_loop(clg, oracle, prec, monkeypatch):
+    """CG inner solves looping on the device (CLG_DEVICE_LOOP=1: a CUDA-graph
+    WHILE node around each chunk with the stop rules evaluated by a kernel)
+    against the host-driven chunk loop: same residual bound, same iteration
+    counts (the stop rules are the same), two solves in a row (the second
+    replays the cached loop graph)."""
+    results = {}
+    for loop in ("1", "0"):
+        monkeypatch.setenv("CLG_DEVICE_LOOP", loop)
+        c = clg.Context(0)
+        lat = clg.Lattice(c, (8, 8, 8, 16))
+        U = gauge(clg, lat, "expH", 0xC1A60001)
+        b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=2)
+        for r in range(2):
+            b.InitialField(clg.SOURCE_GAUSS, 26 + r, 2, rhs=r)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=2)
+        S = clg.CSLASolverCG(c, inner_precision=prec)
+        o = oracle.Operator("WILSON_D", lat.dims, U.CopyDataOut(), KAPPA)
+        for _ in range(2):
+            infos = S.Solve(x, b, U, clg.EFO_F_D)
+            for r in range(2):
+                assert infos[r]["status"] == 0
+                assert o.true_residual(b.to_numpy(r), x.to_numpy(r)) <= TOL
+        results[loop] = [i["iterations"] for i in infos]
+        S.close()
+        c.close()
+    assert results["1"] == results["0"]
+
+
 @pytest.mark.parametrize("op,name", [(0, "WILSON_D"), (1, "WILSON_DDAG")])
 @pytest.mark.parametrize("prec", [0, 1, 2])
 def test_wilson_cg_fused_matches_unfused(clg, oracle, op, name, prec, monkeypatch):
