@@ -382,6 +382,7 @@ def ours(args, world, rank, local):
             extra["batched_config4"] = batched_config4(clg, ctx, stream, args)
             extra["uneven_lattices_config4"] = uneven_lattices(clg, ctx, stream, args)
         if args.workload == DEFAULT_WORKLOAD and not args.no_side:
+            extra["config1"] = config1(clg, ctx, stream)
             extra["dslash_config3"] = dslash_config3(clg, ctx, stream)
             extra["staggered_multishift_config5"] = staggered_config5(clg, ctx, stream)
         if world == 1 and not args.no_cpu:
@@ -461,6 +462,51 @@ def batched_config4(clg, ctx, stream, args, steps=2):
         f.close()
     s.close()
     s64.close()
+    U.close()
+    return out
+
+
+def config1(clg, ctx, stream):
+    """8^4, Haar links (seed 0xC1A60000), kappa 0.1355, one
+    Gaussian source.  The full D and D^+ applied in FP64 (the whole problem
+    sits in L2, so GB/s here is not a roofline claim) and D x = b solved to the
+    true relative residual 1e-10 by GMRES(12), the reference's solver on this
+    case, in FP64 and with FP32 / FP16 inner iterations."""
+    import torch
+
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_HAAR, 0xC1A60000, 1)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, 0.1355)
+    b.InitialField(clg.SOURCE_GAUSS, 0xC1A60000, 2)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, 0.1355)
+    out = {"dims": [8, 8, 8, 8]}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, op in (("D", clg.EFO_F_D), ("Ddagger", clg.EFO_F_Ddagger)):
+        for _ in range(3):
+            b.apply_to(op, x, U)
+        reps = 200
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            b.apply_to(op, x, U)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        out[name] = {"us": round(t * 1e6, 2), "GB/s": round(960 * lat.volume / t / 1e9, 1)}
+    for name, prec in (("fp64_gmres12", clg.DOUBLE), ("mixed_gmres12", clg.SINGLE), ("half_gmres12", clg.HALF)):
+        S = clg.CSLASolverGMRES(ctx, inner_precision=prec, tol_true_rel=TOL, MaxDim=12)
+        S.Solve(x, b, U, clg.EFO_F_D)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        info = S.Solve(x, b, U, clg.EFO_F_D)[0]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = {"solves_per_s": round(1e3 / e0.elapsed_time(e1), 2), "applications": info["iterations"],
+                     "true_rel_residual": info["true_rel_residual"], "status": info["status"]}
+        S.close()
+    for f in (b, x):
+        f.close()
     U.close()
     return out
 
