@@ -34,7 +34,7 @@ WILSON, STAGGERED = 0, 1
 FULL, EVEN = 0, 1
 DOUBLE, SINGLE, HALF = 0, 1, 2
 LAYOUT_CLGBIN, LAYOUT_BRIDGEPP = 0, 1
-GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH = 0, 1, 2
+GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
 SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT = 0, 1, 2, 3
 SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS = 0, 1, 2, 3, 4
 

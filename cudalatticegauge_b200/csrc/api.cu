@@ -500,7 +500,7 @@ clg_status clg_gauge_export(clg_gauge g, double* data, int on_device) {
 }
 
 clg_status clg_gauge_random(clg_gauge g, int init, uint64_t seed, uint32_t field_id, double eps) {
-  if (!g || init < 0 || init > 2) return CLG_ERR_BAD_ARG;
+  if (!g || init < 0 || init > CLG_GAUGE_ZERO) return CLG_ERR_BAD_ARG;
   clg_status st = gauge_generate(g, init, seed, field_id, eps);
   if (!st) st = refresh_unitarity(g);
   return st;

@@ -184,6 +184,8 @@ __global__ void gauge_gen_kernel(Geom g, LinkPtrs L, int init, uint64_t seed, ui
     haar(seed, fid, (uint64_t)l, m);
   else if (init == CLG_GAUGE_EXPH)
     expH(seed, fid, (uint64_t)l, eps, m);
+  else if (init == CLG_GAUGE_ZERO)
+    for (int k = 0; k < 9; ++k) m[k] = mk<double>(0, 0);
   else
     for (int k = 0; k < 9; ++k) m[k] = mk<double>((k % 4 == 0) ? 1.0 : 0.0, 0);
   store_link64(L.u, si.p, mu, g.Vh, si.h, m);

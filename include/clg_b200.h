@@ -63,7 +63,8 @@ typedef enum { CLG_FERMION_WILSON = 0, CLG_FERMION_STAGGERED = 1 } clg_fermion_k
 typedef enum { CLG_SUBSET_FULL = 0, CLG_SUBSET_EVEN = 1 } clg_subset;
 typedef enum { CLG_PREC_DOUBLE = 0, CLG_PREC_SINGLE = 1, CLG_PREC_HALF = 2 } clg_precision;
 typedef enum { CLG_LAYOUT_CLGBIN = 0, CLG_LAYOUT_BRIDGEPP = 1 } clg_layout;
-typedef enum { CLG_GAUGE_IDENTITY = 0, CLG_GAUGE_HAAR = 1, CLG_GAUGE_EXPH = 2 } clg_gauge_init;
+/* ZERO: all links 0 (a force accumulator, CFieldGaugeSU3::InitialField(EFIT_Zero)) */
+typedef enum { CLG_GAUGE_IDENTITY = 0, CLG_GAUGE_HAAR = 1, CLG_GAUGE_EXPH = 2, CLG_GAUGE_ZERO = 3 } clg_gauge_init;
 typedef enum { CLG_SOURCE_ZERO = 0, CLG_SOURCE_GAUSS = 1, CLG_SOURCE_Z2 = 2, CLG_SOURCE_POINT = 3 } clg_source_kind;
 typedef enum {
     CLG_SOLVER_GMRES = 0,       /* CSLASolverGMRES    SparseLinearAlgebra/CSolverGMRES.cpp:111-358   */

@@ -230,6 +230,65 @@ void clgo_wilson_mee(const clgo_lat* lat, const double* U, double kappa, int dag
     }
 }
 
+/* ============================================================== Wilson fermion force
+ * _kernelDWilsonForceSU3 (CFieldFermionWilsonSquareSU3.cu:170-231), launched by
+ * DerivateDOperator (:260-275) from CalculateForceS (:1016-1100) with
+ * X = (D D^+)^-1 phi (pInverseDDdagger) and Y = D^+ X (pInverseD):
+ *   mid  = C(X(x), (1 - g_mu) Y(x+mu)) + C((1 + g_mu) Y(x), X(x+mu)),
+ *          C(l, r) = sum_s r_s l_s^+   (makeSU3Contract, SU3.h:395-500)
+ *   F_mu(x) += s_+ kappa Ta(U_mu(x) mid)
+ * Ta: traceless anti-hermitian part (SU3.h:953-980); s_+ the boundary sign of
+ * the hop to x+mu (NeedToOpposite).  F is added to, in the link layout of U. */
+static inline void su3_ta(cplx m[9]) {
+    for (int r = 0; r < 3; ++r)
+        for (int c = r + 1; c < 3; ++c) {
+            const cplx n = 0.5 * (m[3 * r + c] - conj(m[3 * c + r]));
+            m[3 * r + c] = n;
+            m[3 * c + r] = -conj(n);
+        }
+    const double tr = (cimag(m[0]) + cimag(m[4]) + cimag(m[8])) / 3.0;
+    for (int d = 0; d < 3; ++d) m[4 * d] = I * (cimag(m[4 * d]) - tr);
+}
+
+void clgo_wilson_force(const clgo_lat* lat, const double* U, double kappa, const double* X, const double* Y,
+                       double* F) {
+    const long V = lat_volume(lat->L);
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s) {
+        int c[4];
+        coords_of(lat->L, s, c);
+        cplx xl[12], xr[12];
+        spinor_load(X, s, xl);
+        spinor_load(Y, s, xr);
+        for (int mu = 0; mu < 4; ++mu) {
+            int sg = 1;
+            const long sp = neighbour(lat->L, lat->bc, c, mu, 1, &sg);
+            cplx xpl[12], xpr[12], g[12], r1[12], r2[12];
+            spinor_load(X, sp, xpl);
+            spinor_load(Y, sp, xpr);
+            gamma_mul(mu, xpr, g);
+            for (int k = 0; k < 12; ++k) r1[k] = xpr[k] - g[k];
+            gamma_mul(mu, xr, g);
+            for (int k = 0; k < 12; ++k) r2[k] = xr[k] + g[k];
+            cplx mid[9];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    cplx v = 0;
+                    for (int sp4 = 0; sp4 < 4; ++sp4)
+                        v += conj(xl[3 * sp4 + b]) * r1[3 * sp4 + a] + conj(r2[3 * sp4 + b]) * xpl[3 * sp4 + a];
+                    mid[3 * a + b] = v;
+                }
+            cplx u[9], m[9], f[9];
+            su3_load(U, 4 * s + mu, u);
+            su3_mul(u, mid, m);
+            su3_ta(m);
+            su3_load(F, 4 * s + mu, f);
+            for (int k = 0; k < 9; ++k) f[k] += (double)sg * kappa * m[k];
+            su3_store(F, 4 * s + mu, f);
+        }
+    }
+}
+
 /* ============================================================== staggered D
  * _kernelDFermionKS (CFieldFermionKSSU3.cu:33-117):
  *   out(x) = c * [ 2am chi(x) +/- sum_mu eta_mu(x) ( s_+ U_mu(x) chi(x+mu) - s_- U_mu(x-mu)^+ chi(x-mu) ) ]

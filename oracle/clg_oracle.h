@@ -55,6 +55,9 @@ void clgo_wilson_hop(const clgo_lat* lat, const double* U, int dagger, int out_p
                      const double* in, double* out);
 void clgo_wilson_mee(const clgo_lat* lat, const double* U, double kappa, int dagger,
                      const double* in, double* out, double* tmp);
+/* F += Wilson fermion force from X = (DD^+)^-1 phi and Y = D^+ X (link layout of U) */
+void clgo_wilson_force(const clgo_lat* lat, const double* U, double kappa, const double* X, const double* Y,
+                       double* F);
 void clgo_ks_D(const clgo_lat* lat, const double* U, double mass2am, int dagger,
                int coeff_type, double cre, double cim, const double* in, double* out);
 void clgo_ks_hop(const clgo_lat* lat, const double* U, int out_parity, const double* in, double* out);

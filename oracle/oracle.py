@@ -86,6 +86,7 @@ def lib():
             "clgo_wilson_D": (None, [p, p, d, i, i, d, d, p, p]),
             "clgo_wilson_hop": (None, [p, p, i, i, p, p]),
             "clgo_wilson_mee": (None, [p, p, d, i, p, p, p]),
+            "clgo_wilson_force": (None, [p, p, d, p, p, p]),
             "clgo_ks_D": (None, [p, p, d, i, i, d, d, p, p]),
             "clgo_ks_hop": (None, [p, p, i, p, p]),
             "clgo_ks_dddag_ee": (None, [p, p, d, p, p, p]),
@@ -217,6 +218,18 @@ def wilson_mee(L, U, psi, kappa, dagger=False, bc=(1, 1, 1, -1)):
     tmp = np.empty_like(psi)
     lat = _lat(L, bc)
     lib().clgo_wilson_mee(C.byref(lat), _ptr(U), kappa, int(dagger), _ptr(psi), _ptr(out), _ptr(tmp))
+    return out
+
+
+def wilson_force(L, U, X, Y, kappa, F=None, bc=(1, 1, 1, -1)):
+    """F + the Wilson fermion force of X = (DD^+)^-1 phi, Y = D^+ X
+    (_kernelDWilsonForceSU3, CFieldFermionWilsonSquareSU3.cu:170-231); F and U in
+    the CLGBin link layout (V*4 links of 9 complex)."""
+    X = np.ascontiguousarray(X, np.complex128)
+    Y = np.ascontiguousarray(Y, np.complex128)
+    out = np.zeros_like(np.ascontiguousarray(U, np.complex128)) if F is None else np.array(F, np.complex128)
+    lat = _lat(L, bc)
+    lib().clgo_wilson_force(C.byref(lat), _ptr(U), kappa, _ptr(X), _ptr(Y), _ptr(out))
     return out
 
 

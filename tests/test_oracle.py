@@ -186,3 +186,48 @@ def test_oracle_solvers_small(oracle):
     xs, i5 = oracle.fom_ms(op, b, cs, maxdim=12, restart=200, accuracy=1e-13)
     for k, s in enumerate(cs):
         assert op.true_residual(b, xs[k], complex(s)) < 1e-10
+
+
+def test_wilson_force_is_the_action_derivative(oracle):
+    """The Wilson fermion force as the oracle restates _kernelDWilsonForceSU3
+    (CFieldFermionWilsonSquareSU3.cu:170-231) is the derivative of the action
+    S = phi^+ (DD^+)^-1 phi that CalculateForceS (:1016-1100) differentiates:
+    with X = (DD^+)^-1 phi, Y = D^+ X and U_mu(x) -> exp(i e T) U_mu(x) for a
+    traceless hermitian T,  dS/de = 2 i Tr(T F_mu(x)).  Checked against central
+    finite differences of S (FP64 oracle CG) on random links and generators,
+    including links that cross the antiperiodic t boundary."""
+    L = (4, 4, 4, 4)
+    V = oracle.volume(L)
+    kappa = 0.12
+    U = oracle.gauge_expH(L, 0xC1A60021, 0.3)
+    phi = oracle.gauss(V, 12, 7, 2).reshape(V, 4, 3)
+
+    def action(Ul):
+        op = oracle.Operator("WILSON_DDDAG", L, Ul, kappa)
+        X, info = oracle.cg(op, phi, tol=1e-13, maxiter=20000)
+        assert info["true_rel_residual"] < 1e-12
+        return np.vdot(phi, X).real, X
+
+    _, X = action(U)
+    Y = oracle.wilson_D(L, U, X, kappa, dagger=True)
+    F = oracle.wilson_force(L, U, X, Y, kappa)
+    # anti-hermitian and traceless, as Ta makes it
+    assert np.abs(F + np.conj(np.transpose(F, (0, 2, 1)))).max() < 1e-14
+    assert np.abs(np.trace(F, axis1=1, axis2=2)).max() < 1e-14
+    rng = np.random.default_rng(5)
+    t_edge = int(np.flatnonzero(np.arange(V) % L[3] == L[3] - 1)[3]) * 4 + 3  # a t link across the boundary
+    for link in [t_edge] + [int(v) for v in rng.integers(0, 4 * V, 3)]:
+        A = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+        T = (A + A.conj().T) / 2
+        T -= np.trace(T) / 3 * np.eye(3)
+        w, Q = np.linalg.eigh(T)
+        eps = 1e-5
+
+        def S_at(e):
+            U2 = U.copy()
+            U2[link] = (Q @ np.diag(np.exp(1j * e * w)) @ Q.conj().T) @ U[link]
+            return action(U2)[0]
+
+        dS = (S_at(eps) - S_at(-eps)) / (2 * eps)
+        want = (2j * np.trace(T @ F[link])).real
+        assert abs(dS - want) <= 1e-6 * max(1.0, abs(want)), (link, dS, want)
