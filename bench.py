@@ -385,6 +385,7 @@ def ours(args, world, rank, local):
             extra["config1"] = config1(clg, ctx, stream)
             extra["dslash_config3"] = dslash_config3(clg, ctx, stream)
             extra["staggered_multishift_config5"] = staggered_config5(clg, ctx, stream)
+            extra["wilson_force_32x32x32x16"] = wilson_force_side(clg, ctx, stream)
         if world == 1 and not args.no_cpu:
             extra["cpu_baseline"] = cpu_baseline(U, lat, kappa, plain["fp64_gmres12"]["applications"])
     result = {
@@ -577,6 +578,81 @@ def dslash_config3(clg, ctx, stream):
     return out
 
 
+FORCE_BYTES_PER_SITE = (2 * 24 + 4 * 18 + 2 * 4 * 18) * 8  # X, Y; U; F read + written (FP64)
+
+
+def wilson_force_side(clg, ctx, stream, dims=(32, 32, 32, 16), kappa=0.1355):
+    """The HMC pseudofermion force (CalculateForceS) on the headline lattice.
+
+    kernel: F += force(U, X, Y) alone, FP64, compulsory bytes per site
+    FORCE_BYTES_PER_SITE (X, Y read once, four links read, four force links
+    read and written) against the measured copy peak; the 1.1 GB working set
+    is larger than L2.
+    step: the whole force step -- D D^+ X = phi to 1e-10 (CG, FP16 inner),
+    cache, Y = D^+ X, force -- from a zero start and from the cache of the
+    previous step after a small change of the links (exp(i 0.01 H) U, as one
+    molecular-dynamics step moves them)."""
+    import torch
+
+    peak, _ = peaks()
+    lat = clg.Lattice(ctx, dims)
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+    F = clg.CFieldGaugeSU3(lat)
+    F.InitialField(clg.GAUGE_ZERO)
+    X = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    Y = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    X.InitialField(clg.SOURCE_GAUSS, 0xC1A60040, 2)
+    Y.InitialField(clg.SOURCE_GAUSS, 0xC1A60041, 2)
+    out = {"dims": list(dims), "bytes_per_site": FORCE_BYTES_PER_SITE}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        clg.CFieldFermionWilsonSquareSU3.DerivateDOperator(F, Y, X, U)
+    reps = 20
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        clg.CFieldFermionWilsonSquareSU3.DerivateDOperator(F, Y, X, U)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    gbs = FORCE_BYTES_PER_SITE * lat.volume / t / 1e9
+    out["kernel"] = {"launch_us": round(t * 1e6, 2), "GB/s": round(gbs, 1), "frac": round(gbs / peak, 4)}
+
+    phi = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    phi.InitialField(clg.SOURCE_GAUSS, 0xC1A60042, 2)
+    cache = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    S = clg.CSLASolverCG(ctx, inner_precision=clg.HALF, tol_true_rel=TOL)
+    cache.Zero()
+    phi.CalculateForceS(U, F, S, cache)  # warm-up (workspace, autotuner)
+    steps = {}
+    for name, warm in (("cold_start", False), ("cached_start", True)):
+        if warm:
+            # cache = X of the current links; then move the links in place by a
+            # small step, as one molecular-dynamics update does
+            phi.CalculateForceS(U, F, S, cache)
+            small = clg.CFieldGaugeSU3(lat)
+            small.InitialField(clg.GAUGE_EXPH, 0xC1A60043, 1, 0.01)
+            U.InitialWithByte(np.ascontiguousarray(small.CopyDataOut() @ U.CopyDataOut()))
+            small.close()
+        else:
+            cache.Zero()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        info = phi.CalculateForceS(U, F, S, cache)[0]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dt = e0.elapsed_time(e1) / 1e3
+        steps[name] = {"force_steps_per_s": round(1.0 / dt, 3), "seconds": round(dt, 4),
+                       "applications": info["iterations"], "outer": info["outer"],
+                       "true_rel_residual": info["true_rel_residual"], "status": info["status"]}
+    out["step"] = steps
+    for f in (F, X, Y, phi, cache, U):
+        f.close()
+    S.close()
+    return out
+
+
 def staggered_config5(clg, ctx, stream, steps=2):
     """32^3x16 staggered fermions, 2am = 0.02 (the reference's
     `Mass` parameter is 2am), BC (+,+,+,-), 12 shifts sigma_k = 10^(-4 + 5k/11),
@@ -718,6 +794,15 @@ def profile_driver(args):
         o = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], precision=prec)
         for _ in range(args.steps):
             a.apply_to(clg.OP_DEO, o, U)
+    elif args.profile == "force":
+        F = clg.CFieldGaugeSU3(lat)
+        F.InitialField(clg.GAUGE_ZERO)
+        X = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"])
+        Y = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"])
+        X.InitialField(clg.SOURCE_GAUSS, 5, 2)
+        Y.InitialField(clg.SOURCE_GAUSS, 6, 2)
+        for _ in range(args.steps):
+            clg.CFieldFermionWilsonSquareSU3.DerivateDOperator(F, Y, X, U)
     else:
         b = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=W["nrhs"])
         for r in range(W["nrhs"]):
@@ -746,7 +831,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched config-4 side measurements")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the config-3 Dslash and config-5 staggered multi-shift side measurements")
-    ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve"],
+    ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve", "force"],
                     help="profiling driver (no JSON line): `--steps` hop launches on the workload lattice, "
                          "or `--steps` solves without warm-up")
     args = ap.parse_args()

@@ -109,6 +109,8 @@ SIGNATURES = [
     ("clg_solve", _S, [_P, _P, _P, _P, _I, _P, _P]),
     ("clg_solve_multishift", _S, [_P, _P, _I, _P, _P, _P, _I, _P]),
     ("clg_rational_apply", _S, [_P, _P, _P, _I, _I, _D, _P, _P, _P]),
+    ("clg_wilson_force", _S, [_P, _P, _P, _P]),
+    ("clg_wilson_fermion_force", _S, [_P, _P, _P, _P, _P, _P]),
 ]
 
 _lib = None
@@ -339,6 +341,24 @@ class _FermionField:
 class CFieldFermionWilsonSquareSU3(_FermionField):
     """Wilson fermion, param = Hopping (kappa)."""
     KIND, NC = WILSON, 12
+
+    @staticmethod
+    def DerivateDOperator(force: CFieldGaugeSU3, dphi: "CFieldFermionWilsonSquareSU3",
+                          dddphi: "CFieldFermionWilsonSquareSU3", gauge: CFieldGaugeSU3):
+        """force += the Wilson fermion force from X = dddphi = (DD^+)^-1 phi and
+        Y = dphi = D^+ X (CFieldFermionWilsonSquareSU3.cu:260-275, argument order
+        as there: force, D^+ X, X, gauge)."""
+        gauge.ctx.check(gauge.ctx.lib.clg_wilson_force(force.h, gauge.h, dddphi.h, dphi.h), "clg_wilson_force")
+
+    def CalculateForceS(self, gauge: CFieldGaugeSU3, force: CFieldGaugeSU3, solver: "_Solver",
+                        cache: Optional["CFieldFermionWilsonSquareSU3"] = None):
+        """force += the force of the pseudofermion action phi^+ (DD^+)^-1 phi, phi = self
+        (CFieldFermionWilsonSquareSU3.cu:1016-1100).  cache (nullable) is the start
+        vector of the D D^+ solve and receives its solution.  Returns the solve infos."""
+        infos = (SolveInfo * self.nrhs)()
+        st = self.ctx.lib.clg_wilson_fermion_force(solver.h, force.h, gauge.h, self.h, cache.h if cache else None, infos)
+        self.ctx.check(st, "clg_wilson_fermion_force")
+        return [i.as_dict() for i in infos]
 
 
 class CFieldFermionKSSU3(_FermionField):

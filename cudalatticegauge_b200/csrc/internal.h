@@ -318,4 +318,10 @@ struct clg_solver_s {
   std::unique_ptr<clg::SolveCacheBase> cache;        // single-shift solves
   std::unique_ptr<clg::SolveCacheBase> cache_shift;  // multi-shift refinement
   std::unique_ptr<clg::SolveCacheBase> cache_cgm;    // multi-shift CG vectors, state, graph
+  // X = (DD^+)^-1 phi and Y = D^+ X of clg_wilson_fermion_force
+  clg_field force_x = nullptr, force_y = nullptr;
+  ~clg_solver_s() {
+    if (force_x) clg_field_destroy(force_x);
+    if (force_y) clg_field_destroy(force_y);
+  }
 };

@@ -231,6 +231,25 @@ clg_status clg_solve_multishift(clg_solver s, clg_field* x, int nshift, const do
 clg_status clg_rational_apply(clg_solver s, clg_field f, clg_gauge g, int op, int degree, double c,
                               const double* a, const double* b, clg_solve_info* info);
 
+/* ------------------------------------------------------------------ HMC fermion force
+ * CFieldFermionWilsonSquareSU3::DerivateDOperator / _kernelDWilsonForceSU3
+ * (Data/Field/WilsonDirac/CFieldFermionWilsonSquareSU3.cu:170-231, :260-275):
+ * with X = (D D^+)^-1 phi and Y = D^+ X (FULL FP64 Wilson fields, kappa = X's
+ * param), add to every link
+ *   F_mu(x) += s kappa Ta(U_mu(x) [sum_s ((1 - g_mu) Y(x+mu))_s X(x)_s^+ + X(x+mu)_s ((1 + g_mu) Y(x))_s^+])
+ * (Ta the traceless anti-hermitian part, s the fermion boundary sign of the hop
+ * x -> x+mu).  F is a gauge field used as an accumulator (start it with
+ * clg_gauge_random(F, CLG_GAUGE_ZERO, ...)); it must not be g.  Fields holding
+ * several right-hand sides add the force of each. */
+clg_status clg_wilson_force(clg_gauge F, clg_gauge g, clg_field X, clg_field Y);
+/* CFieldFermionWilsonSquareSU3::CalculateForceS (same file :1016-1100): solve
+ * D D^+ X = phi with solver s (start vector `cache` when given, the reference's
+ * CachedInverseDDdaggerField), store X in `cache`, Y = D^+ X, then
+ * clg_wilson_force(F, g, X, Y).  X and Y are kept by the solver between calls.
+ * A solve that fails returns its status and adds nothing to F. */
+clg_status clg_wilson_fermion_force(clg_solver s, clg_gauge F, clg_gauge g, clg_field phi, clg_field cache,
+                                    clg_solve_info* info);
+
 #ifdef __cplusplus
 }
 #endif
