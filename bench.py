@@ -386,6 +386,7 @@ def ours(args, world, rank, local):
             extra["dslash_config3"] = dslash_config3(clg, ctx, stream)
             extra["staggered_multishift_config5"] = staggered_config5(clg, ctx, stream)
             extra["wilson_force_32x32x32x16"] = wilson_force_side(clg, ctx, stream)
+            extra["staggered_force_32x32x32x16"] = ks_force_side(clg, ctx, stream)
         if world == 1 and not args.no_cpu:
             extra["cpu_baseline"] = cpu_baseline(U, lat, kappa, plain["fp64_gmres12"]["applications"])
     result = {
@@ -653,6 +654,65 @@ def wilson_force_side(clg, ctx, stream, dims=(32, 32, 32, 16), kappa=0.1355):
     return out
 
 
+def ks_force_side(clg, ctx, stream, dims=(32, 32, 32, 16), mass=0.02, poles=12):
+    """The staggered RHMC force (CalculateForceS of CFieldFermionKSSU3) with 12
+    poles on the headline lattice.  kernel: F -= force of 12 (phi_i, phi_id)
+    pairs alone, FP64, compulsory bytes per site 12 x 2 x 48 B + U 576 B + F
+    read and written 1152 B; step: one multi-shift CG solve of (DD^+ + b_i)
+    phi_i = phi (FP32 inner) to 1e-10 for every pole, the 12 D0 applications
+    and the force, from a zero start."""
+    import torch
+
+    peak, _ = peaks()
+    lat = clg.Lattice(ctx, dims)
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+    F = clg.CFieldGaugeSU3(lat)
+    F.InitialField(clg.GAUGE_ZERO)
+    pi = [clg.CFieldFermionKSSU3(lat, mass) for _ in range(poles)]
+    pd = [clg.CFieldFermionKSSU3(lat, mass) for _ in range(poles)]
+    for k in range(poles):
+        pi[k].InitialField(clg.SOURCE_GAUSS, 0xC1A60060, 2 + k)
+        pd[k].InitialField(clg.SOURCE_GAUSS, 0xC1A60061, 2 + k)
+    a = np.logspace(-3, 0.5, poles)
+    b = np.logspace(-4, 1, poles)
+    nbytes = poles * 2 * 48 + 4 * 144 + 2 * 4 * 144
+    out = {"dims": list(dims), "poles": poles, "bytes_per_site": nbytes}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        clg.CFieldFermionKSSU3.DerivateD0(F, U, pi, pd, a)
+    reps = 20
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        clg.CFieldFermionKSSU3.DerivateD0(F, U, pi, pd, a)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    gbs = nbytes * lat.volume / t / 1e9
+    out["kernel"] = {"launch_us": round(t * 1e6, 2), "GB/s": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    for f in pi + pd:
+        f.close()
+    phi = clg.CFieldFermionKSSU3(lat, mass)
+    phi.InitialField(clg.SOURCE_GAUSS, 0xC1A60062, 2)
+    S = clg.CMultiShiftCG(ctx, inner_precision=clg.SINGLE, tol_true_rel=TOL)
+    phi.CalculateForceS(U, F, S, a, b)  # warm-up (workspace, autotuner)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    infos = phi.CalculateForceS(U, F, S, a, b)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dt = e0.elapsed_time(e1) / 1e3
+    out["step"] = {"force_steps_per_s": round(1.0 / dt, 3), "seconds": round(dt, 4),
+                   "applications": max(i["iterations"] for i in infos),
+                   "worst_true_rel_residual": max(i["true_rel_residual"] for i in infos),
+                   "status": max(i["status"] for i in infos)}
+    S.close()
+    for f in (phi, F, U):
+        f.close()
+    return out
+
+
 def staggered_config5(clg, ctx, stream, steps=2):
     """32^3x16 staggered fermions, 2am = 0.02 (the reference's
     `Mass` parameter is 2am), BC (+,+,+,-), 12 shifts sigma_k = 10^(-4 + 5k/11),
@@ -803,6 +863,16 @@ def profile_driver(args):
         Y.InitialField(clg.SOURCE_GAUSS, 6, 2)
         for _ in range(args.steps):
             clg.CFieldFermionWilsonSquareSU3.DerivateDOperator(F, Y, X, U)
+    elif args.profile == "ks-force":
+        F = clg.CFieldGaugeSU3(lat)
+        F.InitialField(clg.GAUGE_ZERO)
+        pi = [clg.CFieldFermionKSSU3(lat, 0.02) for _ in range(12)]
+        pd = [clg.CFieldFermionKSSU3(lat, 0.02) for _ in range(12)]
+        for k in range(12):
+            pi[k].InitialField(clg.SOURCE_GAUSS, 7, 2 + k)
+            pd[k].InitialField(clg.SOURCE_GAUSS, 8, 2 + k)
+        for _ in range(args.steps):
+            clg.CFieldFermionKSSU3.DerivateD0(F, U, pi, pd, np.logspace(-3, 0.5, 12))
     else:
         b = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=W["nrhs"])
         for r in range(W["nrhs"]):
@@ -831,7 +901,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched config-4 side measurements")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the config-3 Dslash and config-5 staggered multi-shift side measurements")
-    ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve", "force"],
+    ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve", "force", "ks-force"],
                     help="profiling driver (no JSON line): `--steps` hop launches on the workload lattice, "
                          "or `--steps` solves without warm-up")
     args = ap.parse_args()

@@ -111,6 +111,8 @@ SIGNATURES = [
     ("clg_rational_apply", _S, [_P, _P, _P, _I, _I, _D, _P, _P, _P]),
     ("clg_wilson_force", _S, [_P, _P, _P, _P]),
     ("clg_wilson_fermion_force", _S, [_P, _P, _P, _P, _P, _P]),
+    ("clg_ks_force", _S, [_P, _P, _I, _P, _P, _P]),
+    ("clg_ks_fermion_force", _S, [_P, _P, _P, _P, _I, _P, _P, _P]),
 ]
 
 _lib = None
@@ -364,6 +366,33 @@ class CFieldFermionWilsonSquareSU3(_FermionField):
 class CFieldFermionKSSU3(_FermionField):
     """Staggered (Kogut-Susskind) fermion, param = Mass (= 2am)."""
     KIND, NC = STAGGERED, 3
+
+    @staticmethod
+    def DerivateD0(force: CFieldGaugeSU3, gauge: CFieldGaugeSU3, phi_i: Sequence["CFieldFermionKSSU3"],
+                   phi_id: Sequence["CFieldFermionKSSU3"], numerators: Sequence[float]):
+        """force -= the staggered rational force of phi_i = (DD^+ + b_i)^-1 phi and
+        phi_id = D0 phi_i with the given numerators (CFieldFermionKSSU3.cu:216-262, :316-331)."""
+        n = len(numerators)
+        if len(phi_i) != n or len(phi_id) != n:
+            raise CLGError(ERR_BAD_ARG, "one phi_i and one phi_id per numerator")
+        hi = (C.c_void_p * n)(*[f.h.value for f in phi_i])
+        hd = (C.c_void_p * n)(*[f.h.value for f in phi_id])
+        a = np.ascontiguousarray(numerators, np.float64)
+        gauge.ctx.check(gauge.ctx.lib.clg_ks_force(force.h, gauge.h, n, hi, hd, _ptr(a)), "clg_ks_force")
+
+    def CalculateForceS(self, gauge: CFieldGaugeSU3, force: CFieldGaugeSU3, solver: "_Solver",
+                        numerators: Sequence[float], shifts: Sequence[float]):
+        """force += the force of the rational pseudofermion action (the reference's
+        m_rMD: numerators a_i, shifts b_i), phi = self (CFieldFermionKSSU3.cu:412-500).
+        solver is a CMultiShiftCG (or CMultiShiftFOM).  Returns the solve infos."""
+        a = np.ascontiguousarray(numerators, np.float64)
+        b = np.ascontiguousarray(shifts, np.float64)
+        if a.size != b.size:
+            raise CLGError(ERR_BAD_ARG, "one shift per numerator")
+        infos = (SolveInfo * a.size)()
+        st = self.ctx.lib.clg_ks_fermion_force(solver.h, force.h, gauge.h, self.h, a.size, _ptr(a), _ptr(b), infos)
+        self.ctx.check(st, "clg_ks_fermion_force")
+        return [i.as_dict() for i in infos]
 
 
 class _Solver:

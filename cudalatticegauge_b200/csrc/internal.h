@@ -320,8 +320,12 @@ struct clg_solver_s {
   std::unique_ptr<clg::SolveCacheBase> cache_cgm;    // multi-shift CG vectors, state, graph
   // X = (DD^+)^-1 phi and Y = D^+ X of clg_wilson_fermion_force
   clg_field force_x = nullptr, force_y = nullptr;
+  // phi_i = (DD^+ + b_i)^-1 phi and phi_id = D0 phi_i of clg_ks_fermion_force
+  std::vector<clg_field> ks_phi_i, ks_phi_id;
   ~clg_solver_s() {
     if (force_x) clg_field_destroy(force_x);
     if (force_y) clg_field_destroy(force_y);
+    for (clg_field f : ks_phi_i) clg_field_destroy(f);
+    for (clg_field f : ks_phi_id) clg_field_destroy(f);
   }
 };

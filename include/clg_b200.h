@@ -108,7 +108,7 @@ clg_status clg_lattice_destroy(clg_lattice lat);
  *   CFieldGaugeSU3.cu:568-592); `data` holds 4*V*18 doubles, on the host unless
  *   on_device != 0.
  * export: CopyDataOutDouble (CFieldGaugeSU3.cu:1693-1760), CLGBin order.
- * random: seeded Haar SU(3), exp(i eps H) or identity links generated on the device. */
+ * random: seeded Haar SU(3), exp(i eps H), identity or zero links generated on the device. */
 clg_status clg_gauge_create(clg_lattice lat, clg_gauge* out);
 clg_status clg_gauge_destroy(clg_gauge g);
 clg_status clg_gauge_import(clg_gauge g, const double* data, int layout, int on_device);
@@ -249,6 +249,22 @@ clg_status clg_wilson_force(clg_gauge F, clg_gauge g, clg_field X, clg_field Y);
  * A solve that fails returns its status and adds nothing to F. */
 clg_status clg_wilson_fermion_force(clg_solver s, clg_gauge F, clg_gauge g, clg_field phi, clg_field cache,
                                     clg_solve_info* info);
+/* CFieldFermionKSSU3::DerivateD0 / _kernelDFermionKSForce
+ * (Data/Field/Staggered/CFieldFermionKSSU3.cu:216-262, :316-331): with the
+ * multi-shift solutions phi_i[i] = (D D^+ + b_i)^-1 phi and phi_id[i] = D0 phi_i[i]
+ * (massless D; FULL FP64 staggered fields of one right-hand side), n <= 64
+ * poles with numerators a[i], subtract from every link
+ *   F_mu(x) -= sum_i Ta(s eta_mu(x) a_i [U_mu(x) phi_i(x+mu) phi_id(x)^+ + phi_i(x) (U_mu(x) phi_id(x+mu))^+])
+ * (s the fermion boundary sign of the hop x -> x+mu, eta_mu the staggered phase). */
+clg_status clg_ks_force(clg_gauge F, clg_gauge g, int n, const clg_field* phi_i, const clg_field* phi_id,
+                        const double* a);
+/* CFieldFermionKSSU3::CalculateForceS (same file :412-500): one multi-shift
+ * solve (s is a CGM or FOM_MS solver) of (D D^+ + b_i) phi_i = phi for the
+ * `degree` poles of the molecular-dynamics rational approximation (numerators
+ * a, shifts b: the reference's m_rMD), phi_id = D0 phi_i, then clg_ks_force.
+ * info holds `degree` entries.  A failed solve adds nothing to F. */
+clg_status clg_ks_fermion_force(clg_solver s, clg_gauge F, clg_gauge g, clg_field phi, int degree, const double* a,
+                                const double* b, clg_solve_info* info);
 
 #ifdef __cplusplus
 }

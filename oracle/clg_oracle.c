@@ -374,6 +374,53 @@ void clgo_ks_dddag_ee(const clgo_lat* lat, const double* U, double mass2am,
     }
 }
 
+/* ============================================================== staggered rational force
+ * _kernelDFermionKSForce (Staggered/CFieldFermionKSSU3.cu:216-262), launched by
+ * DerivateD0 (:316-331) from CalculateForceS (:412-500): with the multi-shift
+ * solutions phi_i = (D D^+ + b_i)^-1 phi and phi_id = D0 phi_i (the massless D),
+ *   F_mu(x) -= Ta( s_+ eta_mu(x) a_i [ U_mu(x) phi_i(x+mu) phi_id(x)^+
+ *                                     + phi_i(x) (U_mu(x) phi_id(x+mu))^+ ] )
+ * summed over i (makeSU3ContractV(l, r) = r l^+, SU3.h:505-519).  phi_i and
+ * phi_id hold n fields of V*3 complex one after another. */
+void clgo_ks_force(const clgo_lat* lat, const double* U, int n, const double* phi_i, const double* phi_id,
+                   const double* a, double* F) {
+    const long V = lat_volume(lat->L);
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s) {
+        int c[4];
+        coords_of(lat->L, s, c);
+        for (int mu = 0; mu < 4; ++mu) {
+            int sg = 1;
+            const long sp = neighbour(lat->L, lat->bc, c, mu, 1, &sg);
+            cplx u[9], f[9], term[9];
+            su3_load(U, 4 * s + mu, u);
+            su3_load(F, 4 * s + mu, f);
+            const double w0 = eta_of(c, mu) * (double)sg;
+            for (int i = 0; i < n; ++i) {
+                const double* pi = phi_i + (long)i * 6 * V;
+                const double* pd = phi_id + (long)i * 6 * V;
+                cplx vi_x[3], vd_x[3], vi_p[3], vd_p[3], t1[3], t2[3];
+                for (int k = 0; k < 3; ++k) {
+                    vi_x[k] = pi[6 * s + 2 * k] + I * pi[6 * s + 2 * k + 1];
+                    vd_x[k] = pd[6 * s + 2 * k] + I * pd[6 * s + 2 * k + 1];
+                    vi_p[k] = pi[6 * sp + 2 * k] + I * pi[6 * sp + 2 * k + 1];
+                    vd_p[k] = pd[6 * sp + 2 * k] + I * pd[6 * sp + 2 * k + 1];
+                }
+                su3_mulvec(u, vi_p, t1);
+                su3_mulvec(u, vd_p, t2);
+                for (int r = 0; r < 3; ++r)
+                    for (int q = 0; q < 3; ++q)
+                        term[3 * r + q] = t1[r] * conj(vd_x[q]) + vi_x[r] * conj(t2[q]);
+                const double w = w0 * a[i];
+                for (int k = 0; k < 9; ++k) term[k] *= w;
+                su3_ta(term);
+                for (int k = 0; k < 9; ++k) f[k] -= term[k];
+            }
+            su3_store(F, 4 * s + mu, f);
+        }
+    }
+}
+
 /* ============================================================== generic op */
 long clgo_op_len(const clgo_op* op) {
     const long V = lat_volume(op->lat.L);

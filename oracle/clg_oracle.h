@@ -61,6 +61,9 @@ void clgo_wilson_force(const clgo_lat* lat, const double* U, double kappa, const
 void clgo_ks_D(const clgo_lat* lat, const double* U, double mass2am, int dagger,
                int coeff_type, double cre, double cim, const double* in, double* out);
 void clgo_ks_hop(const clgo_lat* lat, const double* U, int out_parity, const double* in, double* out);
+/* F -= staggered rational force of phi_i = (DD^+ + b_i)^-1 phi, phi_id = D0 phi_i, numerators a (n fields each) */
+void clgo_ks_force(const clgo_lat* lat, const double* U, int n, const double* phi_i, const double* phi_id,
+                   const double* a, double* F);
 void clgo_ks_dddag_ee(const clgo_lat* lat, const double* U, double mass2am,
                       const double* in, double* out, double* tmp);
 

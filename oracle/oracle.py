@@ -90,6 +90,7 @@ def lib():
             "clgo_ks_D": (None, [p, p, d, i, i, d, d, p, p]),
             "clgo_ks_hop": (None, [p, p, i, p, p]),
             "clgo_ks_dddag_ee": (None, [p, p, d, p, p, p]),
+            "clgo_ks_force": (None, [p, p, i, p, p, p, p]),
             "clgo_op_len": (l, [p]),
             "clgo_apply": (None, [p, p, p]),
             "clgo_dot": (None, [l, p, p, p]),
@@ -230,6 +231,19 @@ def wilson_force(L, U, X, Y, kappa, F=None, bc=(1, 1, 1, -1)):
     out = np.zeros_like(np.ascontiguousarray(U, np.complex128)) if F is None else np.array(F, np.complex128)
     lat = _lat(L, bc)
     lib().clgo_wilson_force(C.byref(lat), _ptr(U), kappa, _ptr(X), _ptr(Y), _ptr(out))
+    return out
+
+
+def ks_force(L, U, phi_i, phi_id, a, F=None, bc=(1, 1, 1, -1)):
+    """F - the staggered rational force (_kernelDFermionKSForce,
+    Staggered/CFieldFermionKSSU3.cu:216-262) of the fields phi_i[n] =
+    (DD^+ + b_n)^-1 phi and phi_id[n] = D0 phi_i[n] with numerators a[n]."""
+    pi = np.ascontiguousarray(np.stack([np.asarray(x, np.complex128).reshape(-1) for x in phi_i]))
+    pd = np.ascontiguousarray(np.stack([np.asarray(x, np.complex128).reshape(-1) for x in phi_id]))
+    aa = np.ascontiguousarray(a, np.float64)
+    out = np.zeros_like(np.ascontiguousarray(U, np.complex128)) if F is None else np.array(F, np.complex128)
+    lat = _lat(L, bc)
+    lib().clgo_ks_force(C.byref(lat), _ptr(U), len(aa), _ptr(pi), _ptr(pd), _ptr(aa), _ptr(out))
     return out
 
 

@@ -231,3 +231,46 @@ def test_wilson_force_is_the_action_derivative(oracle):
         dS = (S_at(eps) - S_at(-eps)) / (2 * eps)
         want = (2j * np.trace(T @ F[link])).real
         assert abs(dS - want) <= 1e-6 * max(1.0, abs(want)), (link, dS, want)
+
+
+def test_ks_force_is_the_rational_action_derivative(oracle):
+    """The staggered rational force as the oracle restates _kernelDFermionKSForce
+    (Staggered/CFieldFermionKSSU3.cu:216-262) is the derivative of
+    S = sum_i a_i phi^+ (DD^+ + b_i)^-1 phi, the U-dependent part of the RHMC
+    action whose force CalculateForceS (:412-500) computes from the multi-shift
+    solutions phi_i and phi_id = D0 phi_i: dS/de = 2 i Tr(T F_mu(x)) for
+    U_mu(x) -> exp(i e T) U_mu(x), on links of every direction, including ones
+    that cross the antiperiodic t boundary and the periodic x boundary."""
+    L = (4, 4, 4, 4)
+    V = oracle.volume(L)
+    m = 0.3
+    U = oracle.gauge_expH(L, 0xC1A60022, 0.3)
+    phi = oracle.gauss(V, 3, 8, 2).reshape(V, 3)
+    a = np.array([0.3, 0.7, 1.1])
+    b = np.array([0.05, 0.4, 2.0])
+
+    def action(Ul):
+        op = oracle.Operator("KS_DDDAG", L, Ul, m)
+        xs, info = oracle.cgm(op, phi, list(b), tol=1e-13)
+        return sum(a[i] * np.vdot(phi, xs[i]).real for i in range(len(a))), xs
+
+    _, xs = action(U)
+    F = oracle.ks_force(L, U, xs, [oracle.ks_D(L, U, x, 0.0) for x in xs], a)
+    assert np.abs(F + np.conj(np.transpose(F, (0, 2, 1)))).max() < 1e-14
+    assert np.abs(np.trace(F, axis1=1, axis2=2)).max() < 1e-14
+    rng = np.random.default_rng(6)
+    for link in [4 * (V - 1) + 0, 4 * 63 + 3, 77, 130, 4 * 5 + 0]:
+        A = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+        T = (A + A.conj().T) / 2
+        T -= np.trace(T) / 3 * np.eye(3)
+        w, Q = np.linalg.eigh(T)
+        eps = 1e-5
+
+        def S_at(e):
+            U2 = U.copy()
+            U2[link] = (Q @ np.diag(np.exp(1j * e * w)) @ Q.conj().T) @ U[link]
+            return action(U2)[0]
+
+        dS = (S_at(eps) - S_at(-eps)) / (2 * eps)
+        want = (2j * np.trace(T @ F[link])).real
+        assert abs(dS - want) <= 1e-6 * max(1.0, abs(want)), (link, dS, want)
