@@ -55,7 +55,8 @@ struct ForceArgs {
 // copies into shared memory -- 96 KB in flight per block, two blocks per SM,
 // instead of the few hundred bytes a thread can hold in registers -- then
 // computed from there.  On 32^3 x 16 this took the kernel from 0.51 to 0.82 of
-// the measured copy bandwidth (331 -> 207 us; staging all but F: 440 us).
+// the measured copy bandwidth (331 -> 207 us; staging all but F: 440 us; a
+// persistent form with one block per SM double-buffering its tiles: 217 us).
 constexpr int TILE = 32;
 constexpr int E_HERE = 2 * 12 * TILE;    // X(x), Y(x)           [field][k][site]
 constexpr int E_NBR = 4 * 2 * 12 * TILE; // X(x+mu), Y(x+mu)     [mu][field][k][site]
@@ -65,6 +66,11 @@ constexpr size_t FORCE_SMEM = sizeof(double2) * (E_HERE + E_NBR + 2 * E_LINK);  
 __device__ __forceinline__ void cp_async16(double2* smem, const double2* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
@@ -281,11 +287,6 @@ struct KsForceArgs {
   double a[KS_FORCE_MAX];
 };
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 // m[r][q] += w * l[r] conj(r[q])
 __device__ __forceinline__ void outer3_acc(C m[9], double w, const double2* l, const double2* r) {
