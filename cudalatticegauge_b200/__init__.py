@@ -35,6 +35,9 @@ FULL, EVEN = 0, 1
 DOUBLE, SINGLE, HALF = 0, 1, 2
 LAYOUT_CLGBIN, LAYOUT_BRIDGEPP = 0, 1
 GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
+# clg_file_format (EFieldFileType)
+(FILE_CLGBIN_DOUBLE, FILE_CLGBIN_FLOAT, FILE_CLGBIN_COMPRESSED, FILE_CLGBIN_COMPRESSED_FLOAT, FILE_BRIDGEPP_BIN,
+ FILE_BRIDGEPP_TXT) = range(6)
 SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT = 0, 1, 2, 3
 SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS = 0, 1, 2, 3, 4
 
@@ -109,6 +112,11 @@ SIGNATURES = [
     ("clg_solve", _S, [_P, _P, _P, _P, _I, _P, _P]),
     ("clg_solve_multishift", _S, [_P, _P, _I, _P, _P, _P, _I, _P]),
     ("clg_rational_apply", _S, [_P, _P, _P, _I, _I, _D, _P, _P, _P]),
+    ("clg_gauge_load", _S, [_P, C.c_char_p, _I]),
+    ("clg_gauge_save", _S, [_P, C.c_char_p, _I, C.c_char_p]),
+    ("clg_md5", _S, [_P, C.c_size_t, C.c_char_p]),
+    ("clg_field_save", _S, [_P, _I, C.c_char_p, _I, C.c_char_p]),
+    ("clg_field_load", _S, [_P, _I, C.c_char_p, _I]),
     ("clg_wilson_force", _S, [_P, _P, _P, _P]),
     ("clg_wilson_fermion_force", _S, [_P, _P, _P, _P, _P, _P]),
     ("clg_ks_force", _S, [_P, _P, _I, _P, _P, _P]),
@@ -213,6 +221,16 @@ class CFieldGaugeSU3:
         self.ctx.check(self.ctx.lib.clg_gauge_export(self.h, _ptr(out), 0), "clg_gauge_export")
         return out
 
+    def InitialFieldWithFile(self, path: str, fmt: int = FILE_CLGBIN_DOUBLE):
+        """CFieldGaugeSU3::InitialFieldWithFile (CFieldGaugeSU3.cu:1080-1265)."""
+        self.ctx.check(self.ctx.lib.clg_gauge_load(self.h, os.fsencode(path), fmt), "clg_gauge_load")
+
+    def SaveToFile(self, path: str, fmt: int = FILE_CLGBIN_DOUBLE) -> str:
+        """CField::SaveToFile / SaveToCompressedFile; returns the MD5 of the bytes written."""
+        out = C.create_string_buffer(33)
+        self.ctx.check(self.ctx.lib.clg_gauge_save(self.h, os.fsencode(path), fmt, out), "clg_gauge_save")
+        return out.value.decode()
+
     def plaquette(self) -> float:
         v = C.c_double()
         self.ctx.check(self.ctx.lib.clg_gauge_plaquette(self.h, C.byref(v)), "clg_gauge_plaquette")
@@ -277,6 +295,16 @@ class _FermionField:
     def wait(self):
         self.ctx.check(self.ctx.lib.clg_field_wait(self.h), "clg_field_wait")
         self._inflight = []
+
+    def InitialFieldWithFile(self, path: str, fmt: int = FILE_CLGBIN_DOUBLE, rhs: int = 0):
+        """InitialFieldWithFile for a fermion field: CLGBin double or float."""
+        self.ctx.check(self.ctx.lib.clg_field_load(self.h, rhs, os.fsencode(path), fmt), "clg_field_load")
+
+    def SaveToFile(self, path: str, fmt: int = FILE_CLGBIN_DOUBLE, rhs: int = 0) -> str:
+        """CField::SaveToFile for one right-hand side; returns the MD5 of the bytes written."""
+        out = C.create_string_buffer(33)
+        self.ctx.check(self.ctx.lib.clg_field_save(self.h, rhs, os.fsencode(path), fmt, out), "clg_field_save")
+        return out.value.decode()
 
     def InitialField(self, kind: int, seed: int = 0, field_id: int = 2, rhs: int = 0, site: int = 0, comp: int = 0):
         self.ctx.check(self.ctx.lib.clg_field_random(self.h, rhs, kind, seed, field_id, site, comp), "clg_field_random")
@@ -471,6 +499,16 @@ class CMultiShiftCG(_MultiShift):
 
 class CMultiShiftFOM(_MultiShift):
     KIND = SOLVER_FOM_MS
+
+
+def md5(data) -> str:
+    """CLGMD5Hash of a bytes-like object through the library (RFC 1321)."""
+    b = bytes(data)
+    out = C.create_string_buffer(33)
+    st = load_library().clg_md5(b, len(b), out)
+    if st != SUCCESS:
+        raise CLGError(st, "clg_md5")
+    return out.value.decode()
 
 
 def eo_parity(dims) -> np.ndarray:

@@ -65,6 +65,18 @@ typedef enum { CLG_PREC_DOUBLE = 0, CLG_PREC_SINGLE = 1, CLG_PREC_HALF = 2 } clg
 typedef enum { CLG_LAYOUT_CLGBIN = 0, CLG_LAYOUT_BRIDGEPP = 1 } clg_layout;
 /* ZERO: all links 0 (a force accumulator, CFieldGaugeSU3::InitialField(EFIT_Zero)) */
 typedef enum { CLG_GAUGE_IDENTITY = 0, CLG_GAUGE_HAAR = 1, CLG_GAUGE_EXPH = 2, CLG_GAUGE_ZERO = 3 } clg_gauge_init;
+/* EFieldFileType (Data/Field/CField.h): CLGBin double / float (18 reals per
+ * link, CLGBin order), CLGBin compressed (9 reals per link: log U; the
+ * reference writes its build's Real, so both widths exist), Bridge++ binary
+ * (big-endian doubles) and text (one value per line), Bridge++ site order */
+typedef enum {
+    CLG_FILE_CLGBIN_DOUBLE = 0,           /* EFFT_CLGBinDouble (EFFT_CLGBin in a double build)    */
+    CLG_FILE_CLGBIN_FLOAT = 1,            /* EFFT_CLGBinFloat                                     */
+    CLG_FILE_CLGBIN_COMPRESSED = 2,       /* EFFT_CLGBinCompressed, double build                  */
+    CLG_FILE_CLGBIN_COMPRESSED_FLOAT = 3, /* EFFT_CLGBinCompressed, single-precision build        */
+    CLG_FILE_BRIDGEPP_BIN = 4,            /* EFFT_BridgePPBin                                     */
+    CLG_FILE_BRIDGEPP_TXT = 5             /* EFFT_BridgePPTXT                                     */
+} clg_file_format;
 typedef enum { CLG_SOURCE_ZERO = 0, CLG_SOURCE_GAUSS = 1, CLG_SOURCE_Z2 = 2, CLG_SOURCE_POINT = 3 } clg_source_kind;
 typedef enum {
     CLG_SOLVER_GMRES = 0,       /* CSLASolverGMRES    SparseLinearAlgebra/CSolverGMRES.cpp:111-358   */
@@ -114,6 +126,17 @@ clg_status clg_gauge_destroy(clg_gauge g);
 clg_status clg_gauge_import(clg_gauge g, const double* data, int layout, int on_device);
 clg_status clg_gauge_export(clg_gauge g, double* data, int on_device);
 clg_status clg_gauge_random(clg_gauge g, int init, uint64_t seed, uint32_t field_id, double eps);
+/* Files.  load: CFieldGaugeSU3::InitialFieldWithFile (CFieldGaugeSU3.cu:1080-1265),
+ * every clg_file_format; the file size must match the lattice.  save:
+ * CField::SaveToFile / SaveToCompressedFile (Data/Field/CField.cpp:32-72,
+ * CFieldGaugeSU3.cu:1651-1690), md5_hex_out (nullable, 33 chars) receives the
+ * MD5 of the bytes written as the reference returns it.  The reference writes
+ * no Bridge++ files; here both Bridge++ forms can be written too.  Compressed
+ * saves need SU(3) links (clg_gauge_unitarity < 1e-12). */
+clg_status clg_gauge_load(clg_gauge g, const char* path, int format);
+clg_status clg_gauge_save(clg_gauge g, const char* path, int format, char* md5_hex_out);
+/* MD5 (RFC 1321) of a host buffer as 32 lowercase hex digits + NUL (CLGMD5Hash) */
+clg_status clg_md5(const void* data, size_t bytes, char* md5_hex_out);
 /* average (1/3) Re tr of the plaquette (TestConfigurationFileIO.cpp:12-38 known answer) */
 clg_status clg_gauge_plaquette(clg_gauge g, double* out);
 /* max |U U^+ - 1| and |det U - 1| over links; the 12-real FP32/FP16 copies are
@@ -154,6 +177,10 @@ clg_status clg_field_wait(clg_field f);
  * GAUSS (E|z|^2 = 1), Z2 ((+-1 +- i)/sqrt 2), POINT (site, spin*3+colour), ZERO. */
 clg_status clg_field_random(clg_field f, int rhs, int kind, uint64_t seed, uint32_t field_id, int64_t site, int comp);
 clg_status clg_field_copy(clg_field dst, clg_field src);  /* CopyTo; converts precision */
+/* CField::SaveToFile / InitialFieldWithFile for fermion fields: one right-hand
+ * side as CLGBin double or float (24 or 6 reals per site, CLGBin order) */
+clg_status clg_field_save(clg_field f, int rhs, const char* path, int format, char* md5_hex_out);
+clg_status clg_field_load(clg_field f, int rhs, const char* path, int format);
 
 /* ------------------------------------------------------------------ operators
  * CField::ApplyOperator (Data/Field/CField.h:203): in place, the field is both

@@ -7,11 +7,19 @@ path below, or pass it as the first argument).  Outputs, next to this script:
                          (Bin/Debug/bridgepp_conf_text.dat) as float64, Bridge++
                          order; known plaquette 0.625129946974942
                          (Code/CLGTest/Tests/TestConfigurationFileIO.cpp:12-38)
+  fileio.json            MD5 digests of the reference's configuration files
+                         Bin/Release/bridgepp_conf_binary.dat (the same 4^3x8
+                         configuration as big-endian doubles; checked here to
+                         hold exactly the text file's values) and
+                         Bin/Debug/testGaugeDouble.con_ / testGaugeSingle.con_
+                         (8^4 CLGBin double / float), with the sum of |U|^2 that
+                         TestConfigurationFileIO.cpp expects of the latter (49152)
   gamma_chiral.json      the chiral gamma-matrix table parsed from
                          Code/CLGLib/Tools/Math/GammaMatrix.h (the `else` branch of
                          gammaMatrixSet::CreateGammaMatrix): for GAMMA1..GAMMA5, per
                          row the non-zero column and the power b of i^b
 """
+import hashlib
 import json
 import os
 import re
@@ -28,6 +36,19 @@ def main(ref="/root/reference"):
     assert vals.size == 4 * 4 * 4 * 8 * 4 * 18
     np.savez_compressed(os.path.join(HERE, "bridgepp_4x4x4x8.npz"), links=vals,
                         dims=np.array([4, 4, 4, 8]), plaquette=np.array(0.625129946974942))
+
+    binf = os.path.join(ref, "Bin", "Release", "bridgepp_conf_binary.dat")
+    raw = open(binf, "rb").read()
+    assert np.array_equal(np.frombuffer(raw, dtype=">f8").astype(np.float64), vals)
+    info = {"bridgepp_conf_binary.dat": {"md5": hashlib.md5(raw).hexdigest(), "bytes": len(raw),
+                                         "dims": [4, 4, 4, 8], "equals": "bridgepp_4x4x4x8.npz links, big-endian"}}
+    for name, dt in (("testGaugeDouble.con_", "<f8"), ("testGaugeSingle.con_", "<f4")):
+        raw = open(os.path.join(ref, "Bin", "Debug", name), "rb").read()
+        u = np.frombuffer(raw, dtype=dt).astype(np.float64)
+        info[name] = {"md5": hashlib.md5(raw).hexdigest(), "bytes": len(raw), "dims": [8, 8, 8, 8],
+                      "sum_abs2": float(np.dot(u, u)), "expected_sum_abs2": 49152.0}
+    with open(os.path.join(HERE, "fileio.json"), "w") as f:
+        json.dump(info, f, indent=1)
 
     src = open(os.path.join(ref, "Code", "CLGLib", "Tools", "Math", "GammaMatrix.h")).read()
     start = src.index("CreateGammaMatrix(EGammaMatrixSet eSet")

@@ -4,6 +4,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -56,3 +57,28 @@ def test_no_device_is_an_error_not_a_crash(lib_path):
     with pytest.raises(clg.CLGError) as e:
         clg.Context(0)
     assert e.value.status == clg.ERR_NO_DEVICE
+
+
+def test_md5_rfc1321_vectors(lib_path):
+    """CLGMD5Hash: the RFC 1321 test suite, and hashlib on lengths around the
+    64-byte block and padding boundaries (host code, no GPU)."""
+    import hashlib
+
+    import cudalatticegauge_b200 as clg
+
+    clg.load_library(lib_path)
+    suite = {
+        b"": "d41d8cd98f00b204e9800998ecf8427e",
+        b"a": "0cc175b9c0f1b6a831c399e269772661",
+        b"abc": "900150983cd24fb0d6963f7d28e17f72",
+        b"message digest": "f96b697d7cb7938d525a2f31aaf161d0",
+        b"abcdefghijklmnopqrstuvwxyz": "c3fcd3d76192e4007dfb496cca67e13b",
+        b"ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789": "d174ab98d277d9f5a5611c2c9f419d9f",
+        b"1234567890" * 8: "57edf4a22be3c955ac49da2e2107b67a",
+    }
+    for msg, want in suite.items():
+        assert clg.md5(msg) == want
+    rng = np.random.default_rng(11)
+    for n in (55, 56, 57, 63, 64, 65, 119, 120, 128, 1 << 20):
+        b = rng.integers(0, 256, n, dtype=np.uint8).tobytes()
+        assert clg.md5(b) == hashlib.md5(b).hexdigest(), n
