@@ -38,7 +38,7 @@ GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
 # clg_file_format (EFieldFileType)
 (FILE_CLGBIN_DOUBLE, FILE_CLGBIN_FLOAT, FILE_CLGBIN_COMPRESSED, FILE_CLGBIN_COMPRESSED_FLOAT, FILE_BRIDGEPP_BIN,
  FILE_BRIDGEPP_TXT) = range(6)
-SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT = 0, 1, 2, 3
+SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT, SOURCE_Z4 = 0, 1, 2, 3, 4
 SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS = 0, 1, 2, 3, 4
 
 
@@ -121,6 +121,10 @@ SIGNATURES = [
     ("clg_wilson_fermion_force", _S, [_P, _P, _P, _P, _P, _P]),
     ("clg_ks_force", _S, [_P, _P, _I, _P, _P, _P]),
     ("clg_ks_fermion_force", _S, [_P, _P, _P, _P, _I, _P, _P, _P]),
+    ("clg_meson_correlator", _S, [_P, _P, _P, _I, _P, _P, _P]),
+    ("clg_meson_contract", _S, [_P, _I, _P, _P]),
+    ("clg_chiral_condensate", _S, [_P, _P, _P, _P, C.c_uint64, _P, _P]),
+    ("clg_condensate_contract", _S, [_P, _P, _P]),
 ]
 
 _lib = None
@@ -499,6 +503,75 @@ class CMultiShiftCG(_MultiShift):
 
 class CMultiShiftFOM(_MultiShift):
     KIND = SOLVER_FOM_MS
+
+
+# EGammaMatrix (clg_gamma)
+GAMMAS = ["UNITY", "GAMMA1", "GAMMA2", "GAMMA3", "GAMMA4", "GAMMA5", "GAMMA51", "GAMMA52", "GAMMA53", "GAMMA54",
+          "GAMMA15", "GAMMA25", "GAMMA35", "GAMMA45", "SIGMA12", "SIGMA23", "SIGMA31", "SIGMA41", "SIGMA42", "SIGMA43",
+          "SIGMA12E", "SIGMA23E", "SIGMA31E", "CHARGECONJG"]
+
+
+def _gamma_ids(gammas):
+    return np.ascontiguousarray([GAMMAS.index(g) if isinstance(g, str) else int(g) for g in gammas], np.int32)
+
+
+class CMeasureMesonCorrelator:
+    """Meson correlator of the 12 point-source propagators at the origin
+    (Measurement/CMeasureMesonCorrelator.cu): Calculate() solves them in one
+    batched call and returns {gamma: C(t)}; the running average over
+    configurations is kept as the reference's m_lstResults."""
+
+    def __init__(self, solver: "_Solver", lattice: Lattice, kappa: float, gammas=("UNITY",)):
+        self.solver, self.lat, self.kappa = solver, lattice, kappa
+        self.gammas = list(gammas)
+        self.prop = CFieldFermionWilsonSquareSU3(lattice, kappa, nrhs=12)
+        self.results = None
+        self.count = 0
+
+    def contract(self, prop: "CFieldFermionWilsonSquareSU3") -> dict:
+        ids = _gamma_ids(self.gammas)
+        out = np.zeros((len(ids), self.lat.dims[3]), np.float64)
+        self.lat.ctx.check(self.lat.ctx.lib.clg_meson_contract(prop.h, len(ids), _ptr(ids), _ptr(out)),
+                           "clg_meson_contract")
+        return {g: out[k] for k, g in enumerate(self.gammas)}
+
+    def Calculate(self, gauge: CFieldGaugeSU3):
+        ids = _gamma_ids(self.gammas)
+        out = np.zeros((len(ids), self.lat.dims[3]), np.float64)
+        infos = (SolveInfo * 12)()
+        st = self.lat.ctx.lib.clg_meson_correlator(self.solver.h, gauge.h, self.prop.h, len(ids), _ptr(ids), _ptr(out),
+                                                   infos)
+        self.lat.ctx.check(st, "clg_meson_correlator")
+        self.results = out if self.results is None else (self.results * self.count + out) / (self.count + 1)
+        self.count += 1
+        return {g: out[k] for k, g in enumerate(self.gammas)}, [i.as_dict() for i in infos]
+
+
+class CMeasureChiralCondensate:
+    """Z4-noise condensate traces (Measurement/CMeasureChiralCondensate.cu):
+    Calculate() draws `fields` Z4 noise vectors, solves them in one batched call
+    and returns the nine traces (1, gamma1..gamma5, gamma4 gamma5, gamma1, gamma2)
+    averaged over the noise vectors."""
+
+    def __init__(self, solver: "_Solver", lattice: Lattice, kappa: float, fields: int = 8):
+        self.solver, self.lat = solver, lattice
+        self.eta = CFieldFermionWilsonSquareSU3(lattice, kappa, nrhs=fields)
+        self.psi = CFieldFermionWilsonSquareSU3(lattice, kappa, nrhs=fields)
+
+    def Calculate(self, gauge: CFieldGaugeSU3, seed: int = 0):
+        out = np.zeros(18, np.float64)
+        infos = (SolveInfo * self.eta.nrhs)()
+        st = self.lat.ctx.lib.clg_chiral_condensate(self.solver.h, gauge.h, self.eta.h, self.psi.h, seed, _ptr(out),
+                                                    infos)
+        self.lat.ctx.check(st, "clg_chiral_condensate")
+        return out[0::2] + 1j * out[1::2], [i.as_dict() for i in infos]
+
+    @staticmethod
+    def contract(eta: "CFieldFermionWilsonSquareSU3", psi: "CFieldFermionWilsonSquareSU3") -> np.ndarray:
+        """per right-hand side r and kind k: (1/V) sum_x eta_r^+ Gamma_k psi_r, shape (nrhs, 9) complex"""
+        out = np.zeros(eta.nrhs * 18, np.float64)
+        eta.ctx.check(eta.ctx.lib.clg_condensate_contract(eta.h, psi.h, _ptr(out)), "clg_condensate_contract")
+        return (out[0::2] + 1j * out[1::2]).reshape(eta.nrhs, 9)
 
 
 def md5(data) -> str:

@@ -615,7 +615,7 @@ clg_status clg_field_export(clg_field f, int rhs, double* data, int on_device) {
 }
 
 clg_status clg_field_random(clg_field f, int rhs, int kind, uint64_t seed, uint32_t field_id, int64_t site, int comp) {
-  if (!f || rhs < 0 || rhs >= f->nrhs || kind < 0 || kind > 3) return CLG_ERR_BAD_ARG;
+  if (!f || rhs < 0 || rhs >= f->nrhs || kind < 0 || kind > CLG_SOURCE_Z4) return CLG_ERR_BAD_ARG;
   if (kind == CLG_SOURCE_POINT && (site < 0 || site >= f->lat->g.V || comp < 0 || comp >= f->nc())) return CLG_ERR_BAD_ARG;
   if (clg_status st = settle(f)) return st;
   return field_source(f, rhs, kind, seed, field_id, site, comp);

@@ -17,7 +17,7 @@ namespace clg {
 
 namespace {
 
-constexpr uint32_t TAG_GAUGE = 0x47415547u, TAG_SPINOR = 0x5350494eu, TAG_Z2 = 0x5a324e53u;
+constexpr uint32_t TAG_GAUGE = 0x47415547u, TAG_SPINOR = 0x5350494eu, TAG_Z2 = 0x5a324e53u, TAG_Z4 = 0x5a344e53u;
 
 __device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
@@ -274,6 +274,14 @@ struct SourceF {
         const int b0 = 2 * k, b1 = 2 * k + 1;
         const uint32_t x0 = w[b0 >> 5] >> (b0 & 31), x1 = w[b1 >> 5] >> (b1 & 31);
         v[k] = mk<double>((x0 & 1u) ? -isq2 : isq2, (x1 & 1u) ? -isq2 : isq2);
+      }
+    } else if (kind == CLG_SOURCE_Z4) {
+      // i^b, b = bits 2k, 2k+1 of one Philox output
+      uint32_t w[4] = {(uint32_t)s, (uint32_t)((uint64_t)s >> 32), 0u, TAG_Z4};
+      philox(w, (uint32_t)seed, (uint32_t)(seed >> 32) ^ fid);
+      for (int k = 0; k < NC; ++k) {
+        const uint32_t b = (w[(2 * k) >> 5] >> ((2 * k) & 31)) & 3u;
+        v[k] = mk<double>(b == 0 ? 1.0 : (b == 2 ? -1.0 : 0.0), b == 1 ? 1.0 : (b == 3 ? -1.0 : 0.0));
       }
     } else {
       for (int k = 0; k < NC; ++k) v[k] = mk<double>((kind == CLG_SOURCE_POINT && s == site && k == comp) ? 1.0 : 0.0, 0);

@@ -77,7 +77,9 @@ typedef enum {
     CLG_FILE_BRIDGEPP_BIN = 4,            /* EFFT_BridgePPBin                                     */
     CLG_FILE_BRIDGEPP_TXT = 5             /* EFFT_BridgePPTXT                                     */
 } clg_file_format;
-typedef enum { CLG_SOURCE_ZERO = 0, CLG_SOURCE_GAUSS = 1, CLG_SOURCE_Z2 = 2, CLG_SOURCE_POINT = 3 } clg_source_kind;
+/* Z2: (+-1 +- i)/sqrt 2 per component; Z4: one of 1, i, -1, -i per component
+ * (EFIT_RandomZ4, Random.h _deviceRandomZ4) */
+typedef enum { CLG_SOURCE_ZERO = 0, CLG_SOURCE_GAUSS = 1, CLG_SOURCE_Z2 = 2, CLG_SOURCE_POINT = 3, CLG_SOURCE_Z4 = 4 } clg_source_kind;
 typedef enum {
     CLG_SOLVER_GMRES = 0,       /* CSLASolverGMRES    SparseLinearAlgebra/CSolverGMRES.cpp:111-358   */
     CLG_SOLVER_BICGSTAB = 1,    /* CSLASolverBiCGStab SparseLinearAlgebra/CSolverBiCGstab.cpp:403-607 */
@@ -292,6 +294,40 @@ clg_status clg_ks_force(clg_gauge F, clg_gauge g, int n, const clg_field* phi_i,
  * info holds `degree` entries.  A failed solve adds nothing to F. */
 clg_status clg_ks_fermion_force(clg_solver s, clg_gauge F, clg_gauge g, clg_field phi, int degree, const double* a,
                                 const double* b, clg_solve_info* info);
+
+/* ------------------------------------------------------------------ measurements
+ * EGammaMatrix (Core/CudaHelper.h:37-63), chiral set and products as
+ * gammaMatrixSet::CreateGammaMatrix (Tools/Math/GammaMatrix.h:405-511). */
+typedef enum {
+    CLG_GAMMA_UNITY = 0, CLG_GAMMA1, CLG_GAMMA2, CLG_GAMMA3, CLG_GAMMA4, CLG_GAMMA5, CLG_GAMMA51, CLG_GAMMA52,
+    CLG_GAMMA53, CLG_GAMMA54, CLG_GAMMA15, CLG_GAMMA25, CLG_GAMMA35, CLG_GAMMA45, CLG_SIGMA12, CLG_SIGMA23,
+    CLG_SIGMA31, CLG_SIGMA41, CLG_SIGMA42, CLG_SIGMA43, CLG_SIGMA12E, CLG_SIGMA23E, CLG_SIGMA31E, CLG_CHARGECONJG,
+    CLG_GAMMA_COUNT
+} clg_gamma;
+/* CMeasureMesonCorrelator::CalculateCorrelator (Measurement/CMeasureMesonCorrelator.cu:254-411):
+ * the 12 spin-colour point sources at the origin solved in one batched call of
+ * solver s into prop (a FULL FP64 Wilson field of 12 right-hand sides, rhs =
+ * spin*3 + colour, kappa = its param; info holds 12 entries), then
+ * clg_meson_contract.  corr receives ngamma x Lt doubles, corr[k*Lt + t]. */
+clg_status clg_meson_correlator(clg_solver s, clg_gauge g, clg_field prop, int ngamma, const int* gammas, double* corr,
+                                clg_solve_info* info);
+/* _kernelCalculateCorrelatorSU3 (same file :26-174) on given propagators and the
+ * spatial sums per time slice times 2/sqrt(V) (:366-380) */
+clg_status clg_meson_contract(clg_field prop, int ngamma, const int* gammas, double* corr);
+/* Stochastic condensate (CMeasurementManager.cpp:71-115 with
+ * CMeasureChiralCondensate::OnConfigurationAcceptedZ4SingleField,
+ * Measurement/CMeasureChiralCondensate.cu:236-290): one Z4 noise vector per
+ * right-hand side of eta (seed, field id = rhs + 1), psi = D^-1 eta in one
+ * batched solve, then the nine traces of clg_condensate_contract averaged over
+ * the noise vectors: re_im receives 9 complex numbers. */
+clg_status clg_chiral_condensate(clg_solver s, clg_gauge g, clg_field eta, clg_field psi, uint64_t seed, double* re_im,
+                                 clg_solve_info* info);
+/* _kernelDotMeasureAll (same file :38-100) summed over sites: per right-hand
+ * side r and kind k, (1/V) sum_x eta_r(x)^+ Gamma_k psi_r(x) into
+ * re_im[(r*9 + k)*2 + {0, 1}], Gamma_k = 1, gamma1..gamma5, gamma4 gamma5,
+ * gamma1, gamma2 (the last two are the reference's rotating-frame kinds 7 and 8
+ * at omega = 0) */
+clg_status clg_condensate_contract(clg_field eta, clg_field psi, double* re_im);
 
 #ifdef __cplusplus
 }

@@ -39,6 +39,7 @@ void clgo_gen_gauge_expH(const int L[4], uint64_t seed, uint32_t field_id, doubl
 void clgo_gen_gauge_identity(const int L[4], double* U);
 void clgo_gen_gauss(long nsites, int ncomp, uint64_t seed, uint32_t field_id, double* psi);
 void clgo_gen_z2(long nsites, int ncomp, uint64_t seed, uint32_t field_id, double* psi);
+void clgo_gen_z4(long nsites, int ncomp, uint64_t seed, uint32_t field_id, double* psi);
 void clgo_gen_point(long nsites, int ncomp, long site, int comp, double* psi);
 void clgo_zero_parity(const int L[4], int ncomp, int parity, double* psi);
 double clgo_plaquette(const int L[4], const double* U);
@@ -66,6 +67,21 @@ void clgo_ks_force(const clgo_lat* lat, const double* U, int n, const double* ph
                    const double* a, double* F);
 void clgo_ks_dddag_ee(const clgo_lat* lat, const double* U, double mass2am,
                       const double* in, double* out, double* tmp);
+
+/* ---------------------------------------------------------------- measurements */
+/* EGammaMatrix (Core/CudaHelper.h:37-63) */
+enum {
+    CLGO_UNITY = 0, CLGO_GAMMA1, CLGO_GAMMA2, CLGO_GAMMA3, CLGO_GAMMA4, CLGO_GAMMA5, CLGO_GAMMA51, CLGO_GAMMA52,
+    CLGO_GAMMA53, CLGO_GAMMA54, CLGO_GAMMA15, CLGO_GAMMA25, CLGO_GAMMA35, CLGO_GAMMA45, CLGO_SIGMA12, CLGO_SIGMA23,
+    CLGO_SIGMA31, CLGO_SIGMA41, CLGO_SIGMA42, CLGO_SIGMA43, CLGO_SIGMA12E, CLGO_SIGMA23E, CLGO_SIGMA31E,
+    CLGO_CHARGECONJG, CLGO_EGM_MAX
+};
+/* chiral gamma matrix `which`: row r -> column idx[r] with phase i^z[r]; next symmetric index */
+int clgo_gamma(int which, int idx[4], int z[4], int* next_symmetric);
+/* meson correlator C(t), t < Lt, of 12 propagators prop[r = spin*3 + colour] (each V*12 complex) */
+void clgo_meson_correlator(const int L[4], const double* prop, int gamma, double* C);
+/* (1/V) sum_x eta(x)^+ Gamma_kind psi(x), kind 0..8 as _kernelDotMeasureAll at omega = 0 */
+void clgo_condensate(long V, const double* eta, const double* psi, int kind, double* re_im);
 
 /* generic operator descriptor used by the solvers */
 enum {

@@ -29,7 +29,7 @@
 
 typedef double _Complex cplx;
 
-enum { TAG_GAUGE = 0x47415547u, TAG_SPINOR = 0x5350494eu, TAG_Z2 = 0x5a324e53u };
+enum { TAG_GAUGE = 0x47415547u, TAG_SPINOR = 0x5350494eu, TAG_Z2 = 0x5a324e53u, TAG_Z4 = 0x5a344e53u };
 
 void clgo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
     uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
@@ -224,6 +224,23 @@ void clgo_gen_z2(long nsites, int ncomp, uint64_t seed, uint32_t field_id, doubl
             const uint32_t w0 = o[b0 >> 5] >> (b0 & 31), w1 = o[b1 >> 5] >> (b1 & 31);
             psi[2 * (s * ncomp + k)] = (w0 & 1u) ? -isq2 : isq2;
             psi[2 * (s * ncomp + k) + 1] = (w1 & 1u) ? -isq2 : isq2;
+        }
+    }
+}
+
+/* Z4 noise i^b per component (EFIT_RandomZ4, Tools/Math/Random.h:199-220), b =
+ * bits 2k, 2k+1 of one 128-bit Philox output per site (ncomp <= 64). */
+void clgo_gen_z4(long nsites, int ncomp, uint64_t seed, uint32_t field_id, double* psi) {
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32) ^ field_id};
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < nsites; ++s) {
+        const uint32_t ctr[4] = {(uint32_t)s, (uint32_t)((uint64_t)s >> 32), 0u, TAG_Z4};
+        uint32_t o[4];
+        clgo_philox4x32_10(ctr, key, o);
+        for (int k = 0; k < ncomp; ++k) {
+            const uint32_t b = (o[(2 * k) >> 5] >> ((2 * k) & 31)) & 3u;
+            psi[2 * (s * ncomp + k)] = b == 0 ? 1.0 : (b == 2 ? -1.0 : 0.0);
+            psi[2 * (s * ncomp + k) + 1] = b == 1 ? 1.0 : (b == 3 ? -1.0 : 0.0);
         }
     }
 }

@@ -20,7 +20,7 @@ _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(_HERE, f) for f in ("clg_oracle.c", "clg_oracle_fields.c", "clg_oracle.h")]
+    srcs = [os.path.join(_HERE, f) for f in ("clg_oracle.c", "clg_oracle_fields.c", "clg_oracle_measure.c", "clg_oracle.h")]
     if force or not os.path.exists(_LIB_PATH) or any(
         os.path.getmtime(s) > os.path.getmtime(_LIB_PATH) for s in srcs
     ):
@@ -78,6 +78,7 @@ def lib():
             "clgo_gen_gauge_identity": (None, [p, p]),
             "clgo_gen_gauss": (None, [l, i, u64, u32, p]),
             "clgo_gen_z2": (None, [l, i, u64, u32, p]),
+            "clgo_gen_z4": (None, [l, i, u64, u32, p]),
             "clgo_gen_point": (None, [l, i, l, i, p]),
             "clgo_zero_parity": (None, [p, i, i, p]),
             "clgo_plaquette": (d, [p, p]),
@@ -91,6 +92,9 @@ def lib():
             "clgo_ks_hop": (None, [p, p, i, p, p]),
             "clgo_ks_dddag_ee": (None, [p, p, d, p, p, p]),
             "clgo_ks_force": (None, [p, p, i, p, p, p, p]),
+            "clgo_gamma": (i, [i, p, p, p]),
+            "clgo_meson_correlator": (None, [p, p, i, p]),
+            "clgo_condensate": (None, [l, p, p, i, p]),
             "clgo_op_len": (l, [p]),
             "clgo_apply": (None, [p, p, p]),
             "clgo_dot": (None, [l, p, p, p]),
@@ -164,6 +168,12 @@ def z2(nsites, ncomp, seed, field_id):
     return psi
 
 
+def z4(nsites, ncomp, seed, field_id):
+    psi = np.empty((nsites, ncomp), np.complex128)
+    lib().clgo_gen_z4(nsites, ncomp, seed, field_id, _ptr(psi))
+    return psi
+
+
 def philox(ctr, key):
     c = np.asarray(ctr, np.uint32)
     k = np.asarray(key, np.uint32)
@@ -232,6 +242,48 @@ def wilson_force(L, U, X, Y, kappa, F=None, bc=(1, 1, 1, -1)):
     lat = _lat(L, bc)
     lib().clgo_wilson_force(C.byref(lat), _ptr(U), kappa, _ptr(X), _ptr(Y), _ptr(out))
     return out
+
+
+GAMMAS = ["UNITY", "GAMMA1", "GAMMA2", "GAMMA3", "GAMMA4", "GAMMA5", "GAMMA51", "GAMMA52", "GAMMA53", "GAMMA54",
+          "GAMMA15", "GAMMA25", "GAMMA35", "GAMMA45", "SIGMA12", "SIGMA23", "SIGMA31", "SIGMA41", "SIGMA42", "SIGMA43",
+          "SIGMA12E", "SIGMA23E", "SIGMA31E", "CHARGECONJG"]
+
+
+def gamma(which):
+    """(idx[4], z[4], next_symmetric_index) of EGammaMatrix `which` (chiral set)."""
+    idx = (C.c_int * 4)()
+    z = (C.c_int * 4)()
+    ns = C.c_int()
+    if lib().clgo_gamma(which, idx, z, C.byref(ns)) != 0:
+        raise ValueError(which)
+    return list(idx), list(z), ns.value
+
+
+def gamma_matrix(which):
+    idx, z, _ = gamma(which)
+    m = np.zeros((4, 4), np.complex128)
+    for r in range(4):
+        m[r, idx[r]] = 1j ** z[r]
+    return m
+
+
+def meson_correlator(L, props, which):
+    """C(t) of the 12 point-source propagators props[spin*3 + colour] (CMeasureMesonCorrelator.cu:26-174, 366-380)."""
+    P = np.ascontiguousarray(np.stack([np.asarray(x, np.complex128).reshape(-1) for x in props]))
+    assert P.shape[0] == 12
+    out = np.zeros(L[3], np.float64)
+    Li = (C.c_int * 4)(*L)
+    lib().clgo_meson_correlator(Li, _ptr(P), which, _ptr(out))
+    return out
+
+
+def condensate(eta, psi, kind):
+    """(1/V) sum_x eta^+ Gamma_kind psi (CMeasureChiralCondensate.cu:38-100, omega = 0)."""
+    e = np.ascontiguousarray(eta, np.complex128).reshape(-1)
+    q = np.ascontiguousarray(psi, np.complex128).reshape(-1)
+    out = np.zeros(2, np.float64)
+    lib().clgo_condensate(e.size // 12, _ptr(e), _ptr(q), kind, _ptr(out))
+    return complex(out[0], out[1])
 
 
 def ks_force(L, U, phi_i, phi_id, a, F=None, bc=(1, 1, 1, -1)):

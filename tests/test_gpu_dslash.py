@@ -46,6 +46,8 @@ def test_generator_matches_oracle(ctx, clg, oracle):
     np.testing.assert_allclose(f.to_numpy(), oracle.gauss(lat.volume, 12, 99, 2).reshape(-1, 4, 3), atol=1e-14)
     f.InitialField(clg.SOURCE_Z2, 98, 3)
     np.testing.assert_array_equal(f.to_numpy(), oracle.z2(lat.volume, 12, 98, 3).reshape(-1, 4, 3))
+    f.InitialField(clg.SOURCE_Z4, 97, 4)
+    np.testing.assert_array_equal(f.to_numpy(), oracle.z4(lat.volume, 12, 97, 4).reshape(-1, 4, 3))
 
 
 def test_bridgepp_import_plaquette(ctx, clg):

@@ -92,6 +92,9 @@ def test_generators(oracle):
     assert abs(np.mean(np.abs(g) ** 2) - 1.0) < 0.02
     z = oracle.z2(1000, 12, 7, 3)
     np.testing.assert_allclose(np.abs(z), 1.0, atol=1e-15)
+    z4 = oracle.z4(4000, 12, 7, 3)
+    assert set(np.unique(z4).tolist()) == {1, 1j, -1, -1j}
+    assert abs(np.mean(z4 == 1j) - 0.25) < 0.01 and abs(np.mean(z4)) < 0.02
 
 
 @pytest.mark.parametrize("L", [(4, 4, 4, 4), (4, 2, 4, 6)])
@@ -274,3 +277,69 @@ def test_ks_force_is_the_rational_action_derivative(oracle):
         dS = (S_at(eps) - S_at(-eps)) / (2 * eps)
         want = (2j * np.trace(T @ F[link])).real
         assert abs(dS - want) <= 1e-6 * max(1.0, abs(want)), (link, dS, want)
+
+
+def test_gamma_table(oracle):
+    """The chiral gamma set and its products (GammaMatrix.h:405-511): GAMMA1..5
+    equal the table parsed from the reference header (golden gamma_chiral.json);
+    every product equals the matrix product it is defined as; the Clifford
+    algebra holds; the next-symmetric index follows CalculateNextSymmetricIndex."""
+    gold = json.load(open(os.path.join(GOLDEN, "gamma_chiral.json")))["rows"]
+    G = {name: oracle.gamma_matrix(k) for k, name in enumerate(oracle.GAMMAS)}
+    for name in ("GAMMA1", "GAMMA2", "GAMMA3", "GAMMA4", "GAMMA5"):
+        m = np.zeros((4, 4), np.complex128)
+        for r, (c, b) in enumerate(gold[name]):
+            m[r, c] = 1j ** b
+        np.testing.assert_array_equal(G[name], m)
+    g = [None] + [G["GAMMA%d" % k] for k in range(1, 6)]
+    prod = {
+        "GAMMA51": g[5] @ g[1], "GAMMA52": g[5] @ g[2], "GAMMA53": g[5] @ g[3], "GAMMA54": g[5] @ g[4],
+        "GAMMA15": g[1] @ g[5], "GAMMA25": g[2] @ g[5], "GAMMA35": g[3] @ g[5], "GAMMA45": g[4] @ g[5],
+        "SIGMA12": 1j * g[2] @ g[1], "SIGMA23": 1j * g[3] @ g[2], "SIGMA31": 1j * g[1] @ g[3],
+        "SIGMA12E": 1j * g[1] @ g[2], "SIGMA23E": 1j * g[2] @ g[3], "SIGMA31E": 1j * g[3] @ g[1],
+        "SIGMA41": 1j * g[1] @ g[4], "SIGMA42": 1j * g[2] @ g[4], "SIGMA43": 1j * g[3] @ g[4],
+        "CHARGECONJG": g[4] @ g[2], "UNITY": np.eye(4),
+    }
+    for name, m in prod.items():
+        np.testing.assert_allclose(G[name], m, atol=1e-15, err_msg=name)
+    for mu in range(1, 6):
+        for nu in range(1, 6):
+            ac = g[mu] @ g[nu] + g[nu] @ g[mu]
+            np.testing.assert_allclose(ac, 2 * np.eye(4) * (mu == nu), atol=1e-15)
+    for k in range(len(oracle.GAMMAS)):
+        idx, z, ns = oracle.gamma(k)
+        assert ns == {0: 0, 1: 2, 2: 3, 3: 1}[idx[0]]
+
+
+def test_meson_and_condensate_contractions(oracle):
+    """The oracle's meson contraction and condensate traces equal an independent
+    numpy restatement of _kernelCalculateCorrelatorSU3 (CMeasureMesonCorrelator.cu:26-174,
+    366-380) and _kernelDotMeasureAll (CMeasureChiralCondensate.cu:38-100) on random fields."""
+    L = (4, 4, 2, 6)
+    V = oracle.volume(L)
+    rng = np.random.default_rng(3)
+    props = [rng.normal(size=(V, 4, 3)) + 1j * rng.normal(size=(V, 4, 3)) for _ in range(12)]
+    S = np.stack(props)  # [j*3 + a][site][i][b]
+    for k in range(len(oracle.GAMMAS)):
+        idx, z, ns = oracle.gamma(k)
+
+        def term(i, j, pi, pj):
+            return np.sum((np.conj(S[3 * j:3 * j + 3, :, i, :]) * S[3 * pj:3 * pj + 3, :, pi, :]).real, axis=(0, 2))
+
+        res = np.zeros(V)
+        for i in range(1, 4):
+            for j in range(i + 1, 4):
+                zz = z[i] + (((z[j] & 1) << 1) + z[j])
+                res += (1.0 - (zz & 2)) * term(i, j, idx[i], idx[j])
+        if ns == 0:
+            res += 0.5 * sum(term(i, i, i, i) for i in range(4))
+        else:
+            res += term(0, 0, idx[0], idx[0]) + term(ns, ns, idx[ns], idx[ns])
+        want = res.reshape(-1, L[3]).sum(axis=0) * 2 / np.sqrt(V)
+        np.testing.assert_allclose(oracle.meson_correlator(L, props, k), want, rtol=1e-12, atol=1e-12)
+    eta, psi = props[0], props[1]
+    for kind, name in enumerate(["UNITY", "GAMMA1", "GAMMA2", "GAMMA3", "GAMMA4", "GAMMA5", "GAMMA45", "GAMMA1",
+                                 "GAMMA2"]):
+        G = oracle.gamma_matrix(oracle.GAMMAS.index(name))
+        want = np.vdot(eta, np.einsum("rs,xsc->xrc", G, psi)) / V
+        assert abs(oracle.condensate(eta, psi, kind) - want) < 1e-12 * abs(want) + 1e-14
