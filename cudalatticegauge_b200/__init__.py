@@ -39,7 +39,7 @@ GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
 (FILE_CLGBIN_DOUBLE, FILE_CLGBIN_FLOAT, FILE_CLGBIN_COMPRESSED, FILE_CLGBIN_COMPRESSED_FLOAT, FILE_BRIDGEPP_BIN,
  FILE_BRIDGEPP_TXT) = range(6)
 SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT, SOURCE_Z4 = 0, 1, 2, 3, 4
-SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS = 0, 1, 2, 3, 4
+SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS, SOLVER_GCRODR = 0, 1, 2, 3, 4, 5
 
 
 class CLGError(RuntimeError):
@@ -54,7 +54,7 @@ class SolverParams(C.Structure):
         ("absolute_accuracy", C.c_int32), ("deviation_step", C.c_int32), ("max_step", C.c_int32),
         ("small_rho", C.c_double), ("inner_precision", C.c_int32), ("tol_true_rel", C.c_double),
         ("inner_tol", C.c_double), ("max_iterations", C.c_int32), ("max_outer", C.c_int32),
-        ("even_odd", C.c_int32), ("use_graphs", C.c_int32),
+        ("even_odd", C.c_int32), ("use_graphs", C.c_int32), ("kdim", C.c_int32),
     ]
 
 
@@ -109,6 +109,7 @@ SIGNATURES = [
     ("clg_solver_default_params", _S, [_I, C.POINTER(SolverParams)]),
     ("clg_solver_create", _S, [_P, C.POINTER(SolverParams), C.POINTER(_P)]),
     ("clg_solver_destroy", _S, [_P]),
+    ("clg_solver_reset", _S, [_P]),
     ("clg_solve", _S, [_P, _P, _P, _P, _I, _P, _P]),
     ("clg_solve_multishift", _S, [_P, _P, _I, _P, _P, _P, _I, _P]),
     ("clg_rational_apply", _S, [_P, _P, _P, _I, _I, _D, _P, _P, _P]),
@@ -121,6 +122,7 @@ SIGNATURES = [
     ("clg_wilson_fermion_force", _S, [_P, _P, _P, _P, _P, _P]),
     ("clg_ks_force", _S, [_P, _P, _I, _P, _P, _P]),
     ("clg_ks_fermion_force", _S, [_P, _P, _P, _P, _I, _P, _P, _P]),
+    ("clg_small_eig", _S, [_I, _P, _P, _P, _P]),
     ("clg_meson_correlator", _S, [_P, _P, _P, _I, _P, _P, _P]),
     ("clg_meson_contract", _S, [_P, _I, _P, _P]),
     ("clg_chiral_condensate", _S, [_P, _P, _P, _P, C.c_uint64, _P, _P]),
@@ -435,7 +437,7 @@ class _Solver:
         p = SolverParams()
         ctx.check(ctx.lib.clg_solver_default_params(self.KIND, C.byref(p)), "clg_solver_default_params")
         names = {
-            "MaxDim": "max_dim", "Restart": "restart", "Accuracy": "accuracy", "AbsoluteAccuracy": "absolute_accuracy",
+            "MaxDim": "max_dim", "MDim": "max_dim", "KDim": "kdim", "Restart": "restart", "Accuracy": "accuracy", "AbsoluteAccuracy": "absolute_accuracy",
             "DiviationStep": "deviation_step", "MaxStep": "max_step", "SmallRho": "small_rho",
         }
         for k, v in kw.items():
@@ -505,6 +507,16 @@ class CMultiShiftFOM(_MultiShift):
     KIND = SOLVER_FOM_MS
 
 
+class CSLASolverGCRODR(_Solver):
+    """GCRO-DR with a recycled subspace kept between solves (CSolverGCRODR.cpp);
+    MDim / KDim as the reference's keys, FP64, one right-hand side."""
+    KIND = SOLVER_GCRODR
+
+    def Reset(self):
+        """Drop the recycled subspace (the start of a new trajectory)."""
+        self.ctx.check(self.ctx.lib.clg_solver_reset(self.h), "clg_solver_reset")
+
+
 # EGammaMatrix (clg_gamma)
 GAMMAS = ["UNITY", "GAMMA1", "GAMMA2", "GAMMA3", "GAMMA4", "GAMMA5", "GAMMA51", "GAMMA52", "GAMMA53", "GAMMA54",
           "GAMMA15", "GAMMA25", "GAMMA35", "GAMMA45", "SIGMA12", "SIGMA23", "SIGMA31", "SIGMA41", "SIGMA42", "SIGMA43",
@@ -572,6 +584,19 @@ class CMeasureChiralCondensate:
         out = np.zeros(eta.nrhs * 18, np.float64)
         eta.ctx.check(eta.ctx.lib.clg_condensate_contract(eta.h, psi.h, _ptr(out)), "clg_condensate_contract")
         return (out[0::2] + 1j * out[1::2]).reshape(eta.nrhs, 9)
+
+
+def small_eig(A: np.ndarray, B: Optional[np.ndarray] = None):
+    """Eigenvalues and unit eigenvectors (columns) of A, or of A x = w B x (clg_small_eig)."""
+    n = A.shape[0]
+    a = np.ascontiguousarray(A, np.complex128)
+    b = None if B is None else np.ascontiguousarray(B, np.complex128)
+    w = np.zeros(n, np.complex128)
+    x = np.zeros((n, n), np.complex128)
+    st = load_library().clg_small_eig(n, _ptr(a), None if b is None else _ptr(b), _ptr(w), _ptr(x))
+    if st != SUCCESS:
+        raise CLGError(st, "clg_small_eig")
+    return w, x
 
 
 def md5(data) -> str:

@@ -1,0 +1,577 @@
+// gcrodr.cu -- GCRO-DR: GMRES with deflated restarting and a recycled
+// subspace kept between solves (CSLASolverGCRODR,
+// SparseLinearAlgebra/CSolverGCRODR.cpp:196-911; Parks, de Sturler, Mackey,
+// Johnson & Maiti, SIAM J. Sci. Comput. 28 (2006) 1651).
+//
+// Each cycle works in [U_k, V_{m-k}] with A U_k = C_k, C_k^+ C_k = 1 and the
+// Arnoldi vectors V orthogonal to C_k, so that
+//   A [U_k, V_{m-k}] = [C_k, V_{m-k+1}] G,  G = [[D_k, B], [0, Hbar]]
+// (D_k the norms that make U_k unit vectors).  The correction minimises the
+// residual over that space; then the k harmonic-Ritz-type vectors of the
+// cycle (the reference's default deflation space EEDT_SVD: the k smallest
+// eigenpairs of G^+ G p = l blockdiag(U^+ U, 1) p) become the next U_k:
+//   U_k = [U_k, V] P R^-1, C_k = [C_k, V] Q with G P = Q R.
+// The first solve starts with one GMRES(m) cycle whose Hbar gives the first
+// U_k; later solves (the same operator, e.g. successive molecular-dynamics
+// steps or right-hand sides) start from the kept U_k: C_k = A U_k, QR,
+// U_k R^-1 (GenerateCUFirstTime).  clg_solver_reset drops U_k (the
+// reference's start of a trajectory).
+//
+// B200 form: FP64 vectors on the device, one right-hand side; every
+// orthogonalisation is one multi-dot launch (up to 16 inner products per
+// pass, classical Gram-Schmidt applied twice) and one linear-combination
+// launch, so a cycle costs (m - k) operator applications, one explicit
+// residual b - A x (the reference's RecalculateR option, which it calls "the
+// accurate result") and O(m) small launches with one host read each.  The
+// small dense problems (least squares, QR, generalized eigenproblem, order
+// <= 33) run on the host (dense.h); the reference runs them on the device.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "blas.cuh"
+#include "dense.h"
+
+namespace clg {
+
+namespace {
+
+using dense::Mat;
+using dense::Z;
+
+constexpr int MD = 16;    // inner products per multi-dot launch
+constexpr int MAXV = 34;  // vectors per linear combination (m + 1 <= 33, + 1)
+
+template <int NC>
+struct MultiDotF {  // out[i] = sum_x conj(v_i(x)) w(x), i < n
+  DField w;
+  DField v[MD];
+  int n;
+  double* out;
+  __device__ bool active(int) const { return true; }
+  __device__ void operator()(int, int p, int64_t h, double* acc) const {
+    cpx<double> wv[NC];
+    ldv<P64, NC, double>(w, 0, p, h, wv);
+#pragma unroll
+    for (int i = 0; i < MD; ++i) {
+      if (i >= n) break;
+      cpx<double> a[NC];
+      ldv<P64, NC, double>(v[i], 0, p, h, a);
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        re = fma(a[c].x, wv[c].x, fma(a[c].y, wv[c].y, re));
+        im = fma(a[c].x, wv[c].y, fma(-a[c].y, wv[c].x, im));
+      }
+      acc[2 * i] += re;
+      acc[2 * i + 1] += im;
+    }
+  }
+  __device__ void finalize(int, const double* s) const {
+    for (int k = 0; k < 2 * n; ++k) out[k] = s[k];
+  }
+};
+
+template <int NC>
+struct LinCombF {  // out = beta out + sum_i c_i v_i
+  DField out;
+  DField v[MAXV];
+  double2 c[MAXV];
+  double2 beta;
+  int n;
+  __device__ bool active(int) const { return true; }
+  __device__ void operator()(int, int p, int64_t h, double*) const {
+    cpx<double> o[NC];
+    if (beta.x != 0.0 || beta.y != 0.0) {
+      ldv<P64, NC, double>(out, 0, p, h, o);
+      const cpx<double> b = mk<double>(beta.x, beta.y);
+#pragma unroll
+      for (int k = 0; k < NC; ++k) o[k] = b * o[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NC; ++k) o[k] = mk<double>(0, 0);
+    }
+    for (int i = 0; i < n; ++i) {
+      cpx<double> a[NC];
+      ldv<P64, NC, double>(v[i], 0, p, h, a);
+      const cpx<double> ci = mk<double>(c[i].x, c[i].y);
+#pragma unroll
+      for (int k = 0; k < NC; ++k) o[k] = o[k] + ci * a[k];
+    }
+    stv<P64, NC, double>(out, 0, p, h, o);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
+// the recycled subspace and the per-solve vectors, kept by the solver
+struct GcroWork : SolveCacheBase {
+  clg_context_s* ctx = nullptr;
+  std::vector<void*> allocs;
+  FieldRef proto;
+  const void* lat = nullptr;
+  int kind = -1, subset = -1, op = -1, m = 0, k = 0;
+  std::vector<FieldRef> U, C, V, Tu, Tc;
+  FieldRef x, r, w, t, tmp;
+  double* dev_out = nullptr;
+  bool u_valid = false;
+  ~GcroWork() override {
+    for (void* p : allocs) dfree(p);
+  }
+  clg_status vec(FieldRef& f) {
+    void* p = nullptr;
+    const size_t bytes = (size_t)proto.blk * proto.nparity;
+    if (clg_status st = dalloc(ctx, &p, bytes)) return st;
+    allocs.push_back(p);
+    f = proto;
+    f.data = static_cast<char*>(p);
+    return CLG_SUCCESS;
+  }
+};
+
+struct Gcro {
+  clg_context_s* ctx;
+  GcroWork& W;
+  const clg_gauge_s* Ug;
+  int kind, op, nc;
+  double param;
+  int64_t Vh;
+  int apps = 0;
+
+  clg_status apply(const FieldRef& out, const FieldRef& in) {
+    ++apps;
+    return apply_op(ctx, op, Ug, kind, param, out, in, &W.tmp, make_double2(1.0, 0.0), 1);
+  }
+  // out[i] = v_i^+ w for the n vectors vs (n arbitrary), read to the host
+  clg_status dots(const FieldRef& w, const std::vector<const FieldRef*>& vs, std::vector<Z>& out) {
+    out.assign(vs.size(), Z(0.0, 0.0));
+    for (size_t i0 = 0; i0 < vs.size(); i0 += MD) {
+      const int n = (int)std::min<size_t>(MD, vs.size() - i0);
+      clg_status st;
+      if (nc == 12) {
+        MultiDotF<12> f;
+        f.w = dfield(w);
+        for (int i = 0; i < MD; ++i) f.v[i] = dfield(*vs[i0 + std::min(i, n - 1)]);
+        f.n = n;
+        f.out = W.dev_out;
+        st = launch_sites<2 * MD>(ctx, f, W.proto.first_parity, W.proto.nparity, Vh, 1);
+      } else {
+        MultiDotF<3> f;
+        f.w = dfield(w);
+        for (int i = 0; i < MD; ++i) f.v[i] = dfield(*vs[i0 + std::min(i, n - 1)]);
+        f.n = n;
+        f.out = W.dev_out;
+        st = launch_sites<2 * MD>(ctx, f, W.proto.first_parity, W.proto.nparity, Vh, 1);
+      }
+      if (st) return st;
+      double h[2 * MD];
+      cudaError_t e = cudaMemcpyAsync(h, W.dev_out, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) return ctx->fail(cuda_status(e), cudaGetErrorString(e));
+      for (int i = 0; i < n; ++i) out[i0 + i] = Z(h[2 * i], h[2 * i + 1]);
+    }
+    return CLG_SUCCESS;
+  }
+  double norm(const FieldRef& a) {
+    std::vector<Z> d;
+    if (dots(a, {&a}, d)) return -1.0;
+    return std::sqrt(std::max(d[0].real(), 0.0));
+  }
+  // out = beta out + sum_i c_i v_i
+  clg_status lincomb(const FieldRef& out, Z beta, const std::vector<const FieldRef*>& vs, const std::vector<Z>& c) {
+    if (vs.size() > (size_t)MAXV) return ctx->fail(CLG_ERR_UNSUPPORTED, "GCRO-DR: too many vectors");
+    auto fill = [&](auto& f) {
+      f.out = dfield(out);
+      f.n = (int)vs.size();
+      f.beta = make_double2(beta.real(), beta.imag());
+      for (size_t i = 0; i < vs.size(); ++i) {
+        f.v[i] = dfield(*vs[i]);
+        f.c[i] = make_double2(c[i].real(), c[i].imag());
+      }
+    };
+    if (nc == 12) {
+      LinCombF<12> f;
+      fill(f);
+      return launch_sites<0>(ctx, f, W.proto.first_parity, W.proto.nparity, Vh, 1);
+    }
+    LinCombF<3> f;
+    fill(f);
+    return launch_sites<0>(ctx, f, W.proto.first_parity, W.proto.nparity, Vh, 1);
+  }
+  clg_status copy(const FieldRef& dst, const FieldRef& src) { return lincomb(dst, Z(0.0, 0.0), {&src}, {Z(1.0, 0.0)}); }
+  clg_status scale(const FieldRef& a, Z s) { return lincomb(a, s, {}, {}); }
+  // r = b - A x
+  clg_status residual(const FieldRef& b, const FieldRef& x, const FieldRef& r) {
+    if (clg_status st = apply(W.t, x)) return st;
+    return lincomb(r, Z(0.0, 0.0), {&b, &W.t}, {Z(1.0, 0.0), Z(-1.0, 0.0)});
+  }
+  // w <- w - sum_i (v_i^+ w) v_i, twice; the coefficients of both passes summed into h
+  clg_status orthogonalise(const FieldRef& w, const std::vector<const FieldRef*>& vs, std::vector<Z>& h) {
+    h.assign(vs.size(), Z(0.0, 0.0));
+    for (int pass = 0; pass < 2; ++pass) {
+      std::vector<Z> d;
+      if (clg_status st = dots(w, vs, d)) return st;
+      std::vector<Z> neg(d.size());
+      for (size_t i = 0; i < d.size(); ++i) {
+        h[i] += d[i];
+        neg[i] = -d[i];
+      }
+      if (clg_status st = lincomb(w, Z(1.0, 0.0), vs, neg)) return st;
+    }
+    return CLG_SUCCESS;
+  }
+  // U = T R^-1 for upper triangular R (k x k) (FieldSolveY, CSolverGCRODR.cpp:763-780)
+  clg_status solve_r(std::vector<FieldRef>& T, const Mat& R, int k) {
+    for (int i = 0; i < k; ++i) {
+      std::vector<const FieldRef*> vs;
+      std::vector<Z> c;
+      for (int j = 0; j < i; ++j) {
+        vs.push_back(&T[j]);
+        c.push_back(-R(j, i) / R(i, i));
+      }
+      if (clg_status st = lincomb(T[i], Z(1.0, 0.0) / R(i, i), vs, c)) return st;
+    }
+    return CLG_SUCCESS;
+  }
+};
+
+double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
+}  // namespace
+
+clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_gauge_s* Ug, int op, clg_field_s* X0,
+                        clg_solve_info* info) {
+  clg_context_s* ctx = S->ctx;
+  const double t0 = now_s();
+  if (B->nrhs != 1) return ctx->fail(CLG_ERR_UNSUPPORTED, "GCRO-DR solves one right-hand side at a time");
+  if (B->prec != CLG_PREC_DOUBLE || X->prec != CLG_PREC_DOUBLE || (X0 && X0->prec != CLG_PREC_DOUBLE))
+    return ctx->fail(CLG_ERR_BAD_ARG, "GCRO-DR works on FP64 fields");
+  const bool even = B->subset == CLG_SUBSET_EVEN;
+  const bool even_op = op == CLG_OP_MEE || op == CLG_OP_MEE_DAG || op == CLG_OP_MEE_MEEDAG || op == CLG_OP_DDDAG_EE;
+  const bool full_op = op == CLG_OP_D || op == CLG_OP_DDAG || op == CLG_OP_DDDAG || op == CLG_OP_DD;
+  if (!(even ? even_op : full_op)) return ctx->fail(CLG_ERR_BAD_ARG, "GCRO-DR: operator and field subset do not match");
+  if (clg_status st = gauge_prepare(Ug, CLG_PREC_DOUBLE)) return st;
+  const int m = S->p.max_dim, k = S->p.kdim > 0 ? S->p.kdim : S->p.max_dim - 2;
+
+  // workspace (and the recycled U_k) for this lattice / operator / sizes
+  auto* Wp = dynamic_cast<GcroWork*>(S->cache_gcro.get());
+  if (!Wp || Wp->lat != B->lat || Wp->kind != B->kind || Wp->subset != B->subset || Wp->op != op || Wp->m != m ||
+      Wp->k != k) {
+    S->cache_gcro.reset();
+    auto nw = std::make_unique<GcroWork>();
+    nw->ctx = ctx;
+    nw->proto = B->ref();
+    nw->lat = B->lat;
+    nw->kind = B->kind;
+    nw->subset = B->subset;
+    nw->op = op;
+    nw->m = m;
+    nw->k = k;
+    clg_status st = CLG_SUCCESS;
+    nw->U.resize(k);
+    nw->C.resize(k);
+    nw->Tu.resize(k);
+    nw->Tc.resize(k);
+    nw->V.resize(m - k + 1);
+    for (auto* vv : {&nw->U, &nw->C, &nw->Tu, &nw->Tc, &nw->V})
+      for (FieldRef& f : *vv)
+        if (!st) st = nw->vec(f);
+    for (FieldRef* f : {&nw->x, &nw->r, &nw->w, &nw->t})
+      if (!st) st = nw->vec(*f);
+    if (!st) {  // the operator's temporary: a full field
+      FieldRef full = nw->proto;
+      full.nparity = 2;
+      full.first_parity = 0;
+      full.rstride = full.blk * 2;
+      nw->proto = full;
+      st = nw->vec(nw->tmp);
+      nw->proto = B->ref();
+    }
+    if (!st) {
+      void* p = nullptr;
+      st = dalloc(ctx, &p, sizeof(double) * 2 * MD);
+      if (!st) {
+        nw->allocs.push_back(p);
+        nw->dev_out = static_cast<double*>(p);
+      }
+    }
+    if (st) return st;
+    Wp = nw.get();
+    S->cache_gcro = std::move(nw);
+  }
+  GcroWork& W = *Wp;
+  for (clg_field f : {X, B, X0})
+    if (f)
+      if (clg_status st = settle(f)) return st;
+  Gcro g{ctx, W, Ug, B->kind, op, B->nc(), B->param, B->lat->g.Vh};
+  const FieldRef b = B->ref();
+  const double tol = S->p.tol_true_rel;
+  clg_status st = CLG_SUCCESS;
+  std::memset(info, 0, sizeof(*info));
+
+  const double bnorm = g.norm(b);
+  if (bnorm < 0) return ctx->fail(CLG_ERR_CUDA, "GCRO-DR: reading |b|");
+  // x0 = the start vector, or b (CSolverGCRODR.cpp:216-223)
+  if ((st = g.copy(W.x, X0 ? X0->ref() : b))) return st;
+  if (bnorm == 0.0) {
+    if ((st = g.copy(X->ref(), b))) return st;
+    info->true_rel_residual = 0.0;
+    info->seconds = now_s() - t0;
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? CLG_SUCCESS : ctx->fail(cuda_status(e), cudaGetErrorString(e));
+  }
+
+  auto Wvec = [&](int j) -> FieldRef& { return j < k ? W.C[j] : W.V[j - k]; };  // GetW
+  double rnorm = 0.0;
+  int cycles = 0;
+  auto finish = [&](clg_status s) -> clg_status {
+    // the true residual before x is written (X may alias B)
+    if (!s) s = g.residual(b, W.x, W.r);
+    const double tr = s ? -1.0 : g.norm(W.r) / bnorm;
+    if (!s) s = g.copy(X->ref(), W.x);
+    info->iterations = g.apps;
+    info->restarts = cycles;
+    info->outer = 1;
+    info->true_rel_residual = tr;
+    info->seconds = now_s() - t0;
+    if (!s && !(tr <= tol)) s = CLG_ERR_NOT_CONVERGED;
+    info->status = s;
+    if (tr < 0) info->true_rel_residual = NAN;
+    return s;
+  };
+
+  if (W.u_valid) {
+    // C = A U, QR, U = U R^-1 (GenerateCUFirstTime / QRFactorAY, CSolverGCRODR.cpp:501-539, 817-841)
+    Mat R(k, k);
+    for (int i = 0; i < k; ++i)
+      if ((st = g.apply(W.C[i], W.U[i]))) return finish(st);
+    for (int i = 0; i < k; ++i) {
+      std::vector<const FieldRef*> prev;
+      for (int j = 0; j < i; ++j) prev.push_back(&W.C[j]);
+      std::vector<Z> h;
+      if (i && (st = g.orthogonalise(W.C[i], prev, h))) return finish(st);
+      for (int j = 0; j < i; ++j) R(j, i) = h[j];
+      const double n = g.norm(W.C[i]);
+      if (!(n > 0)) {
+        W.u_valid = false;
+        break;
+      }
+      R(i, i) = n;
+      if ((st = g.scale(W.C[i], Z(1.0 / n, 0.0)))) return finish(st);
+    }
+    if (W.u_valid && (st = g.solve_r(W.U, R, k))) return finish(st);
+  }
+  if ((st = g.residual(b, W.x, W.r))) return finish(st);
+  rnorm = g.norm(W.r);
+
+  if (!W.u_valid) {
+    // one GMRES(m) cycle (FirstTimeGMERESSolve, :400-499), its Hbar gives the first U_k
+    const double beta = rnorm;
+    if (beta <= tol * bnorm) return finish(CLG_SUCCESS);
+    if ((st = g.lincomb(Wvec(0), Z(0.0, 0.0), {&W.r}, {Z(1.0 / beta, 0.0)}))) return finish(st);
+    Mat H(m + 1, m);
+    int mm = m;
+    for (int j = 0; j < m; ++j) {
+      if ((st = g.apply(Wvec(j + 1), Wvec(j)))) return finish(st);
+      std::vector<const FieldRef*> vs;
+      for (int l = 0; l <= j; ++l) vs.push_back(&Wvec(l));
+      std::vector<Z> h;
+      if ((st = g.orthogonalise(Wvec(j + 1), vs, h))) return finish(st);
+      for (int l = 0; l <= j; ++l) H(l, j) = h[l];
+      const double hn = g.norm(Wvec(j + 1));
+      H(j + 1, j) = hn;
+      if (!(hn > 1e-14 * beta)) {  // invariant subspace: the solution is in span(W_0..W_j)
+        mm = j + 1;
+        break;
+      }
+      if ((st = g.scale(Wvec(j + 1), Z(1.0 / hn, 0.0)))) return finish(st);
+    }
+    Mat Hs(mm + 1, mm);
+    for (int i = 0; i <= mm; ++i)
+      for (int j = 0; j < mm; ++j) Hs(i, j) = H(i, j);
+    std::vector<Z> c(mm + 1, Z(0.0, 0.0)), y;
+    c[0] = beta;
+    if (!dense::lstsq(Hs, c, y)) return finish(ctx->fail(CLG_ERR_BREAKDOWN, "GCRO-DR: least squares"));
+    {
+      std::vector<const FieldRef*> vs;
+      for (int j = 0; j < mm; ++j) vs.push_back(&Wvec(j));
+      if ((st = g.lincomb(W.x, Z(1.0, 0.0), vs, y))) return finish(st);
+    }
+    if ((st = g.residual(b, W.x, W.r))) return finish(st);
+    rnorm = g.norm(W.r);
+    cycles = 1;
+    if (mm == m) {
+      // FindPk1 (EEDT_SVD): the k smallest eigenpairs of Hbar^+ Hbar
+      std::vector<Z> ev;
+      Mat X;
+      if (dense::eig(dense::mul_dag(H, H), ev, X)) {
+        const Mat P = dense::select(ev, X, k, true);
+        Mat Q, R;
+        if (dense::qr_thin(dense::mul(H, P), Q, R)) {
+          // GenerateCU right after GMRES: U = W_m P R^-1, C = W_{m+1} Q
+          std::vector<const FieldRef*> wm, wm1;
+          for (int j = 0; j < m; ++j) wm.push_back(&Wvec(j));
+          for (int j = 0; j <= m; ++j) wm1.push_back(&Wvec(j));
+          for (int j = 0; j < k && !st; ++j) {
+            std::vector<Z> cp(m), cq(m + 1);
+            for (int i = 0; i < m; ++i) cp[i] = P(i, j);
+            for (int i = 0; i <= m; ++i) cq[i] = Q(i, j);
+            st = g.lincomb(W.Tu[j], Z(0.0, 0.0), wm, cp);
+            if (!st) st = g.lincomb(W.Tc[j], Z(0.0, 0.0), wm1, cq);
+          }
+          if (!st) st = g.solve_r(W.Tu, R, k);
+          if (st) return finish(st);
+          std::swap(W.U, W.Tu);
+          std::swap(W.C, W.Tc);
+          W.u_valid = true;
+        }
+      }
+    }
+    // without a deflation space from this cycle (an invariant subspace was
+    // found, or the small problems failed) the loop below runs GMRES(m) cycles
+  }
+
+  while (!(rnorm <= tol * bnorm) && cycles < S->p.restart && g.apps < S->p.max_iterations) {
+    ++cycles;
+    if (!W.u_valid) {
+      // plain GMRES(m) cycle
+      const double beta = rnorm;
+      if ((st = g.lincomb(Wvec(0), Z(0.0, 0.0), {&W.r}, {Z(1.0 / beta, 0.0)}))) return finish(st);
+      Mat H(m + 1, m);
+      int mm = m;
+      for (int j = 0; j < m; ++j) {
+        if ((st = g.apply(Wvec(j + 1), Wvec(j)))) return finish(st);
+        std::vector<const FieldRef*> vs;
+        for (int l = 0; l <= j; ++l) vs.push_back(&Wvec(l));
+        std::vector<Z> h;
+        if ((st = g.orthogonalise(Wvec(j + 1), vs, h))) return finish(st);
+        for (int l = 0; l <= j; ++l) H(l, j) = h[l];
+        const double hn = g.norm(Wvec(j + 1));
+        H(j + 1, j) = hn;
+        if (!(hn > 1e-14 * beta)) {
+          mm = j + 1;
+          break;
+        }
+        if ((st = g.scale(Wvec(j + 1), Z(1.0 / hn, 0.0)))) return finish(st);
+      }
+      Mat Hs(mm + 1, mm);
+      for (int i = 0; i <= mm; ++i)
+        for (int j = 0; j < mm; ++j) Hs(i, j) = H(i, j);
+      std::vector<Z> c(mm + 1, Z(0.0, 0.0)), y;
+      c[0] = beta;
+      if (!dense::lstsq(Hs, c, y)) return finish(ctx->fail(CLG_ERR_BREAKDOWN, "GCRO-DR: least squares"));
+      std::vector<const FieldRef*> vs;
+      for (int j = 0; j < mm; ++j) vs.push_back(&Wvec(j));
+      if ((st = g.lincomb(W.x, Z(1.0, 0.0), vs, y))) return finish(st);
+      if ((st = g.residual(b, W.x, W.r))) return finish(st);
+      rnorm = g.norm(W.r);
+      continue;
+    }
+    // x += U C^+ r, r -= C C^+ r (OrthognalXR, :860-875)
+    {
+      std::vector<const FieldRef*> cs, us;
+      for (int i = 0; i < k; ++i) {
+        cs.push_back(&W.C[i]);
+        us.push_back(&W.U[i]);
+      }
+      std::vector<Z> d;
+      if ((st = g.dots(W.r, cs, d))) return finish(st);
+      std::vector<Z> nd(k);
+      for (int i = 0; i < k; ++i) nd[i] = -d[i];
+      if ((st = g.lincomb(W.x, Z(1.0, 0.0), us, d))) return finish(st);
+      if ((st = g.lincomb(W.r, Z(1.0, 0.0), cs, nd))) return finish(st);
+    }
+    // unit U_i, G_ii = 1/|U_i| (NormUkAndSetD, :843-858)
+    Mat G(m + 1, m);
+    for (int i = 0; i < k; ++i) {
+      const double n = g.norm(W.U[i]);
+      if (!(n > 0)) return finish(ctx->fail(CLG_ERR_BREAKDOWN, "GCRO-DR: zero recycled vector"));
+      G(i, i) = 1.0 / n;
+      if ((st = g.scale(W.U[i], Z(1.0 / n, 0.0)))) return finish(st);
+    }
+    const double beta = g.norm(W.r);
+    if ((st = g.lincomb(W.V[0], Z(0.0, 0.0), {&W.r}, {Z(1.0 / beta, 0.0)}))) return finish(st);
+    // Arnoldi with (1 - C C^+) A on the V (:259-301)
+    int mm = m;
+    for (int j = k; j < m; ++j) {
+      const int jj = j - k;
+      if ((st = g.apply(W.V[jj + 1], W.V[jj]))) return finish(st);
+      std::vector<const FieldRef*> vs;
+      for (int i = 0; i < k; ++i) vs.push_back(&W.C[i]);
+      for (int l = 0; l <= jj; ++l) vs.push_back(&W.V[l]);
+      std::vector<Z> h;
+      if ((st = g.orthogonalise(W.V[jj + 1], vs, h))) return finish(st);
+      for (int i = 0; i < k; ++i) G(i, j) = h[i];
+      for (int l = 0; l <= jj; ++l) G(k + l, j) = h[k + l];
+      const double hn = g.norm(W.V[jj + 1]);
+      G(j + 1, j) = hn;
+      if (!(hn > 1e-14 * beta)) {
+        mm = j + 1;
+        break;
+      }
+      if ((st = g.scale(W.V[jj + 1], Z(1.0 / hn, 0.0)))) return finish(st);
+    }
+    Mat Gs(mm + 1, mm);
+    for (int i = 0; i <= mm; ++i)
+      for (int j = 0; j < mm; ++j) Gs(i, j) = G(i, j);
+    std::vector<Z> c(mm + 1, Z(0.0, 0.0)), y;
+    c[k] = beta;
+    if (!dense::lstsq(Gs, c, y)) return finish(ctx->fail(CLG_ERR_BREAKDOWN, "GCRO-DR: least squares"));
+    {
+      std::vector<const FieldRef*> vs;
+      for (int i = 0; i < k; ++i) vs.push_back(&W.U[i]);
+      for (int j = k; j < mm; ++j) vs.push_back(&W.V[j - k]);
+      if ((st = g.lincomb(W.x, Z(1.0, 0.0), vs, y))) return finish(st);
+    }
+    if ((st = g.residual(b, W.x, W.r))) return finish(st);
+    rnorm = g.norm(W.r);
+    if (mm < m) continue;  // invariant subspace: keep U_k as it is
+    const bool converged = rnorm <= tol * bnorm;
+    // FindPk2 (EEDT_SVD, :724-760): G^+ G p = l [[U^+ U, 0], [0, 1]] p, k smallest
+    Mat Bm(m, m);
+    for (int i = 0; i < m; ++i) Bm(i, i) = 1.0;
+    for (int i = 0; i < k; ++i) {
+      std::vector<const FieldRef*> us;
+      for (int j = 0; j < k; ++j) us.push_back(&W.U[j]);
+      std::vector<Z> d;
+      if ((st = g.dots(W.U[i], us, d))) return finish(st);
+      for (int j = 0; j < k; ++j)
+        if (j != i) Bm(j, i) = d[j];  // (U_j^+ U_i)
+    }
+    std::vector<Z> ev;
+    Mat Xv;
+    if (!dense::geig(dense::mul_dag(G, G), Bm, ev, Xv)) continue;  // keep U_k
+    const Mat P = dense::select(ev, Xv, k, true);
+    Mat Q, R;
+    if (!dense::qr_thin(dense::mul(G, P), Q, R)) continue;
+    // GenerateCU (:782-815): U = [U, V] P R^-1, C = [C, V] Q (C only while unconverged)
+    std::vector<const FieldRef*> yv, wv;
+    for (int i = 0; i < k; ++i) {
+      yv.push_back(&W.U[i]);
+      wv.push_back(&W.C[i]);
+    }
+    for (int j = 0; j < m - k; ++j) yv.push_back(&W.V[j]);
+    for (int j = 0; j <= m - k; ++j) wv.push_back(&W.V[j]);
+    for (int j = 0; j < k && !st; ++j) {
+      std::vector<Z> cp(m), cq(m + 1);
+      for (int i = 0; i < m; ++i) cp[i] = P(i, j);
+      for (int i = 0; i <= m; ++i) cq[i] = Q(i, j);
+      st = g.lincomb(W.Tu[j], Z(0.0, 0.0), yv, cp);
+      if (!st && !converged) st = g.lincomb(W.Tc[j], Z(0.0, 0.0), wv, cq);
+    }
+    if (!st) st = g.solve_r(W.Tu, R, k);
+    if (st) return finish(st);
+    std::swap(W.U, W.Tu);
+    if (!converged) std::swap(W.C, W.Tc);
+  }
+  return finish(CLG_SUCCESS);
+}
+
+}  // namespace clg
+
+extern "C" clg_status clg_solver_reset(clg_solver s) {
+  if (!s) return CLG_ERR_BAD_ARG;
+  if (auto* w = dynamic_cast<clg::GcroWork*>(s->cache_gcro.get())) w->u_valid = false;
+  return CLG_SUCCESS;
+}

@@ -318,6 +318,7 @@ struct clg_solver_s {
   std::unique_ptr<clg::SolveCacheBase> cache;        // single-shift solves
   std::unique_ptr<clg::SolveCacheBase> cache_shift;  // multi-shift refinement
   std::unique_ptr<clg::SolveCacheBase> cache_cgm;    // multi-shift CG vectors, state, graph
+  std::unique_ptr<clg::SolveCacheBase> cache_gcro;   // GCRO-DR vectors and the recycled subspace
   // X = (DD^+)^-1 phi and Y = D^+ X of clg_wilson_fermion_force
   clg_field force_x = nullptr, force_y = nullptr;
   // phi_i = (DD^+ + b_i)^-1 phi and phi_id = D0 phi_i of clg_ks_fermion_force
@@ -329,3 +330,9 @@ struct clg_solver_s {
     for (clg_field f : ks_phi_id) clg_field_destroy(f);
   }
 };
+
+namespace clg {
+// GCRO-DR (gcrodr.cu)
+clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_gauge_s* U, int op, clg_field_s* X0,
+                        clg_solve_info* info);
+}  // namespace clg

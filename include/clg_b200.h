@@ -85,7 +85,8 @@ typedef enum {
     CLG_SOLVER_BICGSTAB = 1,    /* CSLASolverBiCGStab SparseLinearAlgebra/CSolverBiCGstab.cpp:403-607 */
     CLG_SOLVER_CG = 2,          /* CG on Hermitian positive operators (DD^+, staggered (DD^+)_ee)     */
     CLG_SOLVER_CGM = 3,         /* multi-shift CG (no reference twin; CMultiShiftSolver.h:38-47 API)  */
-    CLG_SOLVER_FOM_MS = 4       /* CMultiShiftFOM     SparseLinearAlgebra/CMultiShiftFOM.cpp:97-270   */
+    CLG_SOLVER_FOM_MS = 4,      /* CMultiShiftFOM     SparseLinearAlgebra/CMultiShiftFOM.cpp:97-270   */
+    CLG_SOLVER_GCRODR = 5       /* CSLASolverGCRODR   SparseLinearAlgebra/CSolverGCRODR.cpp:196-911   */
 } clg_solver_kind;
 
 /* ------------------------------------------------------------------ handles */
@@ -231,6 +232,7 @@ typedef struct {
     int32_t max_outer;         /* defect-correction cycles allowed                        */
     int32_t even_odd;          /* solve D x = b through the even-odd Schur system         */
     int32_t use_graphs;        /* capture the inner iterations in CUDA graphs             */
+    int32_t kdim;              /* KDim (GCRO-DR recycled dimension; 0: MaxDim - 2)         */
 } clg_solver_params;
 
 typedef struct {
@@ -245,10 +247,17 @@ typedef struct {
 clg_status clg_solver_default_params(int kind, clg_solver_params* p);
 clg_status clg_solver_create(clg_context ctx, const clg_solver_params* p, clg_solver* out);
 clg_status clg_solver_destroy(clg_solver s);
+/* GCRO-DR keeps its recycled subspace U_k between clg_solve calls on the same
+ * lattice and operator (the reference's ESP_InTrajectory phase); this drops it
+ * (ESP_StartTrajectory).  No effect on the other solver kinds. */
+clg_status clg_solver_reset(clg_solver s);
 /* CSLASolver::Solve (SparseLinearAlgebra/CSLASolver.h:42-50): solve op x = b for
  * every right-hand side of b; x may alias b; x0 (nullable) is the start vector
  * (pStart).  info holds nrhs entries.  Returns CLG_SUCCESS only when every
- * right-hand side reached tol_true_rel. */
+ * right-hand side reached tol_true_rel.
+ * GCRO-DR (CLG_SOLVER_GCRODR): FP64 fields, one right-hand side, max_dim = MDim
+ * (5..32), kdim = KDim (2..MDim-2), restart = cycles, x0 = b when no start
+ * vector is given (CSolverGCRODR.cpp:216-223); inner_precision is not used. */
 clg_status clg_solve(clg_solver s, clg_field x, clg_field b, clg_gauge g, int op, clg_field x0, clg_solve_info* info);
 /* CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47):
  * (op + c_n) x_n = b for n < nshift; shifts_re_im holds nshift complex shifts
@@ -259,6 +268,14 @@ clg_status clg_solve_multishift(clg_solver s, clg_field* x, int nshift, const do
  * f <- c f + sum_i a_i (op + b_i)^{-1} f through one multi-shift solve. */
 clg_status clg_rational_apply(clg_solver s, clg_field f, clg_gauge g, int op, int degree, double c,
                               const double* a, const double* b, clg_solve_info* info);
+
+/* Small dense eigenproblems of the recycled solver (host code, no device):
+ * A x = w x (b == NULL) or A x = w B x with B Hermitian positive definite,
+ * n <= 64, row-major interleaved complex; w receives n eigenvalues and the
+ * columns of x (row-major n x n) the unit eigenvectors (the reference's
+ * CLinearAlgebraHelper::EigenValueProblem / GeneralizedEigenValueProblem,
+ * Tools/Math/CLinearAlgebraHelper.cu:2155-2610, which run on the device). */
+clg_status clg_small_eig(int n, const double* a, const double* b, double* w, double* x);
 
 /* ------------------------------------------------------------------ HMC fermion force
  * CFieldFermionWilsonSquareSU3::DerivateDOperator / _kernelDWilsonForceSU3

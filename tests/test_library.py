@@ -82,3 +82,28 @@ def test_md5_rfc1321_vectors(lib_path):
     for n in (55, 56, 57, 63, 64, 65, 119, 120, 128, 1 << 20):
         b = rng.integers(0, 256, n, dtype=np.uint8).tobytes()
         assert clg.md5(b) == hashlib.md5(b).hexdigest(), n
+
+
+def test_small_dense_eigensolver(lib_path):
+    """The host eigensolver of the recycled solver: A x = w x and A x = w B x
+    (B Hermitian positive definite) on random complex matrices up to order 33,
+    against numpy's eigenvalues; residuals at rounding level; a Hermitian
+    matrix with repeated eigenvalues."""
+    import cudalatticegauge_b200 as clg
+
+    clg.load_library(lib_path)
+    rng = np.random.default_rng(7)
+    for n in (1, 2, 3, 5, 10, 20, 33):
+        A = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+        w, X = clg.small_eig(A)
+        assert np.abs(A @ X - X * w).max() < 1e-12 * np.abs(A).max()
+        np.testing.assert_allclose(np.sort(np.abs(w)), np.sort(np.abs(np.linalg.eigvals(A))), rtol=1e-10)
+        M = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+        B = M @ M.conj().T + n * np.eye(n)
+        w2, X2 = clg.small_eig(A, B)
+        assert np.abs(A @ X2 - (B @ X2) * w2).max() < 1e-12 * np.abs(A).max() * np.abs(B).max()
+    Q, _ = np.linalg.qr(rng.normal(size=(12, 12)) + 1j * rng.normal(size=(12, 12)))
+    H = Q @ np.diag([1, 1, 1, 2, 2, 3, 4, 5, 6, 7, 8, 9.0]) @ Q.conj().T
+    w, X = clg.small_eig(H)
+    assert np.abs(H @ X - X * w).max() < 1e-12
+    np.testing.assert_allclose(np.sort(w.real), [1, 1, 1, 2, 2, 3, 4, 5, 6, 7, 8, 9], atol=1e-12)
