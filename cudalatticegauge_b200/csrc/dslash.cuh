@@ -161,14 +161,28 @@ __device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packe
       g0[r] = h2_cmac<UDAG>(er, ei, h0[k], g0[r]);
       g1[r] = h2_cmac<UDAG>(er, ei, h1[k], g1[r]);
     }
+  // accumulation in FP32: rows whose phase is real (+-1) take one packed
+  // f32x2 FMA per complex number (sm_100 FFMA2); rows with an imaginary phase
+  // need the swapped pair and stay on two scalar FMAs
+  const float2 ss = make_float2(s, s), sn = make_float2(-s, -s);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const float2 f0 = __half22float2(g0[c]), f1 = __half22float2(g1[c]);
-    const cpx<float> a0 = mk<float>(f0.x, f0.y), a1 = mk<float>(f1.x, f1.y);
-    acc[c] = cfma(s, a0, acc[c]);
-    acc[3 + c] = cfma(s, a1, acc[3 + c]);
-    acc[6 + c] = cfma(s, mul_i(gperm(MU, 2) == 0 ? a0 : a1, gz4(MU, 2) + add), acc[6 + c]);
-    acc[9 + c] = cfma(s, mul_i(gperm(MU, 3) == 0 ? a0 : a1, gz4(MU, 3) + add), acc[9 + c]);
+    float2* av = reinterpret_cast<float2*>(acc);
+    av[c] = __ffma2_rn(ss, f0, av[c]);
+    av[3 + c] = __ffma2_rn(ss, f1, av[3 + c]);
+#pragma unroll
+    for (int row = 2; row < 4; ++row) {
+      const int z = (gz4(MU, row) + add) & 3;
+      const float2 f = gperm(MU, row) == 0 ? f0 : f1;
+      if (z == 0) {
+        av[3 * row + c] = __ffma2_rn(ss, f, av[3 * row + c]);
+      } else if (z == 2) {
+        av[3 * row + c] = __ffma2_rn(sn, f, av[3 * row + c]);
+      } else {
+        acc[3 * row + c] = cfma(s, mul_i(mk<float>(f.x, f.y), z), acc[3 * row + c]);
+      }
+    }
   }
 }
 
