@@ -98,7 +98,9 @@ typedef struct clg_solver_s* clg_solver;
 
 /* ------------------------------------------------------------------ context
  * Replaces appInitialCLG / CCLGLibManager::InitialWithParameter device setup
- * (Core/CLGLibManager.cpp:882-917).  stream == NULL creates a private stream. */
+ * (Core/CLGLibManager.cpp:882-917).  stream == NULL creates a private stream.
+ * Objects made on a context (lattices, gauge and fermion fields, solvers,
+ * whose workspaces hold fields) are destroyed before the context. */
 clg_status clg_context_create(int device, void* cuda_stream, clg_context* out);
 clg_status clg_context_destroy(clg_context ctx);
 clg_status clg_context_set_stream(clg_context ctx, void* cuda_stream);
