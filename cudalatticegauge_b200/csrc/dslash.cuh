@@ -216,16 +216,45 @@ __device__ __forceinline__ void neighbours(const Geom& g, int p, int64_t h, NbrI
 template <int P, typename AT>
 __device__ __forceinline__ void wilson_hop_finish(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
   const int64_t Vh = a.g.Vh;
-  const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
+  // the coefficients of the operators are real (-kappa, -kappa^2, 1): a real
+  // fast path (uniform branch) takes half the multiplies, packed f32x2 in FP32
+  if (a.a.y == 0.0) {
+    const AT ar = (AT)a.a.x;
+    if constexpr (sizeof(AT) == 4) {
+      float2* av = reinterpret_cast<float2*>(acc);
+      const float2 s2 = make_float2(ar, ar);
 #pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = ca * acc[k];
+      for (int k = 0; k < 12; ++k) av[k] = __fmul2_rn(s2, av[k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[k] = ar * acc[k];
+    }
+  } else {
+    const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = ca * acc[k];
+  }
   if (a.x) {
     cpx<AT> xv[12];
     const char* xp = reinterpret_cast<const char*>(a.x) + rhs * a.x_stride;
     load_site<P, 12, AT>(xp, a.x_norm ? a.x_norm + rhs * a.x_nstride : nullptr, Vh, h, xv);
-    const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
+    if (a.xa.y == 0.0) {
+      const AT xr = (AT)a.xa.x;
+      if constexpr (sizeof(AT) == 4) {
+        float2* av = reinterpret_cast<float2*>(acc);
+        const float2* xw = reinterpret_cast<const float2*>(xv);
+        const float2 s2 = make_float2(xr, xr);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) acc[k] = acc[k] + cx * xv[k];
+        for (int k = 0; k < 12; ++k) av[k] = __ffma2_rn(s2, xw[k], av[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) acc[k] = cfma(xr, xv[k], acc[k]);
+      }
+    } else {
+      const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[k] = acc[k] + cx * xv[k];
+    }
   }
   if (a.scale_dev) {
     const AT sc = (AT)a.scale_dev[rhs * a.scale_stride];

@@ -104,7 +104,7 @@ __device__ __forceinline__ void store_site(void* __restrict__ base, float* __res
     // 1/m of a float denormal overflows to inf and would turn the site into NaN
     // (point sources produce such sites after a few hops)
     if (!(m > 1e-30f)) m = 0.f;
-    const float inv = m > 0.f ? 1.0f / m : 0.f;
+    const float inv = m > 0.f ? __frcp_rn(m) : 0.f;  // the correctly rounded 1/m
     nrm[h] = m;
     if constexpr (NC % 4 == 0) {
       uint4* b = reinterpret_cast<uint4*>(base);
