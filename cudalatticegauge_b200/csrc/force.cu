@@ -555,9 +555,10 @@ clg_status clg_ks_force(clg_gauge F, clg_gauge U, int n, const clg_field* phi_i,
   }
   k.blk = phi_i[0]->blk;
   const int64_t nblk = (k.g.Vh + TILE - 1) / TILE;
-  // ring depth 2: 3, 4 and 5 stages (fewer blocks per SM) measured no faster;
-  // a barrier-free form with the poles loaded through registers by four
-  // direction threads per site in one warp ran at 782 us against 403
+  // ring depth 2: 3, 4 and 5 stages (fewer blocks per SM) measured no faster,
+  // nor did two or three poles per stage (409 / 606 us against 403); a
+  // barrier-free form with the poles loaded through registers by four
+  // direction threads per site in one warp ran at 782 us
   constexpr int nstage = 2;
   void (*kern)(KsForceArgs) = ks_force_kernel<nstage>;
   const size_t smem = ks_force_smem(nstage);
