@@ -145,8 +145,22 @@ __device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packe
       t = h2_cmac<false>(__low2half2(as_h2(u[c])), __high2half2(as_h2(u[c])), nd, t);
       return as_u32(t) ^ 0x80000000u;  // conjugate
     };
-    u[6] = cross(1, 5, 2, 4);
-    u[7] = cross(2, 3, 0, 5);
+    // u6 and u7 together, "planar" across the two: lane 0 carries u1 u5 - u2 u4,
+    // lane 1 u2 u3 - u0 u5, so the products need no broadcasts or swaps
+    const __half2 X = as_h2(__byte_perm(u[1], u[2], 0x5410)), Xi = as_h2(__byte_perm(u[1], u[2], 0x7632));
+    const __half2 Y = as_h2(__byte_perm(u[5], u[3], 0x5410)), Yi = as_h2(__byte_perm(u[5], u[3], 0x7632));
+    const __half2 Z = as_h2(__byte_perm(u[2], u[0], 0x5410)), Zi = as_h2(__byte_perm(u[2], u[0], 0x7632));
+    const __half2 W = as_h2(__byte_perm(u[4], u[5], 0x5410)), Wi = as_h2(__byte_perm(u[4], u[5], 0x7632));
+    __half2 re = __hmul2(X, Y);
+    re = __hfma2(__hneg2(Xi), Yi, re);
+    re = __hfma2(__hneg2(Z), W, re);
+    re = __hfma2(Zi, Wi, re);
+    __half2 nim = __hmul2(Z, Wi);  // minus the imaginary parts: the conjugate directly
+    nim = __hfma2(Zi, W, nim);
+    nim = __hfma2(__hneg2(X), Yi, nim);
+    nim = __hfma2(__hneg2(Xi), Y, nim);
+    u[6] = __byte_perm(as_u32(re), as_u32(nim), 0x5410);
+    u[7] = __byte_perm(as_u32(re), as_u32(nim), 0x7632);
     u[8] = cross(0, 4, 1, 3);
   }
   const __half2 zero = __float2half2_rn(0.f);
