@@ -1,6 +1,8 @@
 // api.cu -- the C ABI (include/clg_b200.h): contexts, lattices, gauge and
 // fermion fields, operator application (CField::ApplyOperator,
 // Data/Field/CField.h:203) and field BLAS.
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -14,6 +16,7 @@ namespace clg {
 clg_status gauge_generate(clg_gauge_s* U, int init, uint64_t seed, uint32_t fid, double eps);
 clg_status gauge_reorder(clg_gauge_s* U, double* dev_buf, int layout, int to_device);
 clg_status field_reorder(clg_field_s* f, int rhs, double* dev_buf, int to_device);
+clg_status field_stream(clg_field_s* f, int rhs, double* host_dev, int to_device, cudaStream_t s);
 clg_status field_source(clg_field_s* f, int rhs, int kind, uint64_t seed, uint32_t fid, int64_t site, int comp);
 clg_status gauge_plaquette(clg_gauge_s* U, double* host_out);
 clg_status gauge_unitarity(clg_gauge_s* U, double* host_out);
@@ -45,15 +48,32 @@ void dfree(void* p) {
 // bytes of one right-hand side of a host (FP64 lexicographic) field array
 static size_t host_rhs_bytes(const clg_field_s* f) { return (size_t)f->lat->g.V * f->nc() * 2 * sizeof(double); }
 
-// copy stream, staging slots and events of the asynchronous transfers
-static clg_status xfer_prepare(clg_field_s* f, bool import) {
+// The device address of a host buffer that the SMs can read and write
+// directly (pinned, mapped into the device's address space, 16-byte aligned),
+// for a field that takes the zero-copy path (FP64, CLG_ZERO_COPY=1), or
+// nullptr: pageable memory and other fields go through a device slot.
+static double* mapped_host(const clg_field_s* f, const void* p) {
+  const clg_context_s* ctx = f->lat->ctx;
+  if (!ctx->zero_copy || f->prec != CLG_PREC_DOUBLE || (reinterpret_cast<uintptr_t>(p) & 15)) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // not a pointer the runtime knows: pageable
+    return nullptr;
+  }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+  return static_cast<double*>(a.devicePointer);
+}
+
+// copy stream, staging slots (unless the transfer is zero-copy) and events of
+// the asynchronous transfers
+static clg_status xfer_prepare(clg_field_s* f, bool import, bool slot) {
   clg_context_s* ctx = f->lat->ctx;
   if (!ctx->copy_stream && cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
     ctx->copy_stream = nullptr;
     return ctx->fail(CLG_ERR_CUDA, "copy stream");
   }
   void*& buf = import ? f->xin : f->xout;
-  if (!buf)
+  if (slot && !buf)
     if (clg_status st = dalloc(ctx, &buf, host_rhs_bytes(f) * f->nrhs)) return st;
   auto make = [&](std::vector<cudaEvent_t>& v) -> bool {
     if (!v.empty()) return true;
@@ -65,17 +85,29 @@ static clg_status xfer_prepare(clg_field_s* f, bool import) {
   const bool ok = import ? (make(f->in_copied) && make(f->in_consumed)) : (make(f->out_ready) && make(f->out_copied));
   if (!ok) return ctx->fail(CLG_ERR_CUDA, "transfer events");
   if (import && f->in_pending.empty()) f->in_pending.assign(f->nrhs, 0);
+  if (!import && f->out_pending.empty()) f->out_pending.assign(f->nrhs, 0);
   return CLG_SUCCESS;
 }
 
+// Orders the context stream after the field's asynchronous transfers: an
+// import's data is in the field (reordered out of its slot, or written in
+// place), and no zero-copy export still reads it.  Every entry point that
+// reads or writes a field calls this first.
 clg_status settle(clg_field_s* f) {
-  if (f->in_pending.empty()) return CLG_SUCCESS;
   clg_context_s* ctx = f->lat->ctx;
-  for (int r = 0; r < f->nrhs; ++r) {
+  for (int r = 0; r < (int)f->out_pending.size(); ++r) {
+    if (!f->out_pending[r]) continue;
+    f->out_pending[r] = 0;
+    if (cudaStreamWaitEvent(ctx->stream, f->out_copied[r], 0) != cudaSuccess)
+      return ctx->fail(CLG_ERR_CUDA, "export: wait for the copy");
+  }
+  for (int r = 0; r < (int)f->in_pending.size(); ++r) {
     if (!f->in_pending[r]) continue;
+    const bool in_place = f->in_pending[r] == 2;
     f->in_pending[r] = 0;
     if (cudaStreamWaitEvent(ctx->stream, f->in_copied[r], 0) != cudaSuccess)
       return ctx->fail(CLG_ERR_CUDA, "import: wait for the copy");
+    if (in_place) continue;
     double* slot = reinterpret_cast<double*>(static_cast<char*>(f->xin) + r * host_rhs_bytes(f));
     if (clg_status st = field_reorder(f, r, slot, 1)) return st;
     if (cudaEventRecord(f->in_consumed[r], ctx->stream) != cudaSuccess) return ctx->fail(CLG_ERR_CUDA, "import event");
@@ -311,6 +343,8 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   ctx->l2_bytes = prop.l2CacheSize > 0 ? (size_t)prop.l2CacheSize : 0;
   if (const char* t = std::getenv("CLG_L2_WINDOW")) ctx->l2_window = t[0] != '0';
   if (const char* t = std::getenv("CLG_DEVICE_LOOP")) ctx->device_loops = t[0] == '1';
+  if (const char* t = std::getenv("CLG_ZERO_COPY")) ctx->zero_copy = t[0] == '1';
+  if (const char* t = std::getenv("CLG_XFER_BLOCKS")) ctx->xfer_blocks = std::max(1, std::min(4096, std::atoi(t)));
   // CLG_AUTOTUNE=0 keeps the default block size (reproducible profiling runs)
   if (const char* t = std::getenv("CLG_AUTOTUNE")) ctx->tuning_enabled = t[0] != '0';
   if (const char* t = std::getenv("CLG_FUSED_CG")) ctx->fused_cg = t[0] != '0';
@@ -624,7 +658,21 @@ clg_status clg_field_random(clg_field f, int rhs, int kind, uint64_t seed, uint3
 clg_status clg_field_import_async(clg_field f, int rhs, const double* data) {
   if (!f || !data || rhs < 0 || rhs >= f->nrhs) return CLG_ERR_BAD_ARG;
   clg_context_s* ctx = f->lat->ctx;
-  if (clg_status st = xfer_prepare(f, true)) return st;
+  double* direct = mapped_host(f, data);
+  if (clg_status st = xfer_prepare(f, true, !direct)) return st;
+  if (direct) {
+    // the field is rewritten on the copy stream once the work queued on the
+    // context stream so far (which may read or write it) has finished
+    if (clg_status st = settle(f)) return st;
+    cudaError_t e = cudaEventRecord(f->in_consumed[rhs], ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, f->in_consumed[rhs], 0);
+    if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("import_async: ") + cudaGetErrorString(e));
+    if (clg_status st = field_stream(f, rhs, direct, 1, ctx->copy_stream)) return st;
+    e = cudaEventRecord(f->in_copied[rhs], ctx->copy_stream);
+    if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("import_async: ") + cudaGetErrorString(e));
+    f->in_pending[rhs] = 2;
+    return CLG_SUCCESS;
+  }
   const size_t bytes = host_rhs_bytes(f);
   char* slot = static_cast<char*>(f->xin) + rhs * bytes;
   // the slot is overwritten only after the last reorder out of it
@@ -640,7 +688,20 @@ clg_status clg_field_export_async(clg_field f, int rhs, double* data) {
   if (!f || !data || rhs < 0 || rhs >= f->nrhs) return CLG_ERR_BAD_ARG;
   clg_context_s* ctx = f->lat->ctx;
   if (clg_status st = settle(f)) return st;
-  if (clg_status st = xfer_prepare(f, false)) return st;
+  double* direct = mapped_host(f, data);
+  if (clg_status st = xfer_prepare(f, false, !direct)) return st;
+  if (direct) {
+    // read on the copy stream after the work queued so far; later work on the
+    // field waits for the read (settle)
+    cudaError_t e = cudaEventRecord(f->out_ready[rhs], ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, f->out_ready[rhs], 0);
+    if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("export_async: ") + cudaGetErrorString(e));
+    if (clg_status st = field_stream(f, rhs, direct, 0, ctx->copy_stream)) return st;
+    e = cudaEventRecord(f->out_copied[rhs], ctx->copy_stream);
+    if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("export_async: ") + cudaGetErrorString(e));
+    f->out_pending[rhs] = 1;
+    return CLG_SUCCESS;
+  }
   const size_t bytes = host_rhs_bytes(f);
   double* slot = reinterpret_cast<double*>(static_cast<char*>(f->xout) + rhs * bytes);
   // the slot is refilled only after its last copy to the host

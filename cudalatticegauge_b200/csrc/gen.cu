@@ -243,6 +243,70 @@ __global__ void field_reorder_kernel(Geom g, DField f, int nparity, int rhs, dou
   }
 }
 
+// The same reorder with the FP64 lexicographic data in mapped pinned host
+// memory, read or written by the SMs over the host link (zero copy).  It runs
+// on the copy stream beside a solve, so it is built not to disturb one:
+//   - a block moves tiles of XS sites; the host side as consecutive 16-byte
+//     chunks (whole, contiguous link requests, all a thread's loads issued
+//     before the first is used), the device side one site per thread through
+//     a shared tile padded to NC + 1 chunks per site (conflict-free);
+//   - every access is a streaming one (ld/st .cs, evict-first in L2), so the
+//     transfer's bytes do not displace the solve's L2 working set;
+//   - a small grid-stride grid: a few blocks keep the link busy, and the SMs
+//     stay with the solve.
+// Used for FP64 fields only (the transfer format); others take the staging path.
+template <int NC>
+__global__ void __launch_bounds__(256) field_stream_kernel(Geom g, DField f, int nparity, int rhs, double2* host,
+                                                           int to_device) {
+  constexpr int XS = 128, ROW = NC + 1, CH = XS * NC, PER = (CH + 255) / 256;
+  __shared__ double2 tile[XS * ROW];
+  const int64_t ntiles = (g.V + XS - 1) / XS;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t s0 = t * XS;
+    const int ns = (int)min((int64_t)XS, g.V - s0);
+    double2* hb = host + s0 * NC;
+    const int j = threadIdx.x;
+    SiteIdx si;
+    bool held = false;
+    if (j < ns) {
+      si = site_from_linear(g, s0 + j);
+      held = nparity == 2 || si.p == f.first_parity;
+    }
+    if (to_device) {
+      double2 r[PER];
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int i = j + q * 256;
+        if (i < ns * NC) r[q] = __ldcs(hb + i);
+      }
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int i = j + q * 256;
+        if (i < ns * NC) tile[i + i / NC] = r[q];
+      }
+      __syncthreads();
+      if (held) {
+        double2* b = reinterpret_cast<double2*>(f.base(rhs, si.p));
+#pragma unroll
+        for (int k = 0; k < NC; ++k) __stcs(b + k * f.Vh + si.h, tile[j * ROW + k]);
+      }
+    } else {
+      if (j < ns) {
+        const double2* b = reinterpret_cast<const double2*>(f.base(rhs, held ? si.p : f.first_parity));
+#pragma unroll
+        for (int k = 0; k < NC; ++k) tile[j * ROW + k] = held ? __ldcs(b + k * f.Vh + si.h) : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int i = j + q * 256;
+        if (i < ns * NC) __stcs(hb + i, tile[i + i / NC]);
+      }
+    }
+    __syncthreads();  // the tile is refilled by the next iteration
+  }
+}
+
 template <int P, int NC>
 struct SourceF {
   DField f;
@@ -398,6 +462,23 @@ clg_status field_reorder(clg_field_s* f, int rhs, double* dev_buf, int to_device
     CLG_CUDA_OK(cudaGetLastError());
     return CLG_SUCCESS;
   });
+}
+
+clg_status field_stream(clg_field_s* f, int rhs, double* host_dev, int to_device, cudaStream_t s) {
+  clg_context_s* ctx = f->lat->ctx;
+  const Geom& g = f->lat->g;
+  if (f->prec != CLG_PREC_DOUBLE) return CLG_ERR_BAD_ARG;
+  const FieldRef r = f->ref();
+  const int64_t tiles = (g.V + 127) / 128;
+  const unsigned grid = (unsigned)std::min<int64_t>(tiles, ctx->xfer_blocks);
+  double2* h = reinterpret_cast<double2*>(host_dev);
+  if (f->nc() == 12)
+    field_stream_kernel<12><<<grid, 256, 0, s>>>(g, dfield(r), r.nparity, rhs, h, to_device);
+  else
+    field_stream_kernel<3><<<grid, 256, 0, s>>>(g, dfield(r), r.nparity, rhs, h, to_device);
+  ctx->kernels++;
+  CLG_CUDA_OK(cudaGetLastError());
+  return CLG_SUCCESS;
 }
 
 clg_status field_source(clg_field_s* f, int rhs, int kind, uint64_t seed, uint32_t fid, int64_t site, int comp) {

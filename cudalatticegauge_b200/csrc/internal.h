@@ -75,6 +75,14 @@ struct clg_context_s {
   size_t staging_bytes = 0;
   // stream of the asynchronous host transfers (created on first use)
   cudaStream_t copy_stream = nullptr;
+  // CLG_ZERO_COPY=1: asynchronous transfers of FP64 fields from/to pinned
+  // host memory are made by CLG_XFER_BLOCKS blocks on the copy stream reading
+  // or writing the host buffer directly, instead of a copy engine into a
+  // device slot plus a reorder.  Off by default: beside a 32^3x16 solve (13.8
+  // ms) the two 100 MB transfers per solve cost 0.85 ms with 8 blocks, 1.6 ms
+  // with 16 (the blocks take SM room from the solve), 0.8 ms by copy engine
+  bool zero_copy = false;
+  int xfer_blocks = 8;
   // block size chosen per kernel variant by the autotuner
   std::map<std::string, int> tuned;
   bool tuning_enabled = true;
@@ -137,7 +145,8 @@ struct clg_field_s {
   std::vector<cudaEvent_t> in_consumed;      // reorder out of a slot finished (context stream)
   std::vector<cudaEvent_t> out_ready;        // reorder into a slot finished (context stream)
   std::vector<cudaEvent_t> out_copied;       // D2H of a slot finished (copy stream)
-  std::vector<char> in_pending;              // slot copied but not yet reordered into the field
+  std::vector<char> in_pending;              // 1: slot copied, not yet reordered; 2: written in place
+  std::vector<char> out_pending;             // a zero-copy export may still be reading the field
   int nparity() const { return subset == CLG_SUBSET_FULL ? 2 : 1; }
   int nc() const { return kind == CLG_FERMION_WILSON ? 12 : 3; }
   clg::FieldRef ref() const {

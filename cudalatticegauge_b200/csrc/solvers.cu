@@ -111,6 +111,14 @@ struct Summary {
   double rr, rr0, resid_est, pad2;
 };
 
+// A few bytes between device memory and a solve's mapped pinned host buffers,
+// moved by one warp instead of a copy engine: a copy engine busy with a large
+// transfer queued on another stream (an overlapped field import or export of
+// 100 MB) holds a small copy back until that transfer has ended.
+__global__ void small_copy_kernel(uint32_t* dst, const uint32_t* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
 __global__ void kstate_summary(const KState* st, Summary* out, int nrhs) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nrhs) return;
@@ -274,6 +282,10 @@ struct Work : public SolveCacheBase {
   double* tol_d = nullptr;
   double* red_d = nullptr;   // per-rhs reduction outputs
   double* host_buf = nullptr;
+  // device addresses of sum_h and host_buf (mapped pinned memory), or nullptr
+  // where the device cannot address them (then the copy engines move them)
+  Summary* sum_hd = nullptr;
+  double* host_buf_d = nullptr;
   double2* shift_dev = nullptr;  // per-rhs shift sigma_r: the system is (op + sigma_r) x_r = b_r
   // Krylov operator temporaries (precision P)
   Owned kt_odd, kt_even, kt_full;
@@ -323,10 +335,28 @@ struct Work : public SolveCacheBase {
   }
 };
 
+// dst <- src, `bytes` (a multiple of 4) between device memory and a mapped
+// pinned host buffer, in stream order on the context stream
+static cudaError_t small_copy(clg_context_s* ctx, void* dst, const void* src, size_t bytes) {
+  small_copy_kernel<<<1, 32, 0, ctx->stream>>>(static_cast<uint32_t*>(dst), static_cast<const uint32_t*>(src),
+                                               (int)(bytes / 4));
+  ctx->kernels++;
+  return cudaGetLastError();
+}
+
+// host_buf[0, bytes) <- device memory, in stream order
+static cudaError_t to_host(Work& w, const void* src, size_t bytes) {
+  if (w.host_buf_d) return small_copy(w.ctx, w.host_buf_d, src, bytes);
+  return cudaMemcpyAsync(w.host_buf, src, bytes, cudaMemcpyDeviceToHost, w.ctx->stream);
+}
+
 clg_status read_summary(Work& w) {
-  kstate_summary<<<(w.nrhs + 63) / 64, 64, 0, w.ctx->stream>>>(w.st, w.sum_d, w.nrhs);
+  // the summary kernel writes the host buffer directly where it is mapped
+  kstate_summary<<<(w.nrhs + 63) / 64, 64, 0, w.ctx->stream>>>(w.st, w.sum_hd ? w.sum_hd : w.sum_d, w.nrhs);
   w.ctx->kernels++;
-  cudaError_t e = cudaMemcpyAsync(w.sum_h, w.sum_d, sizeof(Summary) * w.nrhs, cudaMemcpyDeviceToHost, w.ctx->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && !w.sum_hd)
+    e = cudaMemcpyAsync(w.sum_h, w.sum_d, sizeof(Summary) * w.nrhs, cudaMemcpyDeviceToHost, w.ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(w.ctx->stream);
   if (e != cudaSuccess) return w.ctx->fail(cuda_status(e), std::string("solver sync: ") + cudaGetErrorString(e));
   return CLG_SUCCESS;
@@ -912,6 +942,12 @@ clg_status clg::solve_core(const SolveReq& q) {
     if (cudaMallocHost((void**)&w.sum_h, sizeof(Summary) * nrhs) != cudaSuccess ||
         cudaMallocHost((void**)&w.host_buf, sizeof(double) * 4 * nrhs + 64) != cudaSuccess)
       return ctx->fail(CLG_ERR_OOM, "pinned host buffer");
+    if (cudaHostGetDevicePointer((void**)&w.sum_hd, w.sum_h, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&w.host_buf_d, w.host_buf, 0) != cudaSuccess) {
+      cudaGetLastError();
+      w.sum_hd = nullptr;
+      w.host_buf_d = nullptr;
+    }
   }
   cudaMemsetAsync(w.st, 0, sizeof(KState) * nrhs, ctx->stream);
 
@@ -964,8 +1000,7 @@ clg_status clg::solve_core(const SolveReq& q) {
   if (s) return s;
   if ((s = blas_norm2(ctx, b64.ref, w.red_d))) return s;
   std::vector<double> bn2(nrhs), rn2(nrhs);
-  if (cudaMemcpyAsync(w.host_buf, w.red_d, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+  if (to_host(w, w.red_d, sizeof(double) * nrhs) != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
     return ctx->fail(CLG_ERR_CUDA, "solve: reading |b|");
   for (int r = 0; r < nrhs; ++r) bn2[r] = w.host_buf[r];
 
@@ -1005,8 +1040,7 @@ clg_status clg::solve_core(const SolveReq& q) {
       return launch_sites<1>(ctx, Resid<NN.value>{dfield(b64.ref), dfield(r64.ref), w.red_d}, 0, npar, Vh, nrhs);
     });
     if (s) return s;
-    if (cudaMemcpyAsync(w.host_buf, w.red_d, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    if (to_host(w, w.red_d, sizeof(double) * nrhs) != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
       return ctx->fail(CLG_ERR_CUDA, "solve: reading |r|");
     bool all = true;
     for (int r = 0; r < nrhs; ++r) {
@@ -1037,8 +1071,13 @@ clg_status clg::solve_core(const SolveReq& q) {
       ((int*)(w.host_buf + nrhs))[r] = done[r];
       if (!done[r]) outer_count[r]++;
     }
-    cudaMemcpyAsync(w.tol_d, w.host_buf, sizeof(double) * nrhs, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(w.outer_done_d, w.host_buf + nrhs, sizeof(int) * nrhs, cudaMemcpyHostToDevice, ctx->stream);
+    if (w.host_buf_d) {
+      small_copy(ctx, w.tol_d, w.host_buf_d, sizeof(double) * nrhs);
+      small_copy(ctx, w.outer_done_d, w.host_buf_d + nrhs, sizeof(int) * nrhs);
+    } else {
+      cudaMemcpyAsync(w.tol_d, w.host_buf, sizeof(double) * nrhs, cudaMemcpyHostToDevice, ctx->stream);
+      cudaMemcpyAsync(w.outer_done_d, w.host_buf + nrhs, sizeof(int) * nrhs, cudaMemcpyHostToDevice, ctx->stream);
+    }
     // e ~= A^{-1} r in the inner precision
     if ((s = blas_copy(ctx, rP.ref, r64.ref))) return s;
     auto schur_solve = [&](bool dag, const FieldRef& rhs, const FieldRef& sol) -> clg_status {
