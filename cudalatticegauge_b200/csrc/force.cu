@@ -558,7 +558,9 @@ clg_status clg_ks_force(clg_gauge F, clg_gauge U, int n, const clg_field* phi_i,
   // ring depth 2: 3, 4 and 5 stages (fewer blocks per SM) measured no faster,
   // nor did two or three poles per stage (409 / 606 us against 403); a
   // barrier-free form with the poles loaded through registers by four
-  // direction threads per site in one warp ran at 782 us
+  // direction threads per site in one warp ran at 782 us; U and F read from
+  // global memory at the end instead of staged (4 blocks per SM at 128
+  // registers, against 3 with staging) ran at 551 us against 399
   constexpr int nstage = 2;
   void (*kern)(KsForceArgs) = ks_force_kernel<nstage>;
   const size_t smem = ks_force_smem(nstage);
