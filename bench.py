@@ -33,7 +33,7 @@ UNIT = "solves/s"
 WORKLOADS = {
     "wilson_eo_32x32x32x16": dict(dims=(32, 32, 32, 16), kappa=0.1355, eps=0.25, seed=0xC1A60001, nrhs=1),
     "wilson_eo_16x16x16x8": dict(dims=(16, 16, 16, 8), kappa=0.1355, eps=0.25, seed=0xC1A60001, nrhs=1),
-    # BASELINE config 4: 12 spin-colour point sources + 16 Z2 noise sources in one batched solve
+    # 12 spin-colour point sources + 16 Z2 noise sources in one batched solve
     "wilson_eo_batched_32x32x32x32": dict(dims=(32, 32, 32, 32), kappa=0.1355, eps=0.25, seed=0xC1A60003, nrhs=28,
                                           sources="point12_z2_16"),
 }
@@ -379,12 +379,12 @@ def ours(args, world, rank, local):
             xs.close()
         extra["solves"] = plain
         if args.workload == DEFAULT_WORKLOAD and not args.no_batched:
-            extra["batched_config4"] = batched_config4(clg, ctx, stream, args)
-            extra["uneven_lattices_config4"] = uneven_lattices(clg, ctx, stream, args)
+            extra["batched_28rhs_32x32x32x32"] = batched_sources(clg, ctx, stream, args)
+            extra["batched_uneven_lattices"] = uneven_lattices(clg, ctx, stream, args)
         if args.workload == DEFAULT_WORKLOAD and not args.no_side:
-            extra["config1"] = config1(clg, ctx, stream)
-            extra["dslash_config3"] = dslash_config3(clg, ctx, stream)
-            extra["staggered_multishift_config5"] = staggered_config5(clg, ctx, stream)
+            extra["wilson_8x8x8x8"] = wilson_small(clg, ctx, stream)
+            extra["dslash_48x48x48x24"] = dslash_large(clg, ctx, stream)
+            extra["staggered_multishift_32x32x32x16"] = staggered_multishift(clg, ctx, stream)
             extra["wilson_force_32x32x32x16"] = wilson_force_side(clg, ctx, stream)
             extra["staggered_force_32x32x32x16"] = ks_force_side(clg, ctx, stream)
         if world == 1 and not args.no_cpu:
@@ -413,8 +413,8 @@ def ours(args, world, rank, local):
     ctx.close()
 
 
-def batched_config4(clg, ctx, stream, args, steps=2):
-    """BASELINE config 4 measured beside the headline: 32^3x32, 12 spin-colour point
+def batched_sources(clg, ctx, stream, args, steps=2):
+    """Measured beside the headline: 32^3x32, 12 spin-colour point
     sources + 16 Z2 noise sources solved in one batched call (CGNE in the
     `--inner` precision inside FP64 defect correction), against one FP64 CGNE
     solve of a single source."""
@@ -468,8 +468,8 @@ def batched_config4(clg, ctx, stream, args, steps=2):
     return out
 
 
-def config1(clg, ctx, stream):
-    """BASELINE config 1: 8^4, Haar links (seed 0xC1A60000), kappa 0.1355, one
+def wilson_small(clg, ctx, stream):
+    """8^4, Haar links (seed 0xC1A60000), kappa 0.1355, one
     Gaussian source.  The full D and D^+ applied in FP64 (the whole problem
     sits in L2, so GB/s here is not a roofline claim) and D x = b solved to the
     true relative residual 1e-10 by GMRES(12), the reference's solver on this
@@ -514,7 +514,7 @@ def config1(clg, ctx, stream):
 
 
 def uneven_lattices(clg, ctx, stream, args, steps=2):
-    """BASELINE config 4, second part: the uneven set 8^4, 12^4, 16^4, 16^3x32,
+    """The uneven set 8^4, 12^4, 16^4, 16^3x32,
     24^3x16 (442,624 sites), 4 complex Gaussian sources each.  Each lattice's
     sources are one batched call (CGNE in the `--inner` precision, FP64 defect
     correction); the five calls are issued back to back on the context stream.
@@ -559,8 +559,8 @@ def uneven_lattices(clg, ctx, stream, args, steps=2):
     return out
 
 
-def dslash_config3(clg, ctx, stream):
-    """checkerboard Wilson hop on 48^3x24 (V = 2,654,208) in
+def dslash_large(clg, ctx, stream):
+    """Checkerboard Wilson hop on 48^3x24 (V = 2,654,208) in
     FP64 (18-real links), FP32 (12-real) and FP16 (12-real FP16 links, FP16
     spinors with a per-site FP32 norm); compulsory bytes per output site as in
     hop_bytes_per_site, against the measured copy peak."""
@@ -713,8 +713,8 @@ def ks_force_side(clg, ctx, stream, dims=(32, 32, 32, 16), mass=0.02, poles=12):
     return out
 
 
-def staggered_config5(clg, ctx, stream, steps=2):
-    """BASELINE config 5: 32^3x16 staggered fermions, 2am = 0.02 (the reference's
+def staggered_multishift(clg, ctx, stream, steps=2):
+    """32^3x16 staggered fermions, 2am = 0.02 (the reference's
     `Mass` parameter is 2am), BC (+,+,+,-), 12 shifts sigma_k = 10^(-4 + 5k/11),
     complex Gaussian source on the even sites; multi-shift CG on (DD^+)_ee + sigma_k
     in FP32 with every shift refined to the FP64 true residual 1e-10.  Unit: all

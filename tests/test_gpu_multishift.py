@@ -9,7 +9,7 @@ TOL = 1e-10
 
 
 def test_staggered_cgm_12_shifts(ctx, clg, oracle):
-    """BASELINE config 5 shape on 8^4: (DD^+)_ee + sigma_k, 12 shifts log-spaced 1e-4..10."""
+    """The 32^3x16 staggered multi-shift problem on 8^4: (DD^+)_ee + sigma_k, 12 shifts log-spaced 1e-4..10."""
     lat = clg.Lattice(ctx, (8, 8, 8, 8))
     m = 0.02
     U = clg.CFieldGaugeSU3(lat)

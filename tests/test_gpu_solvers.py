@@ -25,7 +25,7 @@ def gauge(clg, lat, kind, seed):
 
 @pytest.mark.parametrize("solver,prec", [("GMRES", 0), ("BiCGStab", 0), ("GMRES", 1), ("BiCGStab", 1), ("BiCGStab", 2)])
 def test_wilson_solve_haar_8x4(ctx, clg, oracle, solver, prec):
-    """BASELINE config 1 shape: 8^4 Haar links, kappa 0.1355, Gaussian source, D x = b."""
+    """8^4 Haar links, kappa 0.1355, Gaussian source, D x = b."""
     lat = clg.Lattice(ctx, (8, 8, 8, 8))
     U = gauge(clg, lat, "haar", 0xC1A60000)
     Uh = U.CopyDataOut()
