@@ -40,6 +40,7 @@ GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
  FILE_BRIDGEPP_TXT) = range(6)
 SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT, SOURCE_Z4 = 0, 1, 2, 3, 4
 SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS, SOLVER_GCRODR = 0, 1, 2, 3, 4, 5
+EEDT_SVD, EEDT_REV, EEDT_HEV = 0, 1, 2  # GCRO-DR deflation spaces (EEigenDeflationType)
 
 
 class CLGError(RuntimeError):
@@ -54,7 +55,7 @@ class SolverParams(C.Structure):
         ("absolute_accuracy", C.c_int32), ("deviation_step", C.c_int32), ("max_step", C.c_int32),
         ("small_rho", C.c_double), ("inner_precision", C.c_int32), ("tol_true_rel", C.c_double),
         ("inner_tol", C.c_double), ("max_iterations", C.c_int32), ("max_outer", C.c_int32),
-        ("even_odd", C.c_int32), ("use_graphs", C.c_int32), ("kdim", C.c_int32),
+        ("even_odd", C.c_int32), ("use_graphs", C.c_int32), ("kdim", C.c_int32), ("deflation", C.c_int32),
     ]
 
 
@@ -437,7 +438,7 @@ class _Solver:
         p = SolverParams()
         ctx.check(ctx.lib.clg_solver_default_params(self.KIND, C.byref(p)), "clg_solver_default_params")
         names = {
-            "MaxDim": "max_dim", "MDim": "max_dim", "KDim": "kdim", "Restart": "restart", "Accuracy": "accuracy", "AbsoluteAccuracy": "absolute_accuracy",
+            "MaxDim": "max_dim", "MDim": "max_dim", "KDim": "kdim", "DeflateSpace": "deflation", "Restart": "restart", "Accuracy": "accuracy", "AbsoluteAccuracy": "absolute_accuracy",
             "DiviationStep": "deviation_step", "MaxStep": "max_step", "SmallRho": "small_rho",
         }
         for k, v in kw.items():

@@ -7,9 +7,10 @@
 // Arnoldi vectors V orthogonal to C_k, so that
 //   A [U_k, V_{m-k}] = [C_k, V_{m-k+1}] G,  G = [[D_k, B], [0, Hbar]]
 // (D_k the norms that make U_k unit vectors).  The correction minimises the
-// residual over that space; then the k harmonic-Ritz-type vectors of the
-// cycle (the reference's default deflation space EEDT_SVD: the k smallest
-// eigenpairs of G^+ G p = l blockdiag(U^+ U, 1) p) become the next U_k:
+// residual over that space; then k vectors of the cycle's space become the
+// next U_k (the deflation space: the reference's default EEDT_SVD, the k
+// smallest eigenpairs of G^+ G p = l blockdiag(U^+ U, 1) p; or EEDT_REV Ritz
+// or EEDT_HEV harmonic Ritz vectors, clg_deflation):
 //   U_k = [U_k, V] P R^-1, C_k = [C_k, V] Q with G P = Q R.
 // The first solve starts with one GMRES(m) cycle whose Hbar gives the first
 // U_k; later solves (the same operator, e.g. successive molecular-dynamics
@@ -253,6 +254,7 @@ clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_g
   if (!(even ? even_op : full_op)) return ctx->fail(CLG_ERR_BAD_ARG, "GCRO-DR: operator and field subset do not match");
   if (clg_status st = gauge_prepare(Ug, CLG_PREC_DOUBLE)) return st;
   const int m = S->p.max_dim, k = S->p.kdim > 0 ? S->p.kdim : S->p.max_dim - 2;
+  const int defl = S->p.deflation;
 
   // workspace (and the recycled U_k) for this lattice / operator / sizes
   auto* Wp = dynamic_cast<GcroWork*>(S->cache_gcro.get());
@@ -402,11 +404,19 @@ clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_g
     rnorm = g.norm(W.r);
     cycles = 1;
     if (mm == m) {
-      // FindPk1 (EEDT_SVD): the k smallest eigenpairs of Hbar^+ Hbar
+      // FindPk1 (:541-570): SVD the k smallest eigenpairs of Hbar^+ Hbar; REV
+      // the k smallest of the square H_m; HEV the k largest of H_m p = l Hbar^+ Hbar p
       std::vector<Z> ev;
       Mat X;
-      if (dense::eig(dense::mul_dag(H, H), ev, X)) {
-        const Mat P = dense::select(ev, X, k, true);
+      Mat Hm(m, m);
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) Hm(i, j) = H(i, j);
+      bool ok;
+      if (defl == CLG_DEFLATION_REV) ok = dense::eig(Hm, ev, X);
+      else if (defl == CLG_DEFLATION_HEV) ok = dense::geig(Hm, dense::mul_dag(H, H), ev, X);
+      else ok = dense::eig(dense::mul_dag(H, H), ev, X);
+      if (ok) {
+        const Mat P = dense::select(ev, X, k, defl != CLG_DEFLATION_HEV);
         Mat Q, R;
         if (dense::qr_thin(dense::mul(H, P), Q, R)) {
           // GenerateCU right after GMRES: U = W_m P R^-1, C = W_{m+1} Q
@@ -528,7 +538,11 @@ clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_g
     rnorm = g.norm(W.r);
     if (mm < m) continue;  // invariant subspace: keep U_k as it is
     const bool converged = rnorm <= tol * bnorm;
-    // FindPk2 (EEDT_SVD, :724-760): G^+ G p = l [[U^+ U, 0], [0, 1]] p, k smallest
+    // FindPk2 (:572-760), with W = [U, V_{m-k}], What = [C, V_{m-k+1}], A W = What G:
+    //   SVD  G^+ G p = l B p, k smallest, B = W^+ W = [[U^+ U, U^+ V], [V^+ U, 1]]
+    //        with the U^+ V blocks taken as 0 (the reference's B for SVD);
+    //   REV  (W^+ What) G p = l B p, k smallest;
+    //   HEV  G^+ (What^+ W) p = l G^+ G p, k largest.
     Mat Bm(m, m);
     for (int i = 0; i < m; ++i) Bm(i, i) = 1.0;
     for (int i = 0; i < k; ++i) {
@@ -541,8 +555,43 @@ clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_g
     }
     std::vector<Z> ev;
     Mat Xv;
-    if (!dense::geig(dense::mul_dag(G, G), Bm, ev, Xv)) continue;  // keep U_k
-    const Mat P = dense::select(ev, Xv, k, true);
+    bool ok;
+    if (defl == CLG_DEFLATION_SVD) {
+      ok = dense::geig(dense::mul_dag(G, G), Bm, ev, Xv);
+    } else {
+      // E(l, i) = What_l^+ U_i, i < k (the U columns of What^+ W; the V
+      // columns of W are the unit vectors e_j there, V being orthonormal and
+      // orthogonal to C)
+      std::vector<const FieldRef*> hat;
+      for (int i = 0; i < k; ++i) hat.push_back(&W.C[i]);
+      for (int j = 0; j <= m - k; ++j) hat.push_back(&W.V[j]);
+      Mat E(m + 1, k);
+      for (int i = 0; i < k; ++i) {
+        std::vector<Z> d;
+        if ((st = g.dots(W.U[i], hat, d))) return finish(st);
+        for (int l = 0; l <= m; ++l) E(l, i) = d[l];
+      }
+      if (defl == CLG_DEFLATION_REV) {
+        Mat AL(m, m + 1);  // W^+ What
+        for (int i = 0; i < k; ++i)
+          for (int j = 0; j <= m; ++j) AL(i, j) = std::conj(E(j, i));
+        for (int i = k; i < m; ++i) AL(i, i) = 1.0;
+        for (int i = 0; i < k; ++i)
+          for (int j = k; j < m; ++j) {
+            Bm(i, j) = AL(i, j);  // U_i^+ V_{j-k}
+            Bm(j, i) = std::conj(AL(i, j));
+          }
+        ok = dense::geig(dense::mul(AL, G), Bm, ev, Xv);
+      } else {
+        Mat AL(m + 1, m);  // What^+ W
+        for (int l = 0; l <= m; ++l)
+          for (int j = 0; j < k; ++j) AL(l, j) = E(l, j);
+        for (int j = k; j < m; ++j) AL(j, j) = 1.0;
+        ok = dense::geig(dense::mul_dag(G, AL), dense::mul_dag(G, G), ev, Xv);
+      }
+    }
+    if (!ok) continue;  // keep U_k
+    const Mat P = dense::select(ev, Xv, k, defl != CLG_DEFLATION_HEV);
     Mat Q, R;
     if (!dense::qr_thin(dense::mul(G, P), Q, R)) continue;
     // GenerateCU (:782-815): U = [U, V] P R^-1, C = [C, V] Q (C only while unconverged)

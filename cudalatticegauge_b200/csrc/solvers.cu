@@ -820,8 +820,9 @@ clg_status clg_solver_create(clg_context ctx, const clg_solver_params* p, clg_so
   if ((p->kind == CLG_SOLVER_GMRES || p->kind == CLG_SOLVER_FOM_MS) && (p->max_dim < 1 || p->max_dim > GM_MAXK))
     return ctx->fail(CLG_ERR_UNSUPPORTED, "GMRES / FOM MaxDim must be in [1, 16] on the device");
   if (p->kind == CLG_SOLVER_GCRODR &&
-      (p->max_dim < 5 || p->max_dim > 32 || p->kdim < 0 || (p->kdim > 0 && (p->kdim < 2 || p->kdim > p->max_dim - 2))))
-    return ctx->fail(CLG_ERR_BAD_ARG, "GCRO-DR: MDim in [5, 32], KDim in [2, MDim - 2]");
+      (p->max_dim < 5 || p->max_dim > 32 || p->kdim < 0 || (p->kdim > 0 && (p->kdim < 2 || p->kdim > p->max_dim - 2)) ||
+       p->deflation < CLG_DEFLATION_SVD || p->deflation > CLG_DEFLATION_HEV))
+    return ctx->fail(CLG_ERR_BAD_ARG, "GCRO-DR: MDim in [5, 32], KDim in [2, MDim - 2], deflation SVD / REV / HEV");
   clg_solver_s* s = new clg_solver_s();
   s->ctx = ctx;
   s->p = *p;

@@ -89,6 +89,13 @@ typedef enum {
     CLG_SOLVER_GCRODR = 5       /* CSLASolverGCRODR   SparseLinearAlgebra/CSolverGCRODR.cpp:196-911   */
 } clg_solver_kind;
 
+/* GCRO-DR deflation space (EEigenDeflationType, CSolverGCRODR.cpp:541-760):
+ * SVD the k smallest eigenpairs of G^+ G p = l diag(U^+ U, 1) p (the reference's default),
+ * REV the k smallest Ritz pairs W^+ A W p = l W^+ W p,
+ * HEV the k largest of G^+ What^+ W p = l G^+ G p (harmonic),
+ * where A W = What G is the cycle's Arnoldi relation. */
+typedef enum { CLG_DEFLATION_SVD = 0, CLG_DEFLATION_REV = 1, CLG_DEFLATION_HEV = 2 } clg_deflation;
+
 /* ------------------------------------------------------------------ handles */
 typedef struct clg_context_s* clg_context;
 typedef struct clg_lattice_s* clg_lattice;
@@ -235,6 +242,7 @@ typedef struct {
     int32_t even_odd;          /* solve D x = b through the even-odd Schur system         */
     int32_t use_graphs;        /* capture the inner iterations in CUDA graphs             */
     int32_t kdim;              /* KDim (GCRO-DR recycled dimension; 0: MaxDim - 2)         */
+    int32_t deflation;         /* DeflateSpace (GCRO-DR): clg_deflation, default SVD      */
 } clg_solver_params;
 
 typedef struct {
@@ -258,7 +266,7 @@ clg_status clg_solver_reset(clg_solver s);
  * (pStart).  info holds nrhs entries.  Returns CLG_SUCCESS only when every
  * right-hand side reached tol_true_rel.
  * GCRO-DR (CLG_SOLVER_GCRODR): FP64 fields, one right-hand side, max_dim = MDim
- * (5..32), kdim = KDim (2..MDim-2), restart = cycles, x0 = b when no start
+ * (5..32), kdim = KDim (2..MDim-2), deflation = DeflateSpace, restart = cycles, x0 = b when no start
  * vector is given (CSolverGCRODR.cpp:216-223); inner_precision is not used. */
 clg_status clg_solve(clg_solver s, clg_field x, clg_field b, clg_gauge g, int op, clg_field x0, clg_solve_info* info);
 /* CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47):

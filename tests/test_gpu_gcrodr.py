@@ -77,6 +77,32 @@ def test_gcrodr_recycling_cuts_applications(ctx, clg, oracle):
     assert info["status"] == 0 and ops.true_residual(be.to_numpy(), xe.to_numpy()) <= TOL
 
 
+@pytest.mark.parametrize("space", ["EEDT_REV", "EEDT_HEV"])
+def test_gcrodr_deflation_spaces(ctx, clg, oracle, space):
+    """DeflateSpace REV (Ritz vectors) and HEV (harmonic Ritz vectors) on the
+    near-critical operator: the first solve (one GMRES cycle, FindPk1) and the
+    recycled solves after it (FindPk2 every cycle) reach 1e-10 and equal the
+    oracle's FP64 GMRES solution."""
+    dims = (8, 8, 8, 8)
+    kappa = 0.124
+    lat = clg.Lattice(ctx, dims)
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60093, 1, 0.1)
+    op = oracle.Operator("WILSON_D", dims, U.CopyDataOut(), kappa)
+    S = clg.CSLASolverGCRODR(ctx, MDim=32, KDim=24, Restart=2000, DeflateSpace=getattr(clg, space))
+    for r in range(3):
+        b = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+        b.InitialField(clg.SOURCE_GAUSS, 0xC1A60096, 2 + r)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+        info = S.Solve(x, b, U, clg.EFO_F_D)[0]
+        bh, xh = b.to_numpy(), x.to_numpy()
+        assert info["status"] == 0 and op.true_residual(bh, xh) <= TOL, (space, r, info)
+        if r == 2:
+            xo, _ = oracle.gmres(op, bh, maxdim=12, restart=2000, accuracy=1e-26)
+            assert rel(xh, xo) < 1e-7
+    S.close()
+
+
 def test_gcrodr_rejects_bad_arguments(ctx, clg):
     lat = clg.Lattice(ctx, (4, 4, 4, 4))
     U = clg.CFieldGaugeSU3(lat)
@@ -85,6 +111,8 @@ def test_gcrodr_rejects_bad_arguments(ctx, clg):
         clg.CSLASolverGCRODR(ctx, MDim=40)
     with pytest.raises(clg.CLGError):
         clg.CSLASolverGCRODR(ctx, MDim=10, KDim=9)
+    with pytest.raises(clg.CLGError):
+        clg.CSLASolverGCRODR(ctx, DeflateSpace=3)
     S = clg.CSLASolverGCRODR(ctx)
     b2 = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=2)
     x2 = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=2)
