@@ -435,6 +435,7 @@ clg_status clg_lattice_create(clg_context ctx, const int dims[4], const int bc[4
       return ctx->fail(CLG_ERR_UNSUPPORTED, "lattice extents must be even and >= 2");
     }
     lat->g.L[k] = dims[k];
+    lat->g.dL[k].set((unsigned)dims[k]);
     lat->g.bc[k] = bc ? (bc[k] < 0 ? -1 : 1) : (k == 3 ? -1 : 1);
     V *= dims[k];
   }

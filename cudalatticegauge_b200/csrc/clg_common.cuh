@@ -21,11 +21,31 @@ namespace clg {
 
 enum Prec : int { P64 = 0, P32 = 1, P16 = 2 };
 
+// Unsigned 32-bit division by a divisor fixed per lattice: one multiply-high,
+// a subtraction and two shifts instead of a division sequence (T. Granlund and
+// P. L. Montgomery, "Division by invariant integers using multiplication",
+// PLDI 1994, Fig. 4.1).  Exact for every n < 2^32 and 1 <= d < 2^31.
+struct FastDiv {
+  unsigned m = 1, s1 = 0, s2 = 0;
+  void set(unsigned d) {
+    unsigned l = 0;
+    while ((1ull << l) < d) ++l;
+    m = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    s1 = l < 1 ? l : 1;
+    s2 = l > 0 ? l - 1 : 0;
+  }
+  __device__ __forceinline__ unsigned div(unsigned n) const {
+    const unsigned t = __umulhi(m, n);
+    return (t + ((n - t) >> s1)) >> s2;
+  }
+};
+
 struct Geom {
   int L[4];      // Lx Ly Lz Lt
   int bc[4];     // fermion boundary signs
   int64_t V;     // volume
   int64_t Vh;    // V/2
+  FastDiv dL[4]; // division by L[mu]
 };
 
 // ---------------------------------------------------------------- complex helpers
@@ -69,11 +89,11 @@ template <typename T> __device__ __forceinline__ cpx<T> mul_i(cpx<T> a, int b) {
 __device__ __forceinline__ void eo_coords(const Geom& g, int p, int64_t h, int c[4]) {
   const unsigned s0 = 2u * (unsigned)h;
   const unsigned Lt = (unsigned)g.L[3], Lz = (unsigned)g.L[2], Ly = (unsigned)g.L[1];
-  unsigned r = s0 / Lt;
+  unsigned r = g.dL[3].div(s0);
   const int t0 = (int)(s0 - r * Lt);
-  unsigned q = r / Lz;
+  unsigned q = g.dL[2].div(r);
   c[2] = (int)(r - q * Lz);
-  r = q / Ly;
+  r = g.dL[1].div(q);
   c[1] = (int)(q - r * Ly);
   c[0] = (int)r;
   c[3] = t0 + ((c[0] + c[1] + c[2] + p) & 1);
