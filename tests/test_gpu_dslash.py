@@ -59,7 +59,9 @@ def test_bridgepp_import_plaquette(ctx, clg):
     assert abs(U.plaquette() - 0.625129946974942) < 1e-12
 
 
-@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (4, 6, 4, 8), (2, 2, 2, 2)])
+# (6, 10, 14, 12): extents that are not powers of two, for the multiply-high
+# division that turns a checkerboard index into coordinates
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (4, 6, 4, 8), (2, 2, 2, 2), (6, 10, 14, 12)])
 @pytest.mark.parametrize("dagger", [False, True])
 def test_wilson_D_fp64(ctx, clg, oracle, dims, dagger):
     lat = clg.Lattice(ctx, dims)
