@@ -633,7 +633,11 @@ clg_status schur_hop_odd(Work& w, bool dag, const FieldRef& in_even, const Field
   return hop(w.ctx, w.U, s);
 }
 
-// one CG iteration on A = M M^+ (m_dag_first) or M^+ M, fused as described above
+// one CG iteration on A = M M^+ (m_dag_first) or M^+ M, fused as described above.
+// Folding p = r + beta p into the second hop as well (hops on r, u = M^+ p
+// carried as u = M^+ r + beta u, 4 kernels per iteration) measured no faster on
+// the 32^3x16 FP16-inner solve: 13.44-13.72 against 13.26-13.36 ms (the
+// epilogue re-reads r and spills at the 80-register cap)
 template <int P>
 clg_status cg_fused_iteration(Work& w, int op, const FieldRef& x, const FieldRef& r, const FieldRef& p,
                               const int* skip, int ks) {
