@@ -1013,6 +1013,9 @@ clg_status clg::solve_core(const SolveReq& q) {
   std::vector<int> done(nrhs, 0), outer_count(nrhs, 0), status(nrhs, CLG_ERR_NOT_CONVERGED), iters(nrhs, 0);
   std::vector<int> inner_fail(nrhs, 0);
   const double2 one = make_double2(1, 0);
+  // floor of the inner tolerance per precision.  FP16 on the 32^3x16 solve:
+  // 2e-3 -> 230 applications in 5 outer cycles, 13.5 ms; 1e-3 -> 238 / 5,
+  // 14.2 ms; 5e-4 -> 240 / 4, 13.4 ms; 2e-4 -> 244 / 4, 13.3 ms (within run noise)
   const double lo_tol = w.P == CLG_PREC_DOUBLE ? 1e-14 : (w.P == CLG_PREC_SINGLE ? 1e-6 : 2e-3);
   const char* venv = std::getenv("CLG_VERBOSE");
   const bool verbose = venv && venv[0] == '1';
