@@ -143,14 +143,18 @@ struct SiteIdx {
   int64_t h;
 };
 __device__ __forceinline__ SiteIdx site_from_linear(const Geom& g, int64_t s) {
+  // V < 2^31: 32-bit multiply-high divisions by the extents
   SiteIdx r;
-  int64_t t = s;
-  r.c[3] = (int)(t % g.L[3]);
-  t /= g.L[3];
-  r.c[2] = (int)(t % g.L[2]);
-  t /= g.L[2];
-  r.c[1] = (int)(t % g.L[1]);
-  r.c[0] = (int)(t / g.L[1]);
+  unsigned t = (unsigned)s;
+  unsigned q = g.dL[3].div(t);
+  r.c[3] = (int)(t - q * (unsigned)g.L[3]);
+  t = q;
+  q = g.dL[2].div(t);
+  r.c[2] = (int)(t - q * (unsigned)g.L[2]);
+  t = q;
+  q = g.dL[1].div(t);
+  r.c[1] = (int)(t - q * (unsigned)g.L[1]);
+  r.c[0] = (int)q;
   r.s = s;
   r.p = (r.c[0] + r.c[1] + r.c[2] + r.c[3]) & 1;
   r.h = s >> 1;
