@@ -37,7 +37,11 @@ def gauss(clg, lat, seed):
     return out
 
 
-def test_round_trip_and_order(ctx, clg, oracle, lat):
+@pytest.mark.parametrize("zero_copy", ["0", "1"])
+def test_round_trip_and_order(clg, oracle, monkeypatch, zero_copy):
+    monkeypatch.setenv("CLG_ZERO_COPY", zero_copy)
+    ctx = clg.Context(0)
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
     U = clg.CFieldGaugeSU3(lat)
     U.InitialField(clg.GAUGE_HAAR, 0xC1A60011, 1)
     a = pinned((lat.volume, 4, 3))
@@ -72,6 +76,8 @@ def test_round_trip_and_order(ctx, clg, oracle, lat):
     np.testing.assert_array_equal(o2, b)
     f.close()
     U.close()
+    lat.close()
+    ctx.close()
 
 
 @pytest.mark.parametrize("prec,tol", [(1, 1e-7), (2, 1e-3)])
@@ -87,8 +93,14 @@ def test_low_precision_import(ctx, clg, lat, prec, tol):
     f.close()
 
 
-def test_pipelined_solves(ctx, clg, oracle, lat):
-    """Source k+1 in and solution k out overlap solve k+1 (two field pairs)."""
+@pytest.mark.parametrize("zero_copy", ["0", "1"])
+def test_pipelined_solves(clg, oracle, monkeypatch, zero_copy):
+    """Source k+1 in and solution k out overlap solve k+1 (two field pairs),
+    by copy engine and by SM loads/stores (CLG_ZERO_COPY=1, where a field still
+    being read by an export must not be overwritten by the next solve)."""
+    monkeypatch.setenv("CLG_ZERO_COPY", zero_copy)
+    ctx = clg.Context(0)
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
     U = clg.CFieldGaugeSU3(lat)
     U.InitialField(clg.GAUGE_EXPH, 0xC1A60012, 1, 0.25)
     op = oracle.Operator("WILSON_D", lat.dims, U.CopyDataOut(), KAPPA)
@@ -115,6 +127,8 @@ def test_pipelined_solves(ctx, clg, oracle, lat):
         f.close()
     S.close()
     U.close()
+    lat.close()
+    ctx.close()
 
 
 @pytest.mark.parametrize("cls,dims,subset", [("CFieldFermionWilsonSquareSU3", (4, 6, 4, 6), "FULL"),
