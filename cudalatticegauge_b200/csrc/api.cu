@@ -371,6 +371,13 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
     delete ctx;
     return CLG_ERR_OOM;
   }
+  if (clg_status st = noalloc_prepare(ctx)) {
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    dfree(ctx->red_partials);
+    dfree(ctx->red_counter);
+    delete ctx;
+    return st;
+  }
   *out = ctx;
   return CLG_SUCCESS;
 }

@@ -171,6 +171,8 @@ namespace clg {
 // Queue the pending asynchronous imports of f on the context stream (every
 // entry point that takes a field calls it before using the field).
 clg_status settle(clg_field_s* f);
+// clg_dot_noalloc's one-time set-up on a new context's device (noalloc.cu)
+clg_status noalloc_prepare(clg_context_s* ctx);
 
 // ------------------------------------------------------------ device allocation
 clg_status dalloc(clg_context_s* ctx, void** p, size_t bytes);

@@ -15,9 +15,13 @@
 //  - at most CLG_DOT_NOALLOC_MAX_RHS (64) right-hand sides; the block partials
 //    must fit in the array (checked, CLG_ERR_BAD_ARG otherwise);
 //  - every loaded GPU holds the 64 KiB array until the process exits;
-//  - the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture;
+//  - clg_context_create looks up the array's device address
+//    (cudaGetSymbolAddress, with the context's device current) and loads this
+//    file's kernels (cudaFuncGetAttributes).  Under CUDA's lazy module
+//    loading that is the moment the array and the kernel code take device
+//    memory, so it happens when the context is made, never inside
+//    clg_dot_noalloc: a caller that hands the rest of the GPU to its own pool
+//    after creating the context sees no allocation from this entry point;
 //  - all calls share the array and it keeps the last call's contents; the
 //    arrival counter is cleared at the start of every call; two calls that
 //    overlap on the GPU (different streams or contexts, same device) race on
@@ -83,6 +87,28 @@ struct DotNoAllocF {
 }  // namespace
 
 using namespace clg;
+
+namespace clg {
+// Called once by clg_context_create with the context's device current.
+clg_status noalloc_prepare(clg_context_s* ctx) {
+  double* base = nullptr;
+  if (clg_status st = scratch_address(ctx, &base)) return st;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaSuccess;
+  for (int prec = 0; prec < 3 && e == cudaSuccess; ++prec)
+    for (int nc : {12, 3}) {
+      with_pn(prec, nc, [&](auto P, auto NC) -> clg_status {
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, site_reduce_kernel<2, DotNoAllocF<P.value, NC.value>>);
+        return CLG_SUCCESS;
+      });
+    }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return ctx->fail(cuda_status(e), std::string("clg_dot_noalloc set-up: ") + cudaGetErrorString(e));
+  }
+  return CLG_SUCCESS;
+}
+}  // namespace clg
 
 extern "C" clg_status clg_dot_noalloc(clg_field a, clg_field b, double* re_im) {
   if (!a || !b || !re_im || a->lat != b->lat || a->kind != b->kind || a->subset != b->subset || a->nrhs != b->nrhs ||

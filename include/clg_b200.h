@@ -211,9 +211,12 @@ clg_status clg_dot(clg_field a, clg_field b, double* re_im);
  * cannot afford the device-wide synchronisation cudaMalloc / cudaFree imply.
  * Same result as clg_dot; the scratch lives in one fixed 64 KiB __device__
  * array of the library (held on every GPU that loads it until exit), so at most
- * CLG_DOT_NOALLOC_MAX_RHS right-hand sides (CLG_ERR_BAD_ARG beyond).  The first
- * call on a device looks the array up; make it before any stream capture.  All
- * calls share the array: calls that overlap on one GPU race. */
+ * CLG_DOT_NOALLOC_MAX_RHS right-hand sides (CLG_ERR_BAD_ARG beyond).
+ * clg_context_create looks the array up and loads its kernels on the context's
+ * device (the point where lazy module loading gives them device memory), so no
+ * call of this entry point allocates; create the context before handing the
+ * rest of the GPU to another pool.  All calls share the array: calls that
+ * overlap on one GPU race. */
 #define CLG_DOT_NOALLOC_MAX_RHS 64
 clg_status clg_dot_noalloc(clg_field a, clg_field b, double* re_im);
 clg_status clg_norm2(clg_field a, double* out);

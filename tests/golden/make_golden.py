@@ -30,7 +30,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def main(ref="/root/reference"):
+def main(ref):
     txt = os.path.join(ref, "Bin", "Debug", "bridgepp_conf_text.dat")
     vals = np.loadtxt(txt, dtype=np.float64)
     assert vals.size == 4 * 4 * 4 * 8 * 4 * 18
@@ -71,4 +71,8 @@ def main(ref="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    # the CudaLatticeGauge source tree: first argument, else $CLG_REFERENCE
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CLG_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <CudaLatticeGauge tree>  (or set CLG_REFERENCE)")
+    main(ref)

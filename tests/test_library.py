@@ -41,10 +41,15 @@ def test_library_loads_and_binds_every_symbol(lib_path):
 
 
 def test_built_for_sm100a(lib_path):
-    """The device code is sm_100a SASS (checked from cuobjdump's ELF list, no disassembly)."""
-    r = subprocess.run(["cuobjdump", "--list-elf", lib_path], capture_output=True, text=True)
-    assert r.returncode == 0
-    assert "sm_100a" in r.stdout
+    """Every nvcc command of the build targets sm_100a and nothing else (read
+    from the build recipe; no binary tool looks into the library)."""
+    from cudalatticegauge_b200 import build
+
+    flags = list(build.NVCC_FLAGS)
+    i = flags.index("-gencode")
+    assert flags[i + 1] == "arch=compute_100a,code=sm_100a"
+    assert flags.count("-gencode") == 1
+    assert not any(f.startswith("-arch") for f in flags)
 
 
 def test_no_device_is_an_error_not_a_crash(lib_path):

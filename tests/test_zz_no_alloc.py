@@ -44,6 +44,37 @@ def test_noalloc_dot_matches_dot_twice(ctx, clg):
     np.testing.assert_allclose(got[0], e1.Dot(e2), rtol=1e-12, atol=0)
 
 
+def test_noalloc_dot_allocates_nothing(ctx, clg):
+    """The property the entry point exists for: after the context is made, calls
+    leave the device's free memory unchanged (no allocation, lazy module loading
+    included).  Also the 64-right-hand-side limit and FP16 fields."""
+    import torch
+
+    lat = clg.Lattice(ctx, (8, 8, 8, 8))
+    a = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=64)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=64)
+    for r in range(64):
+        a.InitialField(clg.SOURCE_GAUSS, 100 + r, 2, rhs=r)
+        b.InitialField(clg.SOURCE_Z2, 200 + r, 3, rhs=r)
+    h1 = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF)
+    h2 = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF)
+    h1.InitialField(clg.SOURCE_GAUSS, 72, 2)
+    h2.InitialField(clg.SOURCE_GAUSS, 73, 2)
+    want64 = a.Dot(b)
+    want16 = h1.Dot(h2)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        st, got = noalloc_dot(clg, a, b)
+        assert st == clg.SUCCESS
+        np.testing.assert_allclose(got, want64, rtol=1e-12, atol=0)
+        st, got = noalloc_dot(clg, h1, h2)
+        assert st == clg.SUCCESS
+        np.testing.assert_allclose(got[0], want16, rtol=1e-12, atol=0)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+
+
 def test_noalloc_dot_rejects_too_many_rhs(ctx, clg):
     lat = clg.Lattice(ctx, (4, 4, 4, 4))
     a = clg.CFieldFermionKSSU3(lat, 0.02, nrhs=65)
