@@ -776,7 +776,8 @@ int clgo_fom_ms(const clgo_op* op, const double* b, int nshift, const double* sh
     cplx* y = (cplx*)calloc((size_t)m, sizeof(cplx));
     cplx* beta0 = (cplx*)calloc((size_t)nshift, sizeof(cplx));
     double* beta0len = (double*)calloc((size_t)nshift, sizeof(double));
-    const double blen = absolute ? 1.0 : sqrt(clgo_norm2(n, b));
+    /* fBLength = pFieldB->GetLength() = |b|^2 (CMultiShiftFOM.cpp:118-121), compared with |beta_n| */
+    const double blen = absolute ? 1.0 : clgo_norm2(n, b);
     memset(x, 0, sizeof(double) * 2 * n * nshift);
     int napply = 0, converged = 0, cycles = 0;
     double maxerr = 0;

@@ -207,7 +207,7 @@ def solver_block(kind, bnorm):
     if kind == "gmres":
         # stop when |g_m|^2 < Accuracy (absolute): relative estimate 1e-12
         return {"SolverName": "CSLASolverGMRES", "SolverForFieldId": 2, "UseCudaForSmallMatrix": 0,
-                "MaxDim": 12, "Restart": 500, "AbsoluteAccuracy": 1,
+                "MaxDim": 12, "Restart": 2000, "AbsoluteAccuracy": 1,
                 "Accuracy": repr((1e-12 * bnorm) ** 2)}
     if kind == "bicgstab":
         # stop when |s|^2 < Accuracy, checked every DiviationStep iterations
@@ -217,7 +217,7 @@ def solver_block(kind, bnorm):
     if kind == "fom":
         # stop when every |beta_n| < Accuracy
         return {"SolverName": "CMultiShiftFOM", "SolverForFieldId": 2, "UseCudaForSmallMatrix": 0,
-                "MaxDim": 30, "Restart": 500, "AbsoluteAccuracy": 1,
+                "MaxDim": 30, "Restart": 2000, "AbsoluteAccuracy": 1,
                 "Accuracy": repr(1e-12 * bnorm)}
     raise ValueError(kind)
 

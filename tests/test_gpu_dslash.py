@@ -89,6 +89,10 @@ def test_wilson_coefficients_and_products(ctx, clg, oracle, lat8):
     f.apply_to(clg.EFO_F_DDdagger, g, U)
     want = oracle.wilson_D(L, Uh, oracle.wilson_D(L, Uh, psi, KAPPA, dagger=True), KAPPA)
     assert rel(g.to_numpy(), want) < 1e-12
+    # EFO_F_DD (DDS, CFieldFermionWilsonSquareSU3.cu:989-1014): D applied twice, the coefficient once
+    f.apply_to(clg.EFO_F_DD, g, U, clg.EOCT_Real, 0.5)
+    want = 0.5 * oracle.wilson_D(L, Uh, oracle.wilson_D(L, Uh, psi, KAPPA), KAPPA)
+    assert rel(g.to_numpy(), want) < 1e-12
     # hopping blocks
     pm = clg.eo_parity(L)
     g.Zero()

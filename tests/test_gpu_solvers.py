@@ -23,7 +23,8 @@ def gauge(clg, lat, kind, seed):
     return U
 
 
-@pytest.mark.parametrize("solver,prec", [("GMRES", 0), ("BiCGStab", 0), ("GMRES", 1), ("BiCGStab", 1), ("BiCGStab", 2)])
+@pytest.mark.parametrize("solver,prec", [("GMRES", 0), ("BiCGStab", 0), ("GMRES", 1), ("BiCGStab", 1), ("BiCGStab", 2),
+                                         ("GMRES", 2)])
 def test_wilson_solve_haar_8x4(ctx, clg, oracle, solver, prec):
     """8^4 Haar links, kappa 0.1355, Gaussian source, D x = b."""
     lat = clg.Lattice(ctx, (8, 8, 8, 8))
