@@ -42,6 +42,32 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
   return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 
+// FP16 Wilson hop with the right-hand sides in pairs (wilson_hop_pair_kernel);
+// config = block size | (variant << 16): 0 caps at 128 registers, 1 at 96
+cudaError_t launch_wilson_pair(clg_context_s* ctx, const HopArgs& a, bool dagger, const std::string& key) {
+  const unsigned npairs = (unsigned)(a.nrhs + 1) / 2u;
+  auto go = [&](int cfg) {
+    const int bs = cfg & 0xffff;
+    const int variant = cfg >> 16;
+    dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * npairs));
+    if (variant == 1)
+      return dagger ? launch_pdl(ctx, wilson_hop_pair_kernel<true, 256, 2>, grid, dim3(bs), 0, a)
+                    : launch_pdl(ctx, wilson_hop_pair_kernel<false, 256, 2>, grid, dim3(bs), 0, a);
+    return dagger ? launch_pdl(ctx, wilson_hop_pair_kernel<true, 256, 1>, grid, dim3(bs), 0, a)
+                  : launch_pdl(ctx, wilson_hop_pair_kernel<false, 256, 1>, grid, dim3(bs), 0, a);
+  };
+  if (ctx->hop_pair_config >= 0) {
+    ctx->tuned[key + "_pair"] = ctx->hop_pair_config;  // the fused epilogue launches follow it
+    return go(ctx->hop_pair_config);
+  }
+  std::vector<int> cand;
+  for (int bs : {64, 128, 256}) {
+    cand.push_back(bs);
+    cand.push_back(bs | (1 << 16));
+  }
+  return go(tune_block(ctx, key + "_pair", idempotent(a), go, cand));
+}
+
 template <int P, int RECON>
 cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
   auto go = [&](int bs) {
@@ -232,6 +258,11 @@ static std::string hop_key(const clg_gauge_s* U, const HopSpec& s) {
          std::to_string(s.prec == CLG_PREC_SINGLE ? U->recon32 : 0);
 }
 
+int tuned_hop_pair_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback) {
+  auto it = ctx->tuned.find(hop_key(U, s) + "_pair");
+  return it == ctx->tuned.end() ? fallback : it->second;
+}
+
 int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback) {
   auto it = ctx->tuned.find(hop_key(U, s));
   if (it == ctx->tuned.end()) return fallback;
@@ -251,6 +282,8 @@ clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
       e = wilson ? launch_wilson<P32, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 12>(ctx, a, s.nrhs, key);
     else
       e = wilson ? launch_wilson<P32, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 18>(ctx, a, s.nrhs, key);
+  } else if (wilson && s.nrhs >= 2 && ctx->hop_pair) {
+    e = launch_wilson_pair(ctx, a, s.dagger, key);
   } else {
     e = wilson ? launch_wilson<P16, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P16, 12>(ctx, a, s.nrhs, key);
   }

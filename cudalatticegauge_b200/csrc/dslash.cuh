@@ -396,6 +396,239 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E
                                 !skipped);
 }
 
+// ---------------------------------------------------------------- FP16, two right-hand sides per thread
+// The multi-right-hand-side form of the FP16 hop (the batched solves of many
+// sources on one gauge field): one thread computes one output site for a pair
+// of right-hand sides (rhs0, rhs1).  The link of each direction is loaded and
+// its third row rebuilt once for both, the neighbour indices and boundary
+// signs are computed once, and the two spinors are held "planar": one half2
+// word carries the real parts of the same component of rhs0 and rhs1, another
+// the imaginary parts.  The spin projection's phases then cost nothing (they
+// select a plane and a sign), every HFMA2 of the colour product does useful
+// work for both right-hand sides, and the FP32 accumulation is one packed
+// f32x2 FMA per component pair.  Each product is evaluated with the same
+// operands in the same order as the one-rhs kernel (wilson_hop_dir16), so the
+// two kernels give bit-identical results.
+template <int MU, int SGN, bool UDAG>
+__device__ __forceinline__ void wilson_hop_dir16_pair(float2 accR[12], float2 accI[12], const Packed16& p0,
+                                                      const Packed16& p1, const PackedLink16& l, float s0, float s1) {
+  constexpr int add = SGN < 0 ? 2 : 0;
+  uint32_t w0[12], w1[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    w0[4 * k + 0] = p0.c[k].x; w0[4 * k + 1] = p0.c[k].y; w0[4 * k + 2] = p0.c[k].z; w0[4 * k + 3] = p0.c[k].w;
+    w1[4 * k + 0] = p1.c[k].x; w1[4 * k + 1] = p1.c[k].y; w1[4 * k + 2] = p1.c[k].z; w1[4 * k + 3] = p1.c[k].w;
+  }
+  // planar spin projection: h_j[c] = psi[j][c] + i^z_j psi[perm_j][c], j = 0, 1
+  __half2 hR[2][3], hI[2][3];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int ia = 3 * j + c, ib = 3 * gperm(MU, j) + c;
+      const __half2 aR = as_h2(__byte_perm(w0[ia], w1[ia], 0x5410)), aI = as_h2(__byte_perm(w0[ia], w1[ia], 0x7632));
+      const __half2 bR = as_h2(__byte_perm(w0[ib], w1[ib], 0x5410)), bI = as_h2(__byte_perm(w0[ib], w1[ib], 0x7632));
+      const int z = (gz4(MU, j) + add) & 3;
+      if (z == 0) { hR[j][c] = __hadd2(aR, bR); hI[j][c] = __hadd2(aI, bI); }
+      else if (z == 1) { hR[j][c] = __hsub2(aR, bI); hI[j][c] = __hadd2(aI, bR); }
+      else if (z == 2) { hR[j][c] = __hsub2(aR, bR); hI[j][c] = __hsub2(aI, bI); }
+      else { hR[j][c] = __hadd2(aR, bI); hI[j][c] = __hsub2(aI, bR); }
+    }
+  // the link (rows 0, 1 stored; row 2 = conj(row0 x row1)), as in wilson_hop_dir16
+  uint32_t u[9] = {l.a.x, l.a.y, l.a.z, l.a.w, l.b.x, l.b.y, 0u, 0u, 0u};
+  {
+    const __half2 zero = __float2half2_rn(0.f);
+    auto cross = [&](int a, int b, int c, int d) -> uint32_t {
+      __half2 t = h2_cmac<false>(__low2half2(as_h2(u[a])), __high2half2(as_h2(u[a])), u[b], zero);
+      const uint32_t nd = u[d] ^ 0x80008000u;
+      t = h2_cmac<false>(__low2half2(as_h2(u[c])), __high2half2(as_h2(u[c])), nd, t);
+      return as_u32(t) ^ 0x80000000u;
+    };
+    const __half2 X = as_h2(__byte_perm(u[1], u[2], 0x5410)), Xi = as_h2(__byte_perm(u[1], u[2], 0x7632));
+    const __half2 Y = as_h2(__byte_perm(u[5], u[3], 0x5410)), Yi = as_h2(__byte_perm(u[5], u[3], 0x7632));
+    const __half2 Z = as_h2(__byte_perm(u[2], u[0], 0x5410)), Zi = as_h2(__byte_perm(u[2], u[0], 0x7632));
+    const __half2 W = as_h2(__byte_perm(u[4], u[5], 0x5410)), Wi = as_h2(__byte_perm(u[4], u[5], 0x7632));
+    __half2 re = __hmul2(X, Y);
+    re = __hfma2(__hneg2(Xi), Yi, re);
+    re = __hfma2(__hneg2(Z), W, re);
+    re = __hfma2(Zi, Wi, re);
+    __half2 nim = __hmul2(Z, Wi);
+    nim = __hfma2(Zi, W, nim);
+    nim = __hfma2(__hneg2(X), Yi, nim);
+    nim = __hfma2(__hneg2(Xi), Y, nim);
+    u[6] = __byte_perm(as_u32(re), as_u32(nim), 0x5410);
+    u[7] = __byte_perm(as_u32(re), as_u32(nim), 0x7632);
+    u[8] = cross(0, 4, 1, 3);
+  }
+  // colour products on the planar pair: g = U h (UDAG: U^+ h), with the real
+  // part of the link element first, as h2_cmac does
+  const __half2 zero = __float2half2_rn(0.f);
+  __half2 gR[2][3], gI[2][3];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) { gR[j][r] = zero; gI[j][r] = zero; }
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t e = UDAG ? u[3 * k + r] : u[3 * r + k];
+      const __half2 er = __low2half2(as_h2(e)), ei = __high2half2(as_h2(e));
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        gR[j][r] = __hfma2(er, hR[j][k], gR[j][r]);
+        gI[j][r] = __hfma2(er, hI[j][k], gI[j][r]);
+        if (UDAG) {  // conj(e) h: re += ei hI, im -= ei hR
+          gR[j][r] = __hfma2(ei, hI[j][k], gR[j][r]);
+          gI[j][r] = __hfma2(ei, __hneg2(hR[j][k]), gI[j][r]);
+        } else {     // e h: re -= ei hI, im += ei hR
+          gR[j][r] = __hfma2(ei, __hneg2(hI[j][k]), gR[j][r]);
+          gI[j][r] = __hfma2(ei, hR[j][k], gI[j][r]);
+        }
+      }
+    }
+  // FP32 accumulation, packed over the pair
+  const float2 ss = make_float2(s0, s1), sn = make_float2(-s0, -s1);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float2 fR[2], fI[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      fR[j] = __half22float2(gR[j][c]);
+      fI[j] = __half22float2(gI[j][c]);
+      accR[3 * j + c] = __ffma2_rn(ss, fR[j], accR[3 * j + c]);
+      accI[3 * j + c] = __ffma2_rn(ss, fI[j], accI[3 * j + c]);
+    }
+#pragma unroll
+    for (int row = 2; row < 4; ++row) {
+      const int z = (gz4(MU, row) + add) & 3;
+      const int j = gperm(MU, row);
+      float2& aR = accR[3 * row + c];
+      float2& aI = accI[3 * row + c];
+      if (z == 0) { aR = __ffma2_rn(ss, fR[j], aR); aI = __ffma2_rn(ss, fI[j], aI); }
+      else if (z == 1) { aR = __ffma2_rn(sn, fI[j], aR); aI = __ffma2_rn(ss, fR[j], aI); }
+      else if (z == 2) { aR = __ffma2_rn(sn, fR[j], aR); aI = __ffma2_rn(sn, fI[j], aI); }
+      else { aR = __ffma2_rn(ss, fI[j], aR); aI = __ffma2_rn(sn, fR[j], aI); }
+    }
+  }
+}
+
+// H in for output site h of the right-hand sides rhs0 and rhs1 (FP16 storage,
+// 12-real links), then the finish (a H in + xa x, optional scale) per rhs.
+template <bool DAGGER>
+__device__ __forceinline__ void wilson_hop_site_pair16(const HopArgs& a, int rhs0, int rhs1, int64_t h,
+                                                       cpx<float> acc0[12], cpx<float> acc1[12]) {
+  const int64_t Vh = a.g.Vh;
+  const char* in0 = reinterpret_cast<const char*>(a.in) + rhs0 * a.in_stride;
+  const char* in1 = reinterpret_cast<const char*>(a.in) + rhs1 * a.in_stride;
+  const float* n0 = a.in_norm + rhs0 * a.in_nstride;
+  const float* n1 = a.in_norm + rhs1 * a.in_nstride;
+  NbrInfo nb;
+  int c[4];
+  neighbours(a.g, a.out_parity, h, nb, c);
+  float2 accR[12], accI[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    accR[k] = make_float2(0.f, 0.f);
+    accI[k] = make_float2(0.f, 0.f);
+  }
+  constexpr int SF = DAGGER ? 1 : -1;
+  constexpr int SB = -SF;
+#define CLG_WILSON_DIR16_PAIR(MU)                                                                         \
+  {                                                                                                       \
+    Packed16 pf0, pf1;                                                                                    \
+    PackedLink16 lf;                                                                                      \
+    load_packed16(in0, n0, Vh, nb.hf[MU], pf0);                                                           \
+    load_packed16(in1, n1, Vh, nb.hf[MU], pf1);                                                           \
+    load_packed_link16(a.U_here, MU, Vh, h, lf);                                                          \
+    wilson_hop_dir16_pair<MU, SF, false>(accR, accI, pf0, pf1, lf, nb.sf[MU] * pf0.n, nb.sf[MU] * pf1.n); \
+    Packed16 pb0, pb1;                                                                                    \
+    PackedLink16 lb;                                                                                      \
+    load_packed16(in0, n0, Vh, nb.hb[MU], pb0);                                                           \
+    load_packed16(in1, n1, Vh, nb.hb[MU], pb1);                                                           \
+    load_packed_link16(a.U_there, MU, Vh, nb.hb[MU], lb);                                                 \
+    wilson_hop_dir16_pair<MU, SB, true>(accR, accI, pb0, pb1, lb, nb.sb[MU] * pb0.n, nb.sb[MU] * pb1.n);  \
+  }
+  CLG_WILSON_DIR16_PAIR(0)
+  CLG_WILSON_DIR16_PAIR(1)
+  CLG_WILSON_DIR16_PAIR(2)
+  CLG_WILSON_DIR16_PAIR(3)
+#undef CLG_WILSON_DIR16_PAIR
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    acc0[k] = mk<float>(accR[k].x, accI[k].x);
+    acc1[k] = mk<float>(accR[k].y, accI[k].y);
+  }
+  wilson_hop_finish<P16>(a, rhs0, h, acc0);
+  wilson_hop_finish<P16>(a, rhs1, h, acc1);
+}
+
+// Pairs of right-hand sides are interleaved in blockIdx.x (pair = blockIdx.x %
+// npairs).  With an odd count the last pair's second member repeats the first
+// and is neither stored nor reduced.
+__device__ __forceinline__ void pair_of(const HopArgs& a, unsigned npairs, int& rhs0, int& rhs1, bool& has1,
+                                        unsigned& slot) {
+  const unsigned q = blockIdx.x % npairs;
+  slot = blockIdx.x / npairs;
+  rhs0 = 2 * (int)q;
+  has1 = rhs0 + 1 < a.nrhs;
+  rhs1 = has1 ? rhs0 + 1 : rhs0;
+}
+
+template <bool DAGGER, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_kernel(HopArgs a) {
+  const unsigned npairs = (unsigned)(a.nrhs + 1) / 2u;
+  int rhs0, rhs1;
+  bool has1;
+  unsigned slot;
+  pair_of(a, npairs, rhs0, rhs1, has1, slot);
+  const int64_t h = (int64_t)slot * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait();
+  if (h >= a.g.Vh) return;
+  const bool run0 = !(a.skip_dev && a.skip_dev[(int64_t)rhs0 * a.skip_stride]);
+  const bool run1 = has1 && !(a.skip_dev && a.skip_dev[(int64_t)rhs1 * a.skip_stride]);
+  if (!run0 && !run1) return;
+  cpx<float> acc0[12], acc1[12];
+  wilson_hop_site_pair16<DAGGER>(a, rhs0, rhs1, h, acc0, acc1);
+  if (run0) wilson_hop_store<P16>(a, rhs0, h, acc0);
+  if (run1) wilson_hop_store<P16>(a, rhs1, h, acc1);
+}
+
+// The pair form of wilson_hop_epi_kernel: E::site runs once per right-hand
+// side of the pair; the block reduces both right-hand sides' values.
+template <bool DAGGER, int MAXT, int MINB, class E>
+__global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_epi_kernel(HopArgs a, E e, double* partials,
+                                                                         unsigned* counter) {
+  const unsigned npairs = (unsigned)(a.nrhs + 1) / 2u;
+  int rhs0, rhs1;
+  bool has1;
+  unsigned slot;
+  pair_of(a, npairs, rhs0, rhs1, has1, slot);
+  const int64_t h = (int64_t)slot * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait();
+  const bool run0 = !(a.skip_dev && a.skip_dev[(int64_t)rhs0 * a.skip_stride]);
+  const bool run1 = has1 && !(a.skip_dev && a.skip_dev[(int64_t)rhs1 * a.skip_stride]);
+  double red[2 * E::NRED];
+#pragma unroll
+  for (int k = 0; k < 2 * E::NRED; ++k) red[k] = 0.0;
+  if ((run0 || run1) && h < a.g.Vh) {
+    cpx<float> acc0[12], acc1[12];
+    wilson_hop_site_pair16<DAGGER>(a, rhs0, rhs1, h, acc0, acc1);
+    if (run0) {
+      if constexpr (E::STORE) wilson_hop_store<P16>(a, rhs0, h, acc0);
+      e.site(rhs0, h, acc0, red);
+    }
+    if (run1) {
+      if constexpr (E::STORE) wilson_hop_store<P16>(a, rhs1, h, acc1);
+      e.site(rhs1, h, acc1, red + E::NRED);
+    }
+  }
+  grid_reduce_finalize_pair<E::NRED>(red, e, rhs0, rhs1, run0, run1, slot, gridDim.x / npairs, gridDim.x, a.nrhs,
+                                     partials, counter);
+}
+
 template <int P, int RECON>
 __global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
   using AT = typename AccT<P>::T;

@@ -92,6 +92,12 @@ struct clg_context_s {
   // CG on the Wilson normal equations fuses its vector work into the Schur
   // hops; CLG_FUSED_CG=0 runs the separate kernels instead
   bool fused_cg = true;
+  // FP16 Wilson hops over two or more right-hand sides compute them in pairs
+  // (one link load and reconstruction per pair); CLG_HOP_PAIR=0 keeps one
+  // right-hand side per thread; CLG_HOP_PAIR="<variant>:<block>" pins the paired
+  // launch (variant 0 uncapped, 1 capped at 128 registers)
+  bool hop_pair = true;
+  int hop_pair_config = -1;
   // hops and site kernels are launched with programmatic stream serialization
   // (they overlap the previous kernel's drain); CLG_PDL=0 launches them plainly
   bool pdl = true;
@@ -261,6 +267,8 @@ struct HopArgs;
 clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, HopArgs& a);
 // block size the autotuner chose for this hop (fallback if not tuned yet)
 int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
+// the tuned launch configuration (block | variant << 16) of the paired FP16 hop
+int tuned_hop_pair_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
 clg_status gauge_prepare(clg_gauge_s* U, int prec);  // builds the FP32 / FP16 copies on first use
 // address range of the link copy the hops of precision `prec` read (nullptr, 0 if none)
 void gauge_link_range(const clg_gauge_s* U, int prec, const void** base, size_t* bytes);

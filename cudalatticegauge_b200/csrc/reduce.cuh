@@ -102,4 +102,47 @@ __device__ __forceinline__ void grid_reduce_finalize(double (&acc)[NRED], const 
   grid_final_reduce<NRED>(f, nslots, nrhs, partials, counter);
 }
 
+// The same for a block that computes two right-hand sides (rhs0 with acc[0,
+// NRED), rhs1 with acc[NRED, 2 NRED)); c0 / c1 say which of them contribute
+// (each uniform over the block).  nblocks is the grid's total block count.
+template <int NRED, class F>
+__device__ __forceinline__ void grid_reduce_finalize_pair(double (&acc)[2 * NRED], const F& f, int rhs0, int rhs1,
+                                                          bool c0, bool c1, unsigned slot, unsigned nslots,
+                                                          unsigned nblocks, int nrhs, double* partials,
+                                                          unsigned* counter) {
+  __shared__ double sm[2 * NRED][8];
+  __shared__ bool last;
+  if (c0 || c1) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < 2 * NRED; ++k) {
+      double v = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) sm[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * NRED) {
+      const bool second = threadIdx.x >= NRED;
+      const int k = second ? threadIdx.x - NRED : threadIdx.x;
+      if (second ? c1 : c0) {
+        double v = 0.0;
+        for (int w = 0; w < nw; ++w) v += sm[threadIdx.x][w];
+        partials[((int64_t)(second ? rhs1 : rhs0) * nslots + slot) * NRED + k] = v;
+        __threadfence();
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(counter, 1u);
+    last = (t == nblocks - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  grid_final_reduce<NRED>(f, nslots, nrhs, partials, counter);
+}
+
 }  // namespace clg

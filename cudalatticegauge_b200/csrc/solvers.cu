@@ -560,6 +560,19 @@ bool fused_cg(const Work& w, int op) {
          (op == CLG_OP_MEE_MEEDAG || op == OP_MEEDAG_MEE);
 }
 
+// the paired FP16 form: config = block | variant << 16 as in launch_wilson_pair
+template <bool DAG, class E>
+cudaError_t launch_hop_pair_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int cfg) {
+  const int bs = cfg & 0xffff;
+  const unsigned npairs = (unsigned)(a.nrhs + 1) / 2u;
+  dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * npairs));
+  if ((cfg >> 16) == 1)
+    return launch_pdl(ctx, wilson_hop_pair_epi_kernel<DAG, 256, 2, E>, grid, dim3(bs), 0, a, e, ctx->red_partials,
+                      ctx->red_counter);
+  return launch_pdl(ctx, wilson_hop_pair_epi_kernel<DAG, 256, 1, E>, grid, dim3(bs), 0, a, e, ctx->red_partials,
+                    ctx->red_counter);
+}
+
 template <int P, int RECON, bool DAG, class E>
 cudaError_t launch_hop_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int bs) {
   dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * a.nrhs));
@@ -597,6 +610,17 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
   plain.x = nullptr;
   const int bs = tuned_hop_block(ctx, w.U, plain, P == P64 ? 64 : 128);
   const int64_t nblk = ((w.Vh + bs - 1) / bs) * w.nrhs;
+  if constexpr (P == P16) {
+    if (w.nrhs >= 2 && ctx->hop_pair) {
+      const int cfg = tuned_hop_pair_config(ctx, w.U, plain, 128);
+      const int pbs = cfg & 0xffff;
+      // partials are indexed [rhs][slot]: nslots x nrhs of them
+      if (clg_status st = ensure_reduction(ctx, ((w.Vh + pbs - 1) / pbs) * w.nrhs * E::NRED)) return st;
+      const cudaError_t perr = dag ? launch_hop_pair_epi<true>(ctx, a, e, cfg) : launch_hop_pair_epi<false>(ctx, a, e, cfg);
+      if (perr != cudaSuccess) return ctx->fail(cuda_status(perr), std::string("fused hop: ") + cudaGetErrorString(perr));
+      return CLG_SUCCESS;
+    }
+  }
   if (clg_status st = ensure_reduction(ctx, nblk * E::NRED)) return st;
   cudaError_t err;
   if constexpr (P == P64) {

@@ -67,3 +67,99 @@ def test_hop_variant(clg, oracle, pinned, cfg, prec, tol, dims):
             assert rel(f.to_numpy(r), want) < tol, (cfg, prec, dims, dagger, r)
         f.close()
     src.close()
+
+
+@pytest.fixture(scope="module")
+def ctx_single(clg):
+    """A second context whose FP16 Wilson hops keep one right-hand side per thread."""
+    import os
+
+    old = os.environ.get("CLG_HOP_PAIR")
+    os.environ["CLG_HOP_PAIR"] = "0"
+    try:
+        c = clg.Context(0)
+    finally:
+        if old is None:
+            del os.environ["CLG_HOP_PAIR"]
+        else:
+            os.environ["CLG_HOP_PAIR"] = old
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 10, 14, 12)])
+@pytest.mark.parametrize("nrhs", [2, 3, 5])
+@pytest.mark.parametrize("op", ["MEE", "MEE_DAG"])
+def test_fp16_pair_hop_bit_identical(ctx, ctx_single, clg, dims, nrhs, op):
+    """The paired FP16 hop (two right-hand sides per thread, planar) gives the
+    same bits as the one-rhs kernel; odd counts leave one unpaired member."""
+    outs = []
+    for c in (ctx, ctx_single):
+        lat = clg.Lattice(c, dims)
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+        f = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF, nrhs=nrhs)
+        for r in range(nrhs):
+            f.InitialField(clg.SOURCE_GAUSS, 300 + r, 2, rhs=r)
+        f.ApplyOperator(getattr(clg, "OP_" + op), U)
+        outs.append([f.to_numpy(r) for r in range(nrhs)])
+    for r in range(nrhs):
+        np.testing.assert_array_equal(outs[0][r], outs[1][r])
+
+
+@pytest.mark.parametrize("nrhs", [2, 3])
+def test_fp16_pair_cg_epilogues_identical(ctx, ctx_single, clg, oracle, nrhs):
+    """The fused CGNE iteration with paired hops and epilogues (CgHopAlpha,
+    CgHopUpdate over two right-hand sides per block) runs the same iterations
+    and gives the same solutions as the one-rhs kernels."""
+    res = []
+    for c in (ctx, ctx_single):
+        lat = clg.Lattice(c, (8, 8, 8, 16))
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+        b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=nrhs)
+        for r in range(nrhs):
+            b.InitialField(clg.SOURCE_GAUSS, 400 + r, 2, rhs=r)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=nrhs)
+        S = clg.CSLASolverCG(c, inner_precision=clg.HALF, tol_true_rel=1e-10)
+        infos = S.Solve(x, b, U, clg.EFO_F_D)
+        res.append(([i["iterations"] for i in infos], [x.to_numpy(r) for r in range(nrhs)], U.CopyDataOut(),
+                    [b.to_numpy(r) for r in range(nrhs)]))
+    assert res[0][0] == res[1][0]
+    op = oracle.Operator("WILSON_D", (8, 8, 8, 16), res[0][2], KAPPA)
+    for r in range(nrhs):
+        np.testing.assert_array_equal(res[0][1][r], res[1][1][r])
+        assert op.true_residual(res[0][3][r], res[0][1][r]) <= 1e-10
+
+
+@pytest.mark.parametrize("cfg", ["0:64", "0:128", "0:256", "1:64", "1:128", "1:256"])
+def test_fp16_pair_variants_vs_oracle(clg, oracle, cfg):
+    """Each paired launch variant (CLG_HOP_PAIR="<variant>:<block>") against the
+    FP64 oracle on a lattice with a partial last block, three right-hand sides."""
+    import os
+
+    os.environ["CLG_HOP_PAIR"] = cfg
+    try:
+        c = clg.Context(0)
+    finally:
+        del os.environ["CLG_HOP_PAIR"]
+    try:
+        dims = (6, 10, 14, 12)
+        lat = clg.Lattice(c, dims)
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+        Uh = U.CopyDataOut()
+        pm = clg.eo_parity(dims)
+        f = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF, nrhs=3)
+        src = []
+        for r in range(3):
+            g = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN)
+            g.InitialField(clg.SOURCE_GAUSS, 500 + r, 2)
+            src.append(g.to_numpy())
+            f.from_numpy(src[-1], rhs=r)
+        f.ApplyOperator(clg.OP_MEE, U)
+        for r in range(3):
+            want = oracle.wilson_mee(dims, Uh, src[r], KAPPA)[pm == 0]
+            assert rel(f.to_numpy(r)[pm == 0], want) < 5e-3
+    finally:
+        c.close()
