@@ -618,7 +618,8 @@ int clgo_bicgstab(const clgo_op* op, const double* b, double* x, const double* x
         int broke = 0;
         for (int j = 0; j < max_step * dev_step; ++j) {
             if (j == 0) rho = cdot(n, Rh, R);
-            const double lim = (restart == i + 1) ? 1.1754943508222875e-38 : small_rho;
+            /* last retry: _CLG_FLT_MIN of the FP64 build (Core/CLGFloat.h:115) */
+            const double lim = (restart == i + 1) ? 2.2250738585072014e-308 : small_rho;
             if (creal(rho * conj(rho)) < lim) { broke = 1; ++i; break; }
             clgo_apply(op, P, Vv); ++napply;
             alpha = rho / cdot(n, Rh, Vv);
@@ -857,4 +858,115 @@ int clgo_fom_ms(const clgo_op* op, const double* b, int nshift, const double* sh
     for (int i = 0; i < m; ++i) free(v[i]);
     free(v); free(W); free(R); free(h); free(hc); free(y); free(beta0); free(beta0len);
     return converged;
+}
+
+/* ============================================================== multi-shift BiCGStab
+ * CMultiShiftBiCGStab::Solve (SparseLinearAlgebra/CMultiShiftBiCGStab.cpp:73-437;
+ * B. Jegerlehner, hep-lat/9612014): (A + c_n) x_n = b for every shift over the
+ * BiCGStab recurrences of A, with the shadow residual w0 = conj(b) (the
+ * reference's Dagger of b).  Every `dev_step` iterations the residual estimates
+ * |s| and |s_n| are compared with accuracy * |b| (|b| = 1 when absolute).
+ * x holds nshift solutions of length n; shifts_c interleaved complex. */
+int clgo_bicgstab_ms(const clgo_op* op, const double* b, int nshift, const double* shifts_c, double* x,
+                     int dev_step, int max_step, double accuracy, int absolute, clgo_info* info) {
+    const long n = clgo_op_len(op);
+    double *R = valloc(n), *W = valloc(n), *W0 = valloc(n), *S = valloc(n), *SA = valloc(n), *WA = valloc(n);
+    double** Ss = (double**)malloc(sizeof(double*) * nshift);
+    cplx *betas = (cplx*)malloc(sizeof(cplx) * nshift), *zeta = (cplx*)malloc(sizeof(cplx) * nshift),
+         *zetaold = (cplx*)malloc(sizeof(cplx) * nshift), *rho = (cplx*)malloc(sizeof(cplx) * nshift),
+         *alphas = (cplx*)malloc(sizeof(cplx) * nshift);
+    double* sl = (double*)malloc(sizeof(double) * nshift);
+    memset(x, 0, sizeof(double) * 2 * n * nshift);
+    for (int s = 0; s < nshift; ++s) {
+        Ss[s] = valloc(n);
+        vcopy(n, b, Ss[s]);
+        betas[s] = 1; zeta[s] = 1; zetaold[s] = 1; rho[s] = 1; alphas[s] = 0; sl[s] = 1.0;
+    }
+    const double blen = absolute ? 1.0 : sqrt(clgo_norm2(n, b));
+    vcopy(n, b, R); vcopy(n, b, W); vcopy(n, b, S); vcopy(n, b, SA);
+    vcopy(n, b, W0);
+    for (long k = 0; k < n; ++k) W0[2 * k + 1] = -W0[2 * k + 1];   /* pW->Dagger() */
+    cplx delta = cdot(n, W0, R);
+    double* T = valloc(n);
+    clgo_apply(op, SA, T); vcopy(n, T, SA);
+    int napply = 1;
+    cplx phi = cdot(n, W0, SA) / delta;
+    cplx beta = 0, alpha = 0;
+    int done = 0, it = 0;
+    double maxerr = 0;
+    for (it = 0; it < max_step * dev_step; ++it) {
+        const cplx newbeta = -1.0 / phi;
+        for (int s = 0; s < nshift; ++s) {
+            if (sl[s] < accuracy * blen) continue;
+            const cplx c = shifts_c[2 * s] + I * shifts_c[2 * s + 1];
+            if (it == 0) {
+                zeta[s] = 1.0 / (1.0 - c * newbeta);
+                betas[s] = newbeta * zeta[s];
+            } else {
+                const cplx znm1 = zetaold[s];
+                zetaold[s] = zeta[s];
+                const cplx zb = znm1 * beta;
+                zeta[s] = (zetaold[s] * zb) / (alpha * (newbeta * (znm1 - zetaold[s])) + zb * (1.0 - c * newbeta));
+                betas[s] = newbeta * zeta[s] / zetaold[s];
+            }
+        }
+        beta = newbeta;
+        vcopy(n, R, W);
+        caxpy(n, beta, SA, W);
+        clgo_apply(op, W, WA); ++napply;
+        const cplx chi = cdot(n, WA, W) / clgo_norm2(n, WA);
+        for (int s = 0; s < nshift; ++s) {
+            if (sl[s] < accuracy * blen) continue;
+            const cplx c = shifts_c[2 * s] + I * shifts_c[2 * s + 1];
+            const cplx dinom = 1.0 + c * chi;
+            const cplx chis = chi / dinom;
+            const cplx chirho = chis * rho[s];
+            const cplx crz = chirho * zeta[s];
+            double* xs = x + 2 * n * s;
+            caxpy(n, -betas[s], Ss[s], xs);
+            caxpy(n, crz, W, xs);
+            caxpy(n, -(crz / betas[s]), W, Ss[s]);
+            caxpy(n, chirho * zetaold[s] / betas[s], R, Ss[s]);
+            rho[s] = rho[s] / dinom;
+        }
+        vcopy(n, W, R);
+        caxpy(n, -chi, WA, R);
+        const cplx newdelta = cdot(n, W0, R);
+        alpha = (beta * (-newdelta)) / (chi * delta);
+        delta = newdelta;
+        for (int s = 0; s < nshift; ++s) {
+            if (sl[s] < accuracy * blen) continue;
+            alphas[s] = (alpha * zeta[s] * betas[s]) / (zetaold[s] * beta);
+            cscale(n, alphas[s], Ss[s]);
+            caxpy(n, zeta[s] * rho[s], R, Ss[s]);
+        }
+        caxpy(n, -chi, SA, S);
+        cscale(n, alpha, S);
+        caxpy(n, 1.0, R, S);
+        clgo_apply(op, S, SA); ++napply;
+        phi = cdot(n, W0, SA) / delta;
+        if ((it + 1) % dev_step == 0) {
+            maxerr = sqrt(clgo_norm2(n, S));
+            for (int s = 0; s < nshift; ++s) {
+                if (sl[s] < accuracy * blen) continue;
+                sl[s] = sqrt(clgo_norm2(n, Ss[s]));
+                if (sl[s] > maxerr) maxerr = sl[s];
+            }
+            if (maxerr < accuracy * blen) { done = 1; break; }
+        }
+    }
+    if (info) {
+        info->iterations = napply; info->restarts = it; info->converged = done;
+        info->last_deviation = maxerr;
+        double worst = 0;
+        for (int s = 0; s < nshift; ++s) {
+            const double t = clgo_true_residual(op, b, x + 2 * n * s, shifts_c[2 * s], shifts_c[2 * s + 1]);
+            if (t > worst) worst = t;
+        }
+        info->true_rel_residual = worst;
+    }
+    for (int s = 0; s < nshift; ++s) free(Ss[s]);
+    free(Ss); free(betas); free(zeta); free(zetaold); free(rho); free(alphas); free(sl);
+    free(R); free(W); free(W0); free(S); free(SA); free(WA); free(T);
+    return done;
 }

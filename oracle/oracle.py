@@ -105,6 +105,7 @@ def lib():
             "clgo_cg": (i, [p, p, p, d, i, p]),
             "clgo_cgm": (i, [p, p, i, p, p, d, i, p]),
             "clgo_fom_ms": (i, [p, p, i, p, p, i, i, d, i, p]),
+            "clgo_bicgstab_ms": (i, [p, p, i, p, p, i, i, d, i, p]),
             "clgo_true_residual": (d, [p, p, p, d, d]),
         }
         for name, (res, args) in sig.items():
@@ -402,6 +403,17 @@ def fom_ms(op: Operator, b, shifts, maxdim=12, restart=100, accuracy=1e-10, abso
     info = Info()
     lib().clgo_fom_ms(C.byref(op.op), _ptr(b), len(sh), _ptr(sh.view(np.float64)), _ptr(x), maxdim, restart,
                       accuracy, int(absolute), C.byref(info))
+    return x, info.as_dict()
+
+
+def bicgstab_ms(op: Operator, b, shifts, dev_step=10, max_step=100, accuracy=1e-10, absolute=False):
+    """CMultiShiftBiCGStab (CMultiShiftBiCGStab.cpp:73-437) restated: (A + c_n) x_n = b."""
+    b = np.ascontiguousarray(b, np.complex128)
+    sh = np.ascontiguousarray(np.asarray(shifts, np.complex128))
+    x = np.empty((len(sh),) + b.shape, np.complex128)
+    info = Info()
+    lib().clgo_bicgstab_ms(C.byref(op.op), _ptr(b), len(sh), _ptr(sh.view(np.float64)), _ptr(x), dev_step, max_step,
+                           accuracy, int(absolute), C.byref(info))
     return x, info.as_dict()
 
 

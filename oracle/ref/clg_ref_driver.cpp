@@ -33,6 +33,7 @@
 //=============================================================================
 #include "CLGLib.h"
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -215,6 +216,9 @@ int main(int argc, char* argv[])
         }
         fflush(stdout);
     }
-    appQuitCLG();
-    return failures == 0 ? 0 : 4;
+    // every output is written; the process ends here without the library's
+    // teardown (appQuitCLG), which crashed on the host after the first job
+    fflush(stdout);
+    fflush(stderr);
+    std::_Exit(failures == 0 ? 0 : 4);
 }

@@ -189,6 +189,13 @@ def test_oracle_solvers_small(oracle):
     xs, i5 = oracle.fom_ms(op, b, cs, maxdim=12, restart=200, accuracy=1e-13)
     for k, s in enumerate(cs):
         assert op.true_residual(b, xs[k], complex(s)) < 1e-10
+    # BiCGStab-M (CMultiShiftBiCGStab.cpp:73-437) on the same shifts: every shift
+    # solved, and the same solutions as the FOM over one Krylov space
+    ys, i6 = oracle.bicgstab_ms(op, b, cs, dev_step=10, max_step=100, accuracy=1e-12)
+    assert i6["converged"]
+    for k, s in enumerate(cs):
+        assert op.true_residual(b, ys[k], complex(s)) < 1e-10
+        assert np.linalg.norm(ys[k] - xs[k]) < 1e-9 * np.linalg.norm(xs[k])
 
 
 def test_wilson_force_is_the_action_derivative(oracle):
