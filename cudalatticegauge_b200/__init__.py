@@ -39,7 +39,8 @@ GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
 (FILE_CLGBIN_DOUBLE, FILE_CLGBIN_FLOAT, FILE_CLGBIN_COMPRESSED, FILE_CLGBIN_COMPRESSED_FLOAT, FILE_BRIDGEPP_BIN,
  FILE_BRIDGEPP_TXT) = range(6)
 SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT, SOURCE_Z4 = 0, 1, 2, 3, 4
-SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS, SOLVER_GCRODR = 0, 1, 2, 3, 4, 5
+(SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS, SOLVER_GCRODR, SOLVER_NESTED_MS,
+ SOLVER_BICGSTAB_MS) = 0, 1, 2, 3, 4, 5, 6, 7
 EEDT_SVD, EEDT_REV, EEDT_HEV = 0, 1, 2  # GCRO-DR deflation spaces (EEigenDeflationType)
 
 
@@ -113,6 +114,7 @@ SIGNATURES = [
     ("clg_solver_reset", _S, [_P]),
     ("clg_solve", _S, [_P, _P, _P, _P, _I, _P, _P]),
     ("clg_solve_multishift", _S, [_P, _P, _I, _P, _P, _P, _I, _P]),
+    ("clg_solve_lattices", _S, [_P, _I, _P, _P, _P, _I, _P]),
     ("clg_rational_apply", _S, [_P, _P, _P, _I, _I, _D, _P, _P, _P]),
     ("clg_gauge_load", _S, [_P, C.c_char_p, _I]),
     ("clg_gauge_save", _S, [_P, C.c_char_p, _I, C.c_char_p]),
@@ -457,6 +459,21 @@ class _Solver:
             self.ctx.check(st, "clg_solve")
         return out
 
+    def SolveLattices(self, xs: Sequence["_FermionField"], bs: Sequence["_FermionField"],
+                      gauges: Sequence[CFieldGaugeSU3], op: int = EFO_F_D, raise_on_fail: bool = True):
+        """clg_solve_lattices: b[i] on lattice i (gauge gauges[i]) solved together in one
+        solve; returns one info dict per right-hand side, in lattice order."""
+        n = len(bs)
+        xa = (C.c_void_p * n)(*[x.h.value for x in xs])
+        ba = (C.c_void_p * n)(*[b.h.value for b in bs])
+        ua = (C.c_void_p * n)(*[u.h.value for u in gauges])
+        infos = (SolveInfo * sum(b.nrhs for b in bs))()
+        st = self.ctx.lib.clg_solve_lattices(self.h, n, xa, ba, ua, op, infos)
+        out = [i.as_dict() for i in infos]
+        if st != SUCCESS and raise_on_fail:
+            self.ctx.check(st, "clg_solve_lattices")
+        return out
+
     def close(self):
         if getattr(self, "h", None):
             self.ctx.lib.clg_solver_destroy(self.h)
@@ -505,7 +522,27 @@ class CMultiShiftCG(_MultiShift):
 
 
 class CMultiShiftFOM(_MultiShift):
+    """CMultiShiftFOM (CMultiShiftFOM.cpp:97-270): restarted FOM(MaxDim <= 32)
+    over one Krylov space for every shift, FP64 fields; MaxDim 30 as the
+    reference's TestSuit_Solver.yaml blocks use."""
     KIND = SOLVER_FOM_MS
+
+    def __init__(self, ctx: Context, **kw):
+        kw.setdefault("MaxDim", 30)
+        super().__init__(ctx, **kw)
+
+
+class CMultiShiftBiCGStab(_MultiShift):
+    """CMultiShiftBiCGStab (CMultiShiftBiCGStab.cpp:73-437): BiCGStab-M over one
+    Krylov space for every shift, FP64 fields; DiviationStep / MaxStep as the
+    reference's keys."""
+    KIND = SOLVER_BICGSTAB_MS
+
+
+class CMultiShiftNested(_MultiShift):
+    """CMultiShiftNested (CMultiShiftNested.cpp:69-145) in batched form: every
+    shift one right-hand side of a shifted solve (no shared Krylov space)."""
+    KIND = SOLVER_NESTED_MS
 
 
 class CSLASolverGCRODR(_Solver):

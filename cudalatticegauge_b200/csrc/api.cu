@@ -351,10 +351,12 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   if (const char* t = std::getenv("CLG_HOP_PAIR")) {
     int variant = -1, bs = 0;
     if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && (variant == 0 || variant == 1) &&
-        (bs == 64 || bs == 128 || bs == 256))
+        (bs == 64 || bs == 128 || bs == 256)) {
+      ctx->hop_pair = true;
       ctx->hop_pair_config = bs | (variant << 16);
-    else
-      ctx->hop_pair = t[0] != '0';
+    } else {
+      ctx->hop_pair = t[0] == '1';
+    }
   }
   if (const char* t = std::getenv("CLG_PDL")) ctx->pdl = t[0] != '0';
   if (const char* t = std::getenv("CLG_HOP_CONFIG")) {

@@ -89,6 +89,20 @@ bool same_shape(const FieldRef& a, const FieldRef& b) {
 
 }  // namespace
 
+clg_status blas_copy_strided(clg_context_s* ctx, const FieldRef& d, const FieldRef& s) {
+  if (d.nc != s.nc || d.nrhs != s.nrhs || d.first_parity != s.first_parity || d.nparity != s.nparity)
+    return ctx->fail(CLG_ERR_BAD_ARG, "strided copy: field shapes differ");
+  const int64_t vh = d.Vh < s.Vh ? d.Vh : s.Vh;
+  auto go = [&](auto PD, auto PS, auto NC) {
+    CopyF<PD.value, PS.value, NC.value> f{dfield(d), dfield(s)};
+    return launch_sites<0>(ctx, f, d.first_parity, d.nparity, vh, d.nrhs);
+  };
+  if (d.prec != CLG_PREC_DOUBLE || s.prec != CLG_PREC_DOUBLE)
+    return ctx->fail(CLG_ERR_BAD_ARG, "strided copy: FP64 fields");
+  return d.nc == 12 ? go(std::integral_constant<int, P64>{}, std::integral_constant<int, P64>{}, std::integral_constant<int, 12>{})
+                    : go(std::integral_constant<int, P64>{}, std::integral_constant<int, P64>{}, std::integral_constant<int, 3>{});
+}
+
 clg_status blas_dot(clg_context_s* ctx, const FieldRef& a, const FieldRef& b, double* dev_out) {
   if (!same_shape(a, b) || a.prec != b.prec) return ctx->fail(CLG_ERR_BAD_ARG, "dot: field shapes differ");
   return with_pn(a.prec, a.nc, [&](auto P, auto NC) {

@@ -68,6 +68,15 @@ cudaError_t launch_wilson_pair(clg_context_s* ctx, const HopArgs& a, bool dagger
   return go(tune_block(ctx, key + "_pair", idempotent(a), go, cand));
 }
 
+// a batch of lattices: one right-hand side per lattice segment, untuned
+template <int P, int RECON>
+cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagger) {
+  const int bs = P == P64 ? 64 : 128;
+  dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * a.nrhs));
+  return dagger ? launch_pdl(ctx, wilson_hop_batch_kernel<P, RECON, true>, grid, dim3(bs), 0, a)
+                : launch_pdl(ctx, wilson_hop_batch_kernel<P, RECON, false>, grid, dim3(bs), 0, a);
+}
+
 template <int P, int RECON>
 cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
   auto go = [&](int bs) {
@@ -119,7 +128,7 @@ __global__ void links_to_fp16(const double2* __restrict__ u64, void* out, int64_
 }  // namespace
 
 clg_status gauge_prepare(clg_gauge_s* U, int prec) {
-  if (prec == CLG_PREC_DOUBLE) return CLG_SUCCESS;
+  if (prec == CLG_PREC_DOUBLE || U->seg) return CLG_SUCCESS;  // a batch's lattices are prepared when it is built
   clg_context_s* ctx = U->lat->ctx;
   const int64_t Vh = U->lat->g.Vh;
   if (U->dirty_lowp) {
@@ -236,6 +245,12 @@ clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec
   a.skip_dev = s.skip_dev;
   a.skip_stride = s.skip_stride;
   a.nrhs = s.nrhs > 0 ? s.nrhs : 1;
+  a.seg = U->seg;
+  if (U->seg) {
+    if (s.kind != CLG_FERMION_WILSON) return ctx->fail(CLG_ERR_UNSUPPORTED, "a batch of lattices takes Wilson fermions");
+    a.U_here = a.U_there = nullptr;
+    return CLG_SUCCESS;
+  }
   if (s.prec == CLG_PREC_DOUBLE) {
     a.U_here = U->u64[p];
     a.U_there = U->u64[1 - p];
@@ -275,7 +290,11 @@ clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
   const bool wilson = s.kind == CLG_FERMION_WILSON;
   const std::string key = hop_key(U, s);
   cudaError_t e = cudaSuccess;
-  if (s.prec == CLG_PREC_DOUBLE) {
+  if (a.seg) {
+    e = s.prec == CLG_PREC_DOUBLE   ? launch_wilson_batch<P64, 18>(ctx, a, s.dagger)
+        : s.prec == CLG_PREC_SINGLE ? launch_wilson_batch<P32, 12>(ctx, a, s.dagger)
+                                    : launch_wilson_batch<P16, 12>(ctx, a, s.dagger);
+  } else if (s.prec == CLG_PREC_DOUBLE) {
     e = wilson ? launch_wilson<P64, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P64, 18>(ctx, a, s.nrhs, key);
   } else if (s.prec == CLG_PREC_SINGLE) {
     if (U->recon32 == 12)

@@ -22,6 +22,13 @@
 
 namespace clg {
 
+// One right-hand side of a batch of lattices: its lattice's geometry and link
+// arrays ([precision][parity]; FP64 18-real, FP32 and FP16 12-real).
+struct HopSeg {
+  Geom g;
+  const void* u[3][2];
+};
+
 struct HopArgs {
   Geom g;
   int out_parity;
@@ -46,6 +53,10 @@ struct HopArgs {
   const int* skip_dev;      // optional: rhs with skip_dev[rhs * skip_stride] != 0 are not computed
   int skip_stride;
   int nrhs;                 // right-hand sides (interleaved in blockIdx.x)
+  // a batch of lattices (nullable): right-hand side r lives on lattice seg[r]
+  // (geometry and links); g.Vh is then the fields' chunk stride, the largest
+  // checkerboard of the batch, and sites h >= seg[r].g.Vh are padding
+  const HopSeg* seg;
 };
 
 // chiral gamma tables (GammaMatrix.h:447-478): row r -> column perm[r] with phase i^z4[r]
@@ -283,16 +294,20 @@ __device__ __forceinline__ void wilson_hop_store(const HopArgs& a, int rhs, int6
                         a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, a.g.Vh, h, acc);
 }
 
-// The whole stencil for output site (rhs, h): acc = [scale *] (a H in + xa x)
+// The whole stencil for output site (rhs, h): acc = [scale *] (a H in + xa x),
+// on the lattice g with links U_here (parity out_parity) and U_there.  The
+// spinors' chunk stride is a.g.Vh (equal to g.Vh except in a batch of lattices).
 template <int P, int RECON, bool DAGGER, typename AT>
-__device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
+__device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom& g, const void* U_here,
+                                                   const void* U_there, int rhs, int64_t h, cpx<AT> acc[12]) {
   const int64_t Vh = a.g.Vh;
+  const int64_t lVh = g.Vh;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
   const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
 
   NbrInfo nb;
   int c[4];
-  neighbours(a.g, a.out_parity, h, nb, c);
+  neighbours(g, a.out_parity, h, nb, c);
 
 #pragma unroll
   for (int k = 0; k < 12; ++k) acc[k] = mk<AT>(0, 0);
@@ -312,9 +327,9 @@ __device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64
     Packed16 pf, pb;                                                                    \
     PackedLink16 lf, lb;                                                                \
     load_packed16(in, in_norm, Vh, nb.hf[MU], pf);                                      \
-    load_packed_link16(a.U_here, MU, Vh, h, lf);                                        \
+    load_packed_link16(U_here, MU, lVh, h, lf);                                         \
     load_packed16(in, in_norm, Vh, nb.hb[MU], pb);                                      \
-    load_packed_link16(a.U_there, MU, Vh, nb.hb[MU], lb);                               \
+    load_packed_link16(U_there, MU, lVh, nb.hb[MU], lb);                                \
     wilson_hop_dir16<MU, SF, false>(acc, pf, lf, nb.sf[MU] * pf.n);                     \
     wilson_hop_dir16<MU, SB, true>(acc, pb, lb, nb.sb[MU] * pb.n);                      \
   }
@@ -328,10 +343,10 @@ __device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64
   {                                                                                     \
     cpx<AT> psi[12], u[9];                                                              \
     load_site<P, 12, AT>(in, in_norm, Vh, nb.hf[MU], psi);                              \
-    load_link<P, RECON, AT>(a.U_here, MU, Vh, h, u);                                    \
+    load_link<P, RECON, AT>(U_here, MU, lVh, h, u);                                     \
     wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (AT)nb.sf[MU]);                      \
     load_site<P, 12, AT>(in, in_norm, Vh, nb.hb[MU], psi);                              \
-    load_link<P, RECON, AT>(a.U_there, MU, Vh, nb.hb[MU], u);                           \
+    load_link<P, RECON, AT>(U_there, MU, lVh, nb.hb[MU], u);                            \
     wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU]);                       \
   }
     CLG_WILSON_DIR(0)
@@ -341,6 +356,25 @@ __device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64
 #undef CLG_WILSON_DIR
   }
   wilson_hop_finish<P>(a, rhs, h, acc);
+}
+
+template <int P, int RECON, bool DAGGER, typename AT>
+__device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
+  wilson_hop_site_on<P, RECON, DAGGER>(a, a.g, a.U_here, a.U_there, rhs, h, acc);
+}
+
+// The precision index of the batch link table (HopSeg::u)
+template <int P> constexpr int seg_prec() { return P == P64 ? 0 : (P == P32 ? 1 : 2); }
+
+// Right-hand side rhs of a batch of lattices: its own geometry and links.
+// False for a padding site (h beyond that lattice's checkerboard).
+template <int P, int RECON, bool DAGGER, typename AT>
+__device__ __forceinline__ bool wilson_hop_site_batch(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
+  const HopSeg& sg = a.seg[rhs];
+  if (h >= sg.g.Vh) return false;
+  wilson_hop_site_on<P, RECON, DAGGER>(a, sg.g, sg.u[seg_prec<P>()][a.out_parity], sg.u[seg_prec<P>()][1 - a.out_parity],
+                                       rhs, h, acc);
+  return true;
 }
 
 // Register caps through the launch bounds (the autotuner picks per operator):
@@ -365,6 +399,21 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_kernel(HopArgs a) {
   wilson_hop_store<P>(a, rhs, h, acc);
 }
 
+// The hop over a batch of lattices (HopArgs::seg): right-hand side r on its own
+// lattice, the grid spanning the largest checkerboard.
+template <int P, int RECON, bool DAGGER>
+__global__ void __launch_bounds__(256) wilson_hop_batch_kernel(HopArgs a) {
+  using AT = typename AccT<P>::T;
+  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
+  const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait();
+  if (h >= a.g.Vh) return;
+  if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
+  cpx<AT> acc[12];
+  if (wilson_hop_site_batch<P, RECON, DAGGER>(a, rhs, h, acc)) wilson_hop_store<P>(a, rhs, h, acc);
+}
+
 // The hop with a fused epilogue E (used by the Krylov solvers):
 //   E::STORE      the result is stored to a.out (else it only feeds E::site)
 //   E::NRED       doubles reduced over the grid per rhs, E::finalize(rhs, tot)
@@ -373,7 +422,7 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_kernel(HopArgs a) {
 // Every thread reaches the block reduction: out-of-range sites contribute
 // zero; a block of a skipped (finished) right-hand side only takes its ticket,
 // and E::finalize ignores such right-hand sides.
-template <int P, int RECON, bool DAGGER, int MAXT, int MINB, class E>
+template <int P, int RECON, bool DAGGER, int MAXT, int MINB, class E, bool BATCH = false>
 __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E e, double* partials,
                                                                     unsigned* counter) {
   using AT = typename AccT<P>::T;
@@ -388,9 +437,15 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E
   for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
   if (!skipped && h < a.g.Vh) {
     cpx<AT> acc[12];
-    wilson_hop_site<P, RECON, DAGGER>(a, rhs, h, acc);
-    if constexpr (E::STORE) wilson_hop_store<P>(a, rhs, h, acc);
-    e.site(rhs, h, acc, red);
+    bool valid = true;
+    if constexpr (BATCH)
+      valid = wilson_hop_site_batch<P, RECON, DAGGER>(a, rhs, h, acc);
+    else
+      wilson_hop_site<P, RECON, DAGGER>(a, rhs, h, acc);
+    if (valid) {
+      if constexpr (E::STORE) wilson_hop_store<P>(a, rhs, h, acc);
+      e.site(rhs, h, acc, red);
+    }
   }
   grid_reduce_finalize<E::NRED>(red, e, rhs, slot, gridDim.x / (unsigned)a.nrhs, a.nrhs, partials, counter,
                                 !skipped);

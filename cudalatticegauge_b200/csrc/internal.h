@@ -92,11 +92,14 @@ struct clg_context_s {
   // CG on the Wilson normal equations fuses its vector work into the Schur
   // hops; CLG_FUSED_CG=0 runs the separate kernels instead
   bool fused_cg = true;
-  // FP16 Wilson hops over two or more right-hand sides compute them in pairs
-  // (one link load and reconstruction per pair); CLG_HOP_PAIR=0 keeps one
-  // right-hand side per thread; CLG_HOP_PAIR="<variant>:<block>" pins the paired
-  // launch (variant 0 uncapped, 1 capped at 128 registers)
-  bool hop_pair = true;
+  // CLG_HOP_PAIR=1: FP16 Wilson hops over two or more right-hand sides compute
+  // them in pairs (one link load and reconstruction per pair, planar half2
+  // arithmetic); CLG_HOP_PAIR="<variant>:<block>" pins the paired launch
+  // (variant 0 uncapped, 1 capped at 128 registers).  Off by default: measured
+  // on 32^3x16 / 32^3x32 it is no faster than one right-hand side per thread
+  // with the right-hand sides interleaved over the blocks (13.6 against 13.4 us
+  // per rhs at 8 rhs, 27.2 against 27.5 at 28), whose links are shared through L2
+  bool hop_pair = false;
   int hop_pair_config = -1;
   // hops and site kernels are launched with programmatic stream serialization
   // (they overlap the previous kernel's drain); CLG_PDL=0 launches them plainly
@@ -121,8 +124,15 @@ struct clg_lattice_s {
   clg::Geom g;
 };
 
+namespace clg {
+struct HopSeg;  // dslash.cuh
+}
+
 struct clg_gauge_s {
   clg_lattice_s* lat = nullptr;
+  // a batch of lattices (clg_solve_lattices): per right-hand side geometry and
+  // link arrays on the device; lat is then the batch's padded virtual lattice
+  const clg::HopSeg* seg = nullptr;
   // per parity link arrays [mu][chunk][h]
   void* u64[2] = {nullptr, nullptr};   // FP64, 18 reals
   void* u32[2] = {nullptr, nullptr};   // FP32, 12 reals (SU(3)) or 18
@@ -299,6 +309,9 @@ clg_status blas_norm2(clg_context_s* ctx, const FieldRef& a, double* dev_out);  
 clg_status blas_axpby(clg_context_s* ctx, const FieldRef& y, double2 a, const FieldRef& x, double2 b);  // y = a x + b y
 clg_status blas_copy(clg_context_s* ctx, const FieldRef& dst, const FieldRef& src);               // converts precision
 clg_status blas_zero(clg_context_s* ctx, const FieldRef& y);
+// dst <- src for FP64 fields that differ only in their chunk stride Vh: the
+// first min(Vh) sites of every parity block (a lattice inside a padded batch)
+clg_status blas_copy_strided(clg_context_s* ctx, const FieldRef& dst, const FieldRef& src);
 
 // ------------------------------------------------------------ solves (solvers.cu)
 // Workspace a solver keeps between calls (buffers, pinned host memory, captured
@@ -338,6 +351,8 @@ struct clg_solver_s {
   std::unique_ptr<clg::SolveCacheBase> cache_shift;  // multi-shift refinement
   std::unique_ptr<clg::SolveCacheBase> cache_cgm;    // multi-shift CG vectors, state, graph
   std::unique_ptr<clg::SolveCacheBase> cache_gcro;   // GCRO-DR vectors and the recycled subspace
+  std::unique_ptr<clg::SolveCacheBase> cache_fom;    // multi-shift FOM basis and solutions
+  std::unique_ptr<clg::SolveCacheBase> cache_batch;  // a batch of lattices: table, padded fields, workspace
   // X = (DD^+)^-1 phi and Y = D^+ X of clg_wilson_fermion_force
   clg_field force_x = nullptr, force_y = nullptr;
   // phi_i = (DD^+ + b_i)^-1 phi and phi_id = D0 phi_i of clg_ks_fermion_force

@@ -9,10 +9,14 @@
 // The reference has no CG-M; its multi-shift family (CMultiShiftFOM,
 // CMultiShiftGMRES, CMultiShiftBiCGStab, CMultiShiftNested) shares the interface.
 //
-// CLG_SOLVER_FOM_MS (any operator, complex shifts): all shifts are solved as one
-// batch of right-hand sides (one launch per step covers every shift) by GMRES
-// in the inner precision inside FP64 defect correction, the batched counterpart
-// of CMultiShiftNested::Solve (CMultiShiftNested.cpp:69-145).
+// CLG_SOLVER_FOM_MS (any operator, complex shifts): CMultiShiftFOM's restarted
+// FOM over one Krylov space in FP64 (mskrylov.cu), then the batched FP64
+// defect correction checks (and if needed refines) every shift.
+//
+// CLG_SOLVER_NESTED_MS (any operator, complex shifts): all shifts are solved as
+// one batch of right-hand sides (one launch per step covers every shift) by
+// GMRES in the inner precision inside FP64 defect correction, the batched
+// counterpart of CMultiShiftNested::Solve (CMultiShiftNested.cpp:69-145).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -22,6 +26,14 @@
 #include "krylov.cuh"
 
 namespace clg {
+
+clg_status fom_ms_run(clg_context_s* ctx, std::unique_ptr<SolveCacheBase>& cache, const clg_gauge_s* U, int kind,
+                      double param, int op, const FieldRef& b, const std::vector<double2>& shifts, int m,
+                      int restart, double tol, const FieldRef** X_out, int* apps_out, int* cycles_out);
+
+clg_status bicgstab_ms_run(clg_context_s* ctx, std::unique_ptr<SolveCacheBase>& cache, const clg_gauge_s* U, int kind,
+                           double param, int op, const FieldRef& b, const std::vector<double2>& shifts, int dev_step,
+                           int max_step, double tol, const FieldRef** X_out, int* apps_out, int* iters_out);
 
 constexpr int CGM_MAXSHIFT = 64;
 
@@ -363,11 +375,15 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
   if (clg_status st = settle(b)) return st;
   for (int k = 0; k < nshift; ++k)
     if (clg_status st = settle(x[k])) return st;
-  if (S->p.kind != CLG_SOLVER_CGM && S->p.kind != CLG_SOLVER_FOM_MS)
-    return ctx->fail(CLG_ERR_BAD_ARG, "clg_solve_multishift needs a CGM or FOM_MS solver");
+  if (S->p.kind != CLG_SOLVER_CGM && S->p.kind != CLG_SOLVER_FOM_MS && S->p.kind != CLG_SOLVER_NESTED_MS &&
+      S->p.kind != CLG_SOLVER_BICGSTAB_MS)
+    return ctx->fail(CLG_ERR_BAD_ARG, "clg_solve_multishift needs a CGM, FOM_MS, BICGSTAB_MS or NESTED_MS solver");
   std::vector<double2> sh(nshift);
   for (int k = 0; k < nshift; ++k) sh[k] = make_double2(shifts[2 * k], shifts[2 * k + 1]);
   const bool hermitian = op == CLG_OP_DDDAG || op == CLG_OP_DDDAG_EE || op == CLG_OP_MEE_MEEDAG;
+  // CG needs op + c_n Hermitian positive: real shifts >= 0 (complex shifts take GMRES)
+  bool real_nonneg = true;
+  for (int k = 0; k < nshift; ++k) real_nonneg = real_nonneg && sh[k].y == 0.0 && sh[k].x >= 0.0;
   clg_solver_params prm = S->p;
   clg_status s = CLG_SUCCESS;
   const int P = prm.inner_precision;
@@ -375,6 +391,8 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
   const int64_t Vh = b->lat->g.Vh;
   CgmWork* W = nullptr;
   int cgm_iters = 0;
+  const FieldRef* fom_x = nullptr;
+  int fom_apps = 0, fom_cycles = 0;
   const bool use_cgm = S->p.kind == CLG_SOLVER_CGM;
   if (use_cgm) {
     if (!hermitian) return ctx->fail(CLG_ERR_BAD_ARG, "CG-M needs a Hermitian positive operator (DDdagger forms)");
@@ -413,8 +431,25 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
     if ((s = cgm_run(ctx, *W, g, b->kind, b->param, op, b->ref(), real, itol, prm.max_iterations, &cgm_iters)))
       return s;
     prm.kind = CLG_SOLVER_CG;  // per-shift refinement
+  } else if (S->p.kind == CLG_SOLVER_FOM_MS || S->p.kind == CLG_SOLVER_BICGSTAB_MS) {
+    if (b->prec != CLG_PREC_DOUBLE)
+      return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift FOM / BiCGStab work on FP64 fields");
+    for (int k = 0; k < nshift; ++k)
+      if (x[k]->prec != CLG_PREC_DOUBLE)
+        return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift FOM / BiCGStab work on FP64 fields");
+    if ((s = gauge_prepare(g, CLG_PREC_DOUBLE))) return s;
+    if (S->p.kind == CLG_SOLVER_FOM_MS)
+      s = fom_ms_run(ctx, S->cache_fom, g, b->kind, b->param, op, b->ref(), sh, prm.max_dim, prm.restart,
+                     prm.tol_true_rel * 0.5, &fom_x, &fom_apps, &fom_cycles);
+    else
+      s = bicgstab_ms_run(ctx, S->cache_fom, g, b->kind, b->param, op, b->ref(), sh, std::max(1, prm.deviation_step),
+                          std::max(1, prm.max_step), prm.tol_true_rel * 0.5, &fom_x, &fom_apps, &fom_cycles);
+    if (s) return s;
+    // the FP64 check / refinement of every shift (GMRES at most 16 deep on the device)
+    prm.kind = hermitian && real_nonneg ? CLG_SOLVER_CG : CLG_SOLVER_GMRES;
+    prm.max_dim = std::min(prm.max_dim, (int)GM_MAXK);
   } else {
-    prm.kind = hermitian ? CLG_SOLVER_CG : CLG_SOLVER_GMRES;
+    prm.kind = hermitian && real_nonneg ? CLG_SOLVER_CG : CLG_SOLVER_GMRES;
   }
   SolveReq q;
   q.cache = &S->cache_shift;
@@ -430,11 +465,15 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
   q.b = b->ref();
   q.b_broadcast = true;
   if (use_cgm) q.x0 = &W->X.ref;
+  if (fom_x) q.x0 = fom_x;
   q.shifts = sh.data();
   for (int k = 0; k < nshift; ++k) q.xout.push_back(x[k]->ref());
   q.info = info;
   s = solve_core(q);
-  for (int k = 0; k < nshift; ++k) info[k].iterations += cgm_iters;
+  for (int k = 0; k < nshift; ++k) {
+    info[k].iterations += cgm_iters + fom_apps;
+    info[k].restarts += fom_cycles;
+  }
   return s;
 }
 

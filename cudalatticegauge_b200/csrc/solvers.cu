@@ -227,9 +227,13 @@ struct Owned {
     const int64_t blk = Vh * site_bytes_of(prec, nc);
     clg_status st = dalloc(ctx, &data, (size_t)blk * nparity * nrhs);
     if (st) return st;
+    // zeroed once: in a batch of lattices the sites past a lattice's own
+    // checkerboard are padding that every kernel leaves (or keeps) at zero
+    cudaMemsetAsync(data, 0, (size_t)blk * nparity * nrhs, ctx->stream);
     if (prec == CLG_PREC_HALF) {
       st = dalloc(ctx, (void**)&norm, (size_t)Vh * nparity * nrhs * sizeof(float));
       if (st) return st;
+      cudaMemsetAsync(norm, 0, (size_t)Vh * nparity * nrhs * sizeof(float), ctx->stream);
     }
     ref.data = (char*)data;
     ref.norm = norm;
@@ -577,6 +581,9 @@ template <int P, int RECON, bool DAG, class E>
 cudaError_t launch_hop_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int bs) {
   dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * a.nrhs));
   constexpr int MINB = P == P64 ? 1 : 3;
+  if (a.seg)  // a batch of lattices
+    return launch_pdl(ctx, wilson_hop_epi_kernel<P, RECON, DAG, 256, MINB, E, true>, grid, dim3(bs), 0, a, e,
+                      ctx->red_partials, ctx->red_counter);
   return launch_pdl(ctx, wilson_hop_epi_kernel<P, RECON, DAG, 256, MINB, E>, grid, dim3(bs), 0, a, e,
                     ctx->red_partials, ctx->red_counter);
 }
@@ -611,7 +618,7 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
   const int bs = tuned_hop_block(ctx, w.U, plain, P == P64 ? 64 : 128);
   const int64_t nblk = ((w.Vh + bs - 1) / bs) * w.nrhs;
   if constexpr (P == P16) {
-    if (w.nrhs >= 2 && ctx->hop_pair) {
+    if (w.nrhs >= 2 && ctx->hop_pair && !a.seg) {
       const int cfg = tuned_hop_pair_config(ctx, w.U, plain, 128);
       const int pbs = cfg & 0xffff;
       // partials are indexed [rhs][slot]: nslots x nrhs of them
@@ -842,11 +849,13 @@ clg_status clg_solver_default_params(int kind, clg_solver_params* p) {
 
 clg_status clg_solver_create(clg_context ctx, const clg_solver_params* p, clg_solver* out) {
   if (!ctx || !p || !out) return CLG_ERR_BAD_ARG;
-  if (p->kind < 0 || p->kind > CLG_SOLVER_GCRODR || p->inner_precision < 0 || p->inner_precision > 2 ||
+  if (p->kind < 0 || p->kind > CLG_SOLVER_BICGSTAB_MS || p->inner_precision < 0 || p->inner_precision > 2 ||
       !(p->tol_true_rel > 0) || p->max_iterations < 1 || p->max_outer < 1)
     return ctx->fail(CLG_ERR_BAD_ARG, "invalid solver parameters");
-  if ((p->kind == CLG_SOLVER_GMRES || p->kind == CLG_SOLVER_FOM_MS) && (p->max_dim < 1 || p->max_dim > GM_MAXK))
-    return ctx->fail(CLG_ERR_UNSUPPORTED, "GMRES / FOM MaxDim must be in [1, 16] on the device");
+  if ((p->kind == CLG_SOLVER_GMRES || p->kind == CLG_SOLVER_NESTED_MS) && (p->max_dim < 1 || p->max_dim > GM_MAXK))
+    return ctx->fail(CLG_ERR_UNSUPPORTED, "GMRES MaxDim must be in [1, 16] on the device");
+  if (p->kind == CLG_SOLVER_FOM_MS && (p->max_dim < 2 || p->max_dim > 32 || p->restart < 1))
+    return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift FOM: MaxDim in [2, 32], Restart >= 1");
   if (p->kind == CLG_SOLVER_GCRODR &&
       (p->max_dim < 5 || p->max_dim > 32 || p->kdim < 0 || (p->kdim > 0 && (p->kdim < 2 || p->kdim > p->max_dim - 2)) ||
        p->deflation < CLG_DEFLATION_SVD || p->deflation > CLG_DEFLATION_HEV))
@@ -870,7 +879,8 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
   if (X->lat != B->lat || U->lat != B->lat || X->kind != B->kind || X->subset != B->subset || X->nrhs != B->nrhs ||
       (X0 && (X0->lat != B->lat || X0->subset != B->subset || X0->nrhs != B->nrhs || X0->kind != B->kind)))
     return ctx->fail(CLG_ERR_BAD_ARG, "solve: field shapes differ");
-  if (S->p.kind == CLG_SOLVER_CGM || S->p.kind == CLG_SOLVER_FOM_MS)
+  if (S->p.kind == CLG_SOLVER_CGM || S->p.kind == CLG_SOLVER_FOM_MS || S->p.kind == CLG_SOLVER_NESTED_MS ||
+      S->p.kind == CLG_SOLVER_BICGSTAB_MS)
     return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift solvers are called through clg_solve_multishift");
   if (S->p.kind == CLG_SOLVER_GCRODR) return gcrodr_solve(S, X, B, U, op, X0, info);
   for (clg_field f : {X, B, X0})

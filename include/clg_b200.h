@@ -86,7 +86,9 @@ typedef enum {
     CLG_SOLVER_CG = 2,          /* CG on Hermitian positive operators (DD^+, staggered (DD^+)_ee)     */
     CLG_SOLVER_CGM = 3,         /* multi-shift CG (no reference twin; CMultiShiftSolver.h:38-47 API)  */
     CLG_SOLVER_FOM_MS = 4,      /* CMultiShiftFOM     SparseLinearAlgebra/CMultiShiftFOM.cpp:97-270   */
-    CLG_SOLVER_GCRODR = 5       /* CSLASolverGCRODR   SparseLinearAlgebra/CSolverGCRODR.cpp:196-911   */
+    CLG_SOLVER_GCRODR = 5,      /* CSLASolverGCRODR   SparseLinearAlgebra/CSolverGCRODR.cpp:196-911   */
+    CLG_SOLVER_NESTED_MS = 6,   /* CMultiShiftNested  SparseLinearAlgebra/CMultiShiftNested.cpp:69-145 */
+    CLG_SOLVER_BICGSTAB_MS = 7  /* CMultiShiftBiCGStab SparseLinearAlgebra/CMultiShiftBiCGStab.cpp:73-437 */
 } clg_solver_kind;
 
 /* GCRO-DR deflation space (EEigenDeflationType, CSolverGCRODR.cpp:541-760):
@@ -274,9 +276,33 @@ clg_status clg_solver_reset(clg_solver s);
 clg_status clg_solve(clg_solver s, clg_field x, clg_field b, clg_gauge g, int op, clg_field x0, clg_solve_info* info);
 /* CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47):
  * (op + c_n) x_n = b for n < nshift; shifts_re_im holds nshift complex shifts
- * (real for CGM); x[n] must not alias b (CMultiShiftSolver.h:35). */
+ * (real for CGM); x[n] must not alias b (CMultiShiftSolver.h:35).
+ *   CLG_SOLVER_CGM: multi-shift CG over one Krylov space in the inner precision
+ *     (Hermitian positive op, real shifts >= 0), then per-shift FP64 refinement.
+ *   CLG_SOLVER_FOM_MS: restarted FOM(max_dim <= 32) over one Krylov space for
+ *     every complex shift, FP64 (b and x FP64), restart = cycles, stop when every
+ *     shift's residual |beta_n| <= tol_true_rel |b|; then the true residuals are
+ *     checked in FP64 and refined if needed.
+ *   CLG_SOLVER_BICGSTAB_MS: BiCGStab-M (shadow residual conj(b)) over one Krylov
+ *     space for every complex shift, FP64, checked every deviation_step
+ *     iterations, at most max_step * deviation_step iterations; then checked and
+ *     refined like FOM_MS.
+ *   CLG_SOLVER_NESTED_MS: every shift solved as one right-hand side of a batched
+ *     shifted solve (GMRES / CG in the inner precision, FP64 defect correction):
+ *     the batched form of CMultiShiftNested, no shared Krylov space. */
 clg_status clg_solve_multishift(clg_solver s, clg_field* x, int nshift, const double* shifts_re_im, clg_field b,
                                 clg_gauge g, int op, clg_solve_info* info);
+/* Several lattices of uneven volume in one solve (no reference counterpart:
+ * the reference holds one lattice per process, Core/CudaHelper.cu:14-25, and
+ * changes it with appQuitCLG / appInitialCLG, Core/CLGLibManager.cpp:1131-1162).
+ * Lattice i: x[i], b[i] FULL FP64 Wilson fields with the same nrhs and U[i] its
+ * gauge field; one hopping parameter; op = CLG_OP_D or CLG_OP_DDAG; a GMRES,
+ * BiCGStab or CG solver (CG: CGNE on the even-odd system), low-precision inner
+ * solves need SU(3) links.  Every right-hand side of every lattice is one
+ * right-hand side of a single solve (one kernel per step covers all lattices);
+ * info holds sum_i nrhs_i entries in lattice order. */
+clg_status clg_solve_lattices(clg_solver s, int n, clg_field* x, clg_field* b, clg_gauge* U, int op,
+                              clg_solve_info* info);
 /* CFieldFermion::RationalApproximation (Data/Field/CField.cpp:114-145):
  * f <- c f + sum_i a_i (op + b_i)^{-1} f through one multi-shift solve. */
 clg_status clg_rational_apply(clg_solver s, clg_field f, clg_gauge g, int op, int degree, double c,

@@ -70,12 +70,13 @@ def test_hop_variant(clg, oracle, pinned, cfg, prec, tol, dims):
 
 
 @pytest.fixture(scope="module")
-def ctx_single(clg):
-    """A second context whose FP16 Wilson hops keep one right-hand side per thread."""
+def ctx_pair(clg):
+    """A second context whose FP16 Wilson hops compute pairs of right-hand sides
+    (CLG_HOP_PAIR=1; the default context keeps one right-hand side per thread)."""
     import os
 
     old = os.environ.get("CLG_HOP_PAIR")
-    os.environ["CLG_HOP_PAIR"] = "0"
+    os.environ["CLG_HOP_PAIR"] = "1"
     try:
         c = clg.Context(0)
     finally:
@@ -90,11 +91,11 @@ def ctx_single(clg):
 @pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 10, 14, 12)])
 @pytest.mark.parametrize("nrhs", [2, 3, 5])
 @pytest.mark.parametrize("op", ["MEE", "MEE_DAG"])
-def test_fp16_pair_hop_bit_identical(ctx, ctx_single, clg, dims, nrhs, op):
+def test_fp16_pair_hop_bit_identical(ctx, ctx_pair, clg, dims, nrhs, op):
     """The paired FP16 hop (two right-hand sides per thread, planar) gives the
     same bits as the one-rhs kernel; odd counts leave one unpaired member."""
     outs = []
-    for c in (ctx, ctx_single):
+    for c in (ctx, ctx_pair):
         lat = clg.Lattice(c, dims)
         U = clg.CFieldGaugeSU3(lat)
         U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
@@ -108,12 +109,12 @@ def test_fp16_pair_hop_bit_identical(ctx, ctx_single, clg, dims, nrhs, op):
 
 
 @pytest.mark.parametrize("nrhs", [2, 3])
-def test_fp16_pair_cg_epilogues_identical(ctx, ctx_single, clg, oracle, nrhs):
+def test_fp16_pair_cg_epilogues_identical(ctx, ctx_pair, clg, oracle, nrhs):
     """The fused CGNE iteration with paired hops and epilogues (CgHopAlpha,
     CgHopUpdate over two right-hand sides per block) runs the same iterations
     and gives the same solutions as the one-rhs kernels."""
     res = []
-    for c in (ctx, ctx_single):
+    for c in (ctx, ctx_pair):
         lat = clg.Lattice(c, (8, 8, 8, 16))
         U = clg.CFieldGaugeSU3(lat)
         U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)

@@ -27,8 +27,15 @@ def test_staggered_cgm_12_shifts(ctx, clg, oracle):
         assert op.true_residual(bh, xs[k].to_numpy(), complex(s)) <= TOL
 
 
-def test_wilson_fom_ms_complex_shifts(ctx, clg, oracle):
-    """The reference test's shifts {2, 1, 0.5, i, 0.5+0.5i, 1-i} on D (TestMultiShiftSolver.cpp:12-111)."""
+@pytest.mark.parametrize("op,name", [("EFO_F_D", "WILSON_D"), ("EFO_F_Ddagger", "WILSON_DDAG"),
+                                     ("EFO_F_DDdagger", "WILSON_DDDAG")])
+@pytest.mark.parametrize("method", ["FOM", "BiCGStab"])
+def test_wilson_fom_ms_complex_shifts(ctx, clg, oracle, op, name, method):
+    """CMultiShiftFOM / CMultiShiftBiCGStab over one Krylov space with the reference test's shifts
+    {2, 1, 0.5, i, 0.5+0.5i, 1-i} on D, D^+ and DD^+ (TestMultiShiftSolver.cpp:12-111):
+    every shift to the FP64 true residual 1e-10, the solutions equal to the
+    oracle's restated CMultiShiftFOM, and one shared space (the applications of
+    the FOM phase are counted once for all six shifts)."""
     lat = clg.Lattice(ctx, (4, 4, 4, 8))
     kappa = 0.1355
     U = clg.CFieldGaugeSU3(lat)
@@ -37,12 +44,31 @@ def test_wilson_fom_ms_complex_shifts(ctx, clg, oracle):
     b.InitialField(clg.SOURCE_GAUSS, 22, 2)
     cs = [2, 1, 0.5, 1j, 0.5 + 0.5j, 1 - 1j]
     xs = [clg.CFieldFermionWilsonSquareSU3(lat, kappa) for _ in cs]
-    S = clg.CMultiShiftFOM(ctx, inner_precision=clg.SINGLE)
-    infos = S.Solve(xs, cs, b, U, clg.EFO_F_D)
-    op = oracle.Operator("WILSON_D", lat.dims, U.CopyDataOut(), kappa)
+    if method == "FOM":
+        S = clg.CMultiShiftFOM(ctx, MaxDim=30, Restart=100)
+    else:  # CMultiShiftBiCGStab (CMultiShiftBiCGStab.cpp:73-437)
+        S = clg.CMultiShiftBiCGStab(ctx, DiviationStep=10, MaxStep=100)
+    infos = S.Solve(xs, cs, b, U, getattr(clg, op))
+    Uh = U.CopyDataOut()
+    o = oracle.Operator(name, lat.dims, Uh, kappa)
+    bh = b.to_numpy()
+    if method == "FOM":
+        xo, io = oracle.fom_ms(o, bh, cs, maxdim=30, restart=100, accuracy=1e-12 * np.linalg.norm(bh), absolute=True)
+    else:
+        xo, io = oracle.bicgstab_ms(o, bh, cs, dev_step=10, max_step=100, accuracy=1e-12)
     for k, c in enumerate(cs):
         assert infos[k]["status"] == 0
-        assert op.true_residual(b.to_numpy(), xs[k].to_numpy(), complex(c)) <= TOL
+        assert o.true_residual(bh, xs[k].to_numpy(), complex(c)) <= TOL
+        assert np.linalg.norm(xs[k].to_numpy() - xo[k]) <= 1e-8 * np.linalg.norm(xo[k])
+    # one Krylov space: fewer applications than the six separate solves of the
+    # nested form need together
+    N = clg.CMultiShiftNested(ctx, inner_precision=clg.SINGLE)
+    ys = [clg.CFieldFermionWilsonSquareSU3(lat, kappa) for _ in cs]
+    ninfo = N.Solve(ys, cs, b, U, getattr(clg, op))
+    for k, c in enumerate(cs):
+        assert ninfo[k]["status"] == 0
+        assert o.true_residual(bh, ys[k].to_numpy(), complex(c)) <= TOL
+    assert max(i["iterations"] for i in infos) < sum(i["iterations"] for i in ninfo)
 
 
 def test_rational_round_trip(ctx, clg, oracle):
