@@ -1,14 +1,18 @@
 #!/usr/bin/env python
 """Benchmark of the B200 fermion hot path.
 
-Metric: solves per second of the even-odd Wilson system to a true relative
-residual of 1e-10 (FP32 inner Krylov iterations inside FP64 defect correction),
-with the Dslash HBM bandwidth of the dominant kernel as the roofline.
+Metric: solves per second of the Wilson system D x = b to a true relative
+residual of 1e-10 (mixed precision: FP16 inner Krylov iterations inside FP64
+defect correction, even-odd, right-hand sides batched), with the Dslash HBM
+bandwidth of the dominant kernel as the roofline.
 
-Workload ``wilson_eo_32x32x32x16``: 32^3 x 16 lattice, links exp(i eps H) with a
-seeded traceless-Hermitian Gaussian H and eps = 0.25, kappa = 0.1355, fermion
-boundary (+,+,+,-), one complex Gaussian source per rank (synthetic data).
-A step is one solve of D x = b.  With N GPUs every rank solves its own source
+Default workload ``wilson_eo_batched_32x32x32x32`` (the batched multi-RHS
+configuration): 32^3 x 32 lattice, links exp(i eps H) with a seeded
+traceless-Hermitian Gaussian H and eps = 0.25, kappa = 0.1355, fermion boundary
+(+,+,+,-), 12 spin-colour point sources + 16 Z2 noise sources per rank, solved
+in one batched call (synthetic data).  A step is one batched solve of all 28
+right-hand sides.  ``wilson_eo_32x32x32x16`` (one complex Gaussian source on
+32^3 x 16) is measured beside it.  With N GPUs every rank solves its own batch
 (independent replicas, weak scaling; the path has no exchange step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -37,7 +41,7 @@ WORKLOADS = {
     "wilson_eo_batched_32x32x32x32": dict(dims=(32, 32, 32, 32), kappa=0.1355, eps=0.25, seed=0xC1A60003, nrhs=28,
                                           sources="point12_z2_16"),
 }
-DEFAULT_WORKLOAD = "wilson_eo_32x32x32x16"
+DEFAULT_WORKLOAD = "wilson_eo_batched_32x32x32x32"
 TOL = 1e-10
 SOLVER_NAMES = {"cg": "CGNE on the Schur system (CG on M_ee M_ee^+)", "gmres": "GMRES(12)"}
 
@@ -172,7 +176,15 @@ def hop_bytes_per_site(prec: int) -> int:
     return (48 + 4) * 2 + 8 * 12 * 2
 
 
-def time_hops(clg, ctx, lat, U, prec, stream, reps=60):
+def hop_bytes_launch(prec: int, nrhs: int) -> int:
+    """Compulsory HBM bytes of one hop launch over nrhs right-hand sides, per
+    output site: each right-hand side's input and output spinor, the eight
+    links once (all right-hand sides of the launch use the same links)."""
+    links = 8 * 12 * (2 if prec == 2 else 4) if prec else 8 * 18 * 8
+    return (hop_bytes_per_site(prec) - links) * nrhs + links
+
+
+def time_hops(clg, ctx, lat, U, prec, stream, reps=60, nrhs=1):
     """Average device duration of the checkerboard Wilson hop (odd -> even).
 
     The launches cycle over four input/output pairs so that the working set
@@ -184,10 +196,12 @@ def time_hops(clg, ctx, lat, U, prec, stream, reps=60):
 
     kappa = 0.1355
     fields = []
-    for i in range(4):
-        a = clg.CFieldFermionWilsonSquareSU3(lat, kappa, precision=prec)
-        a.InitialField(clg.SOURCE_GAUSS, 1234 + i, 2)
-        b = clg.CFieldFermionWilsonSquareSU3(lat, kappa, precision=prec)
+    npairs = 4 if nrhs == 1 else 2  # a batch of right-hand sides alone exceeds L2
+    for i in range(npairs):
+        a = clg.CFieldFermionWilsonSquareSU3(lat, kappa, precision=prec, nrhs=nrhs)
+        for r in range(nrhs):
+            a.InitialField(clg.SOURCE_GAUSS, 1234 + i, 2 + r, rhs=r)
+        b = clg.CFieldFermionWilsonSquareSU3(lat, kappa, precision=prec, nrhs=nrhs)
         fields.append((a, b))
     for a, b in fields:  # warm-up (also runs the block-size autotuner)
         a.apply_to(clg.OP_DEO, b, U)
@@ -196,7 +210,7 @@ def time_hops(clg, ctx, lat, U, prec, stream, reps=60):
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=stream):
         for r in range(reps):
-            a, b = fields[r % 4]
+            a, b = fields[r % npairs]
             a.apply_to(clg.OP_DEO, b, U)
     per_replay = ctx.kernel_count() - k0
     replays = 3
@@ -327,26 +341,54 @@ def ours(args, world, rank, local):
     b1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
     b1.from_numpy(src[nrhs - 1])
 
+    # ---------------- the headline solutions against the FP64 oracle: every
+    # right-hand side's true residual |b - D x| / |b| recomputed on the host
+    oracle_check = None
+    if rank == 0 and not args.no_cpu:
+        oracle_check = oracle_residuals(U, lat, kappa, b, x, nrhs)
+
     # ---------------- roofline of the dominant kernel (the checkerboard hop in
-    # the inner precision)
+    # the inner precision, over all right-hand sides of a step)
     peak, peak_kind = peaks()
     pname = {"single": "fp32", "half": "fp16"}[args.inner]
-    t_hop, hop_launches = time_hops(clg, ctx, lat, U, inner, stream)
-    hop_alg = hop_bytes_per_site(inner) * Vh
+    t_hop, hop_launches = time_hops(clg, ctx, lat, U, inner, stream, reps=60 if nrhs == 1 else 12, nrhs=nrhs)
+    hop_alg = hop_bytes_launch(inner, nrhs) * Vh
     achieved = hop_alg / t_hop / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "hop_traffic.json")
     if os.path.exists(tp):
         d = json.load(open(tp))
-        if tuple(d.get("dims", ())) == tuple(W["dims"]):
-            traffic = d.get(pname, {}).get("bytes_per_launch")
+        ent = d.get(pname + ("" if nrhs == 1 else f"_{nrhs}rhs"), {})
+        if tuple(ent.get("dims", d.get("dims", ()))) == tuple(W["dims"]):
+            traffic = ent.get("bytes_per_launch")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic,
-            "kernel": f"wilson_hop_kernel<{'P32' if inner == clg.SINGLE else 'P16'},12-real>",
-            "bytes_per_launch": hop_alg, "launch_us": round(t_hop * 1e6, 2), "peak_source": peak_kind}
+            "kernel": f"wilson_hop_kernel<{'P32' if inner == clg.SINGLE else 'P16'},12-real>, {nrhs} rhs per launch",
+            "bytes_per_launch": hop_alg, "launch_us": round(t_hop * 1e6, 2), "peak_source": peak_kind,
+            "bytes_model": ("one input and one output spinor per rhs and output site, the 8 links once per site "
+                            "for all rhs of the launch")}
+    if nrhs > 1:
+        # the same launch counted as nrhs separate one-rhs hops (links re-read per rhs)
+        roof["frac_links_per_rhs"] = round(hop_bytes_per_site(inner) * nrhs * Vh / t_hop / 1e9 / peak, 4)
 
     extra = {}
-    if rank == 0 and not args.quick:
+    if rank == 0 and not args.quick and nrhs > 1:
+        extra["denominators_32x32x32x32"] = denominators(clg, ctx, stream, lat, U, kappa, W, value)
+        extra["config2_32x32x32x16"] = config2_side(clg, ctx, stream, args)
+        if not args.no_batched:
+            extra["batched_uneven_lattices"] = uneven_lattices(clg, ctx, stream, args)
+        if not args.no_side:
+            extra["wilson_8x8x8x8"] = wilson_small(clg, ctx, stream)
+            extra["dslash_48x48x48x24"] = dslash_large(clg, ctx, stream)
+            extra["staggered_32x32x32x16"] = staggered_hops(clg, ctx, stream)
+            extra["staggered_multishift_32x32x32x16"] = staggered_multishift(clg, ctx, stream)
+            extra["wilson_force_32x32x32x16"] = wilson_force_side(clg, ctx, stream)
+            extra["staggered_force_32x32x32x16"] = ks_force_side(clg, ctx, stream)
+        extra["reference_cuda_build"] = reference_cuda_build()
+        if world == 1 and not args.no_cpu:
+            extra["cpu_baseline"] = cpu_baseline_bicgstab(
+                U, lat, kappa, extra["denominators_32x32x32x32"]["fp64_bicgstab"]["applications"])
+    elif rank == 0 and not args.quick:
         # Dslash bandwidth in each precision, FP64 plain solves, CPU baseline
         dsl = {}
         for name, prec in (("fp64", clg.DOUBLE), ("fp32", clg.SINGLE), ("fp16", clg.HALF)):
@@ -403,7 +445,8 @@ def ours(args, world, rank, local):
                    "tol_true_rel": TOL, "rhs_per_gpu": nrhs, "parallelism": f"replicas x{world}",
                    "l2": "working set (links and spinors of the solve) larger than the 126 MB L2"},
         "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": launches,
-        "iterations_per_solve": infos[0]["iterations"] if infos else None,
+        "iterations_per_solve": max(i["iterations"] for i in infos) if infos else None,
+        "oracle_check": oracle_check,
     }
     result.update(extra)
     if "cpu_baseline" not in result:
@@ -411,6 +454,197 @@ def ours(args, world, rank, local):
     if rank == 0:
         print(json.dumps(result))
     ctx.close()
+
+
+def oracle_residuals(U, lat, kappa, b, x, nrhs):
+    """|b - D x| / |b| of every right-hand side by the FP64 CPU oracle (the
+    checker; nothing of it is timed)."""
+    from oracle import oracle as O
+
+    op = O.Operator("WILSON_D", lat.dims, U.CopyDataOut(), kappa)
+    res = [op.true_residual(b.to_numpy(r), x.to_numpy(r)) for r in range(nrhs)]
+    return {"max_true_rel_residual": max(res), "rhs_checked": nrhs,
+            "checker": "FP64 CPU oracle D (the reference's Wilson kernel restated)"}
+
+
+def timed_solve(S, x, b, U, op, stream):
+    """One warm-up solve (tuning, workspace, graphs), then one timed on the device."""
+    import torch
+
+    S.Solve(x, b, U, op, raise_on_fail=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    infos = S.Solve(x, b, U, op, raise_on_fail=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, infos
+
+
+def denominators(clg, ctx, stream, lat, U, kappa, W, batched_value):
+    """The plain FP64 solvers on one source of the batched 32^3x32 problem (the
+    last Z2 noise source), to the same true residual 1e-10: CGNE on the Schur
+    system, BiCGStab (standard omega), and the reference's GMRES(12) with an
+    application budget (it stagnates on this operator: its final true residual
+    is recorded).  Every solution is checked by the FP64 oracle."""
+    from oracle import oracle as O
+
+    n = W["nrhs"]
+    b1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    b1.InitialField(clg.SOURCE_Z2, W["seed"], 2 + n - 1)
+    x1 = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    op = O.Operator("WILSON_D", lat.dims, U.CopyDataOut(), kappa)
+    bh = b1.to_numpy()
+    out = {"source": "Z2 noise (rhs 27 of the batch)"}
+    for label, cls, kw in (("fp64_cgne", clg.CSLASolverCG, {}),
+                           ("fp64_bicgstab", clg.CSLASolverBiCGStab, {"max_iterations": 60000}),
+                           ("fp64_gmres12", clg.CSLASolverGMRES, {"MaxDim": 12, "max_iterations": 6000, "max_outer": 4})):
+        S = cls(ctx, inner_precision=clg.DOUBLE, tol_true_rel=TOL, **kw)
+        if label == "fp64_gmres12":  # one budget-limited solve (not repeated)
+            import time as _t
+            t0 = _t.perf_counter()
+            inf = S.Solve(x1, b1, U, clg.EFO_F_D, raise_on_fail=False)[0]
+            dt = _t.perf_counter() - t0
+        else:
+            dt, infs = timed_solve(S, x1, b1, U, clg.EFO_F_D, stream)
+            inf = infs[0]
+        r = op.true_residual(bh, x1.to_numpy())
+        out[label] = {"solves_per_s": round(1.0 / dt, 4) if inf["status"] == 0 else 0.0, "seconds": round(dt, 4),
+                      "applications": inf["iterations"], "status": inf["status"],
+                      "oracle_true_rel_residual": r}
+        S.close()
+    out["ratio_batched_mixed_vs_fp64_cgne"] = round(batched_value / out["fp64_cgne"]["solves_per_s"], 2)
+    if out["fp64_bicgstab"]["solves_per_s"] > 0:
+        out["ratio_batched_mixed_vs_fp64_bicgstab"] = round(batched_value / out["fp64_bicgstab"]["solves_per_s"], 2)
+    out["fp64_gmres12_note"] = ("budget of 6000 applications; status 4 = not converged (restarted GMRES stagnates "
+                                "on this operator), its oracle true residual is the value reached")
+    b1.close()
+    x1.close()
+    return out
+
+
+def config2_side(clg, ctx, stream, args, steps=5):
+    """32^3x16 (exp(i 0.25 H) links, one complex Gaussian source): the
+    single-source solve of the metric's FP16-inner CGNE, the other solvers and
+    precisions, and the hop in each precision; every solution checked by the
+    FP64 oracle."""
+    import torch
+
+    from oracle import oracle as O
+
+    W = WORKLOADS["wilson_eo_32x32x32x16"]
+    lat = clg.Lattice(ctx, W["dims"])
+    Vh = lat.volume // 2
+    kappa = W["kappa"]
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, W["seed"], 1, W["eps"])
+    b = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    b.InitialField(clg.SOURCE_GAUSS, W["seed"], 2)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    op = O.Operator("WILSON_D", lat.dims, U.CopyDataOut(), kappa)
+    bh = b.to_numpy()
+    out = {"dims": list(W["dims"])}
+    S = clg.CSLASolverCG(ctx, inner_precision=clg.HALF, tol_true_rel=TOL)
+    S.Solve(x, b, U, clg.EFO_F_D)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        inf = S.Solve(x, b, U, clg.EFO_F_D)[0]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / steps
+    out["half_cgne_headline"] = {"solves_per_s": round(1.0 / t, 3), "ms_per_solve": round(t * 1e3, 3),
+                                 "applications": inf["iterations"], "outer": inf["outer"],
+                                 "oracle_true_rel_residual": op.true_residual(bh, x.to_numpy())}
+    S.close()
+    dsl = {}
+    peak, _ = peaks()
+    for name, prec in (("fp64", clg.DOUBLE), ("fp32", clg.SINGLE), ("fp16", clg.HALF)):
+        th, _ = time_hops(clg, ctx, lat, U, prec, stream, reps=40)
+        gbs = hop_bytes_per_site(prec) * Vh / th / 1e9
+        dsl[name] = {"GB/s": round(gbs, 1), "frac": round(gbs / peak, 4), "GFLOP/s": round(1320 * Vh / th / 1e9, 1),
+                     "launch_us": round(th * 1e6, 2)}
+    out["dslash_hop"] = dsl
+    plain = {}
+    for label, cls, prec in (("fp64_gmres12", clg.CSLASolverGMRES, clg.DOUBLE),
+                             ("fp64_bicgstab", clg.CSLASolverBiCGStab, clg.DOUBLE),
+                             ("fp64_cgne", clg.CSLASolverCG, clg.DOUBLE),
+                             ("mixed_gmres12", clg.CSLASolverGMRES, clg.SINGLE),
+                             ("half_gmres12", clg.CSLASolverGMRES, clg.HALF),
+                             ("mixed_cgne", clg.CSLASolverCG, clg.SINGLE)):
+        s = cls(ctx, inner_precision=prec, tol_true_rel=TOL, MaxDim=12, max_iterations=60000, max_outer=20)
+        dt, infs = timed_solve(s, x, b, U, clg.EFO_F_D, stream)
+        i0 = infs[0]
+        plain[label] = {"solves_per_s": round(1.0 / dt, 3), "seconds": round(dt, 4), "applications": i0["iterations"],
+                        "outer": i0["outer"], "status": i0["status"],
+                        "oracle_true_rel_residual": op.true_residual(bh, x.to_numpy())}
+        s.close()
+    out["solves"] = plain
+    b.close()
+    x.close()
+    U.close()
+    return out
+
+
+def staggered_hops(clg, ctx, stream, reps=40):
+    """Staggered checkerboard hop on 32^3x16 (exp(i 0.25 H) links, seed
+    0xC1A60004) in FP64 (18-real links), FP32 and FP16 (12-real links):
+    compulsory bytes per output site (one input and one output colour vector,
+    eight links), 570 flops per site."""
+    import torch
+
+    peak, _ = peaks()
+    lat = clg.Lattice(ctx, (32, 32, 32, 16))
+    Vh = lat.volume // 2
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60004, 1, 0.25)
+    bytes_site = {clg.DOUBLE: (6 + 6 + 8 * 18) * 8, clg.SINGLE: (6 + 6 + 8 * 12) * 4, clg.HALF: 2 * (12 + 4) + 8 * 24}
+    out = {"dims": [32, 32, 32, 16]}
+    for name, prec in (("fp64", clg.DOUBLE), ("fp32", clg.SINGLE), ("fp16", clg.HALF)):
+        fields = []
+        for i in range(4):
+            a = clg.CFieldFermionKSSU3(lat, 0.02, precision=prec)
+            a.InitialField(clg.SOURCE_GAUSS, 77 + i, 2)
+            c = clg.CFieldFermionKSSU3(lat, 0.02, precision=prec)
+            fields.append((a, c))
+        for a, c in fields:
+            a.apply_to(clg.OP_DEO, c, U)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            for r in range(reps):
+                a, c = fields[r % 4]
+                a.apply_to(clg.OP_DEO, c, U)
+        with torch.cuda.stream(stream):
+            g.replay()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(3):
+                g.replay()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / (3 * reps)
+        del g
+        gbs = bytes_site[prec] * Vh / t / 1e9
+        out[name] = {"GB/s": round(gbs, 1), "frac": round(gbs / peak, 4), "GFLOP/s": round(570 * Vh / t / 1e9, 1),
+                     "launch_us": round(t * 1e6, 2), "bytes_per_site": bytes_site[prec]}
+        for a, c in fields:
+            a.close()
+            c.close()
+    U.close()
+    return out
+
+
+def reference_cuda_build():
+    """The reference's own CUDA build (CLGLib FP64, sm_100a) timed on a B200 by
+    tests/golden/make_ref_golden.py --timing; read from the committed record."""
+    p = os.path.join(ROOT, "profiles", "reference_cuda_build_32x32x32x16.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    d["source"] = "recorded by tests/golden/make_ref_golden.py --timing on a B200 (not re-run by bench.py)"
+    return d
 
 
 def batched_sources(clg, ctx, stream, args, steps=2):
@@ -515,10 +749,14 @@ def wilson_small(clg, ctx, stream):
 
 def uneven_lattices(clg, ctx, stream, args, steps=2):
     """The uneven set 8^4, 12^4, 16^4, 16^3x32,
-    24^3x16 (442,624 sites), 4 complex Gaussian sources each.  Each lattice's
-    sources are one batched call (CGNE in the `--inner` precision, FP64 defect
-    correction); the five calls are issued back to back on the context stream.
-    Unit: one source solved to the true relative residual 1e-10."""
+    24^3x16 (442,624 sites), 4 complex Gaussian sources each, every lattice with
+    its own gauge field.  All 20 sources are one solve (clg_solve_lattices: CGNE
+    in the `--inner` precision, FP64 defect correction; one kernel per step
+    covers every lattice); beside it, the five lattices as five batched calls
+    back to back.  Unit: one source solved to the true relative residual 1e-10,
+    every solution checked by the FP64 oracle."""
+    from oracle import oracle as O
+
     import torch
 
     dims_set = [(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (16, 16, 16, 32), (24, 24, 24, 16)]
@@ -546,11 +784,34 @@ def uneven_lattices(clg, ctx, stream, args, steps=2):
             infos += s.Solve(x, b, U, clg.EFO_F_D)
     e1.record(stream)
     torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1) / 1e3 / steps
+    # all lattices in one solve
+    S = clg.CSLASolverCG(ctx, inner_precision=inner, tol_true_rel=TOL)
+    xs = [clg.CFieldFermionWilsonSquareSU3(j[0], kappa, nrhs=n) for j in jobs]
+    S.SolveLattices(xs, [j[2] for j in jobs], [j[1] for j in jobs], clg.EFO_F_D)  # warm-up
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        binfo = S.SolveLattices(xs, [j[2] for j in jobs], [j[1] for j in jobs], clg.EFO_F_D)
+    e1.record(stream)
+    torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1e3 / steps
+    worst_oracle = 0.0
+    for (lat, U, b, x, s), xb in zip(jobs, xs):
+        op = O.Operator("WILSON_D", lat.dims, U.CopyDataOut(), kappa)
+        for r in range(n):
+            worst_oracle = max(worst_oracle, op.true_residual(b.to_numpy(r), xb.to_numpy(r)))
     out = {"lattices": [list(d) for d in dims_set], "sites": sum(int(np.prod(d)) for d in dims_set),
-           "rhs_per_lattice": n, "solves_per_s": round(len(infos) / t, 3), "ms_per_set": round(t * 1e3, 2),
-           "worst_true_rel_residual": max(i["true_rel_residual"] for i in infos),
-           "max_applications": max(i["iterations"] for i in infos)}
+           "rhs_per_lattice": n, "solver": "one clg_solve_lattices call (all lattices in every launch)",
+           "solves_per_s": round(len(binfo) / t, 3), "ms_per_set": round(t * 1e3, 2),
+           "worst_true_rel_residual": max(i["true_rel_residual"] for i in binfo),
+           "oracle_worst_true_rel_residual": worst_oracle,
+           "max_applications": max(i["iterations"] for i in binfo),
+           "five_calls": {"solves_per_s": round(len(infos) / t_seq, 3), "ms_per_set": round(t_seq * 1e3, 2),
+                          "max_applications": max(i["iterations"] for i in infos)}}
+    S.close()
+    for xb in xs:
+        xb.close()
     for lat, U, b, x, s in jobs:
         for f in (b, x):
             f.close()
@@ -575,6 +836,32 @@ def dslash_large(clg, ctx, stream):
         gbs = hop_bytes_per_site(prec) * Vh / t / 1e9
         out[name] = {"GB/s": round(gbs, 1), "frac": round(gbs / peak, 4), "GFLOP/s": round(1320 * Vh / t / 1e9, 1),
                      "launch_us": round(t * 1e6, 2)}
+    # the solve in each inner precision (CGNE, FP64 defect correction), with the
+    # error of each solution against the FP64 oracle: the oracle's true residual
+    # and the distance to the FP64 solution
+    from oracle import oracle as O
+
+    kappa = 0.1355
+    b = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    b.InitialField(clg.SOURCE_GAUSS, 0xC1A60002, 2)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    op = O.Operator("WILSON_D", lat.dims, U.CopyDataOut(), kappa)
+    bh = b.to_numpy()
+    sols = {}
+    solves = {}
+    for name, prec in (("fp64", clg.DOUBLE), ("fp32", clg.SINGLE), ("fp16", clg.HALF)):
+        S = clg.CSLASolverCG(ctx, inner_precision=prec, tol_true_rel=TOL)
+        dt, infs = timed_solve(S, x, b, U, clg.EFO_F_D, stream)
+        sols[name] = x.to_numpy()
+        solves[name] = {"solves_per_s": round(1.0 / dt, 3), "applications": infs[0]["iterations"],
+                        "outer": infs[0]["outer"], "oracle_true_rel_residual": op.true_residual(bh, sols[name])}
+        S.close()
+    for name in ("fp32", "fp16"):
+        solves[name]["rel_error_vs_fp64_solution"] = float(np.linalg.norm(sols[name] - sols["fp64"]) /
+                                                           np.linalg.norm(sols["fp64"]))
+    out["solves_cgne"] = solves
+    b.close()
+    x.close()
     U.close()
     return out
 
@@ -778,6 +1065,37 @@ def cpu_baseline(U, lat, kappa, fp64_applications):
                       f"solves/s = 1/(t_apply x {fp64_applications} applications of the FP64 GMRES(12) solve)"}
 
 
+def bicgstab_iteration_time(L, kappa, seed, eps, iters):
+    """Seconds per iteration of the oracle's FP64 BiCGStab (the reference's
+    CSLASolverBiCGStab restated, with the residual-minimising omega) on the
+    even-odd Wilson system M_ee of lattice L, timed over `iters` iterations on
+    the host cores (OpenMP)."""
+    from oracle import oracle as O
+
+    V = int(np.prod(L))
+    U = O.gauge_expH(L, seed, eps)
+    b = O.gauss(V, 12, seed, 2).reshape(V, 4, 3)
+    b[O.parity_mask(L) == 1] = 0
+    op = O.Operator("WILSON_MEE", L, U, kappa)
+    O.bicgstab(op, b, dev_step=1, max_step=1, restart=1, accuracy=0.0, std_omega=True)  # warm-up
+    t0 = time.perf_counter()
+    _, info = O.bicgstab(op, b, dev_step=iters, max_step=1, restart=1, accuracy=0.0, std_omega=True)
+    return (time.perf_counter() - t0) / iters
+
+
+def cpu_baseline_bicgstab(U, lat, kappa, fp64_applications, iters=3):
+    """Oracle FP64 BiCGStab on the host cores for the batched 32^3x32 problem:
+    solves/s = 1 / (t_iteration x iterations of this run's FP64 BiCGStab solve)."""
+    W = WORKLOADS["wilson_eo_batched_32x32x32x32"]
+    t_it = bicgstab_iteration_time(W["dims"], kappa, W["seed"], W["eps"], iters)
+    n_it = max(fp64_applications // 2, 1)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": round(1.0 / (t_it * n_it), 8), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{iters} iterations of the oracle's FP64 even-odd BiCGStab on {tuple(W['dims'])} "
+                      f"({t_it:.3f} s each, 2 M_ee applications per iteration); solves/s = 1/(t_iteration x "
+                      f"{n_it} iterations of this run's FP64 BiCGStab solve)"}
+
+
 # ------------------------------------------------------------------ reference arm
 def reference(args, world, rank):
     """The reference algorithm on the host cores: the oracle's restatement of
@@ -792,6 +1110,34 @@ def reference(args, world, rank):
     W = WORKLOADS[args.workload]
     L, kappa = W["dims"], W["kappa"]
     V = int(np.prod(L))
+    cp = os.path.join(ROOT, "oracle", "reference_cycles.json")
+    counts = json.load(open(cp)) if os.path.exists(cp) else {}
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if W["nrhs"] > 1:
+        # batched 32^3x32: the reference's GMRES(12) stagnates on this operator
+        # and its BiCGStab with the conjugated omega diverges, so the reference
+        # algorithm timed is CSLASolverBiCGStab with the residual-minimising
+        # omega (the oracle's std_omega), FP64, even-odd, one right-hand side at
+        # a time as the reference solves sources; a step is one iteration
+        apps = counts.get(args.workload, {}).get("bicgstab_applications")
+        t_it = bicgstab_iteration_time(L, kappa, W["seed"], W["eps"], max(args.steps, 1))
+        value = 1.0 / (t_it * apps / 2) if apps else None
+        sample = (f"{args.steps} FP64 even-odd BiCGStab iterations of the C/OpenMP oracle on {tuple(L)} "
+                  f"({t_it:.3f} s each); {apps} applications per solve (oracle/reference_cycles.json)")
+        out = {"metric": METRIC, "value": round(value, 8) if value else None, "unit": UNIT, "impl": "reference",
+               "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex)", "data": "synthetic",
+               "ms_per_step": round(t_it * 1e3, 3),
+               "config": {"workload": args.workload, "dims": list(L), "kappa": kappa,
+                          "links": f"exp(i eps H), eps={W['eps']}",
+                          "solver": "BiCGStab even-odd FP64 (reference algorithm, residual-minimising omega, CPU), "
+                                    "one source at a time"},
+               "cpu_baseline": {"value": round(value, 8) if value else None, "unit": UNIT, "cores": cores,
+                                "kind": "port", "sample": sample},
+               "e2e": {"value": round(value, 8) if value else None, "unit": UNIT, "h2d_bytes_per_step": 0,
+                       "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return
     U = O.gauge_expH(L, W["seed"], W["eps"])
     b = O.gauss(V, 12, W["seed"], 2).reshape(V, 4, 3)
     pm = O.parity_mask(L)
@@ -807,12 +1153,7 @@ def reference(args, world, rank):
     for _ in range(args.steps):
         x, _ = O.gmres(op, bt, x0=x, maxdim=12, restart=1, accuracy=0.0)
     t_cycle = (time.perf_counter() - t0) / args.steps
-    counts = {}
-    cp = os.path.join(ROOT, "oracle", "reference_cycles.json")
-    if os.path.exists(cp):
-        counts = json.load(open(cp))
     cycles = counts.get(args.workload, {}).get("cycles")
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     if cycles:
         value = 1.0 / (t_cycle * cycles)
         how = f"{cycles} GMRES(12) cycles per solve (oracle/reference_cycles.json)"
@@ -849,9 +1190,11 @@ def profile_driver(args):
     U.InitialField(clg.GAUGE_EXPH, W["seed"], 1, W["eps"])
     if args.profile.startswith("hop"):
         prec = {"hop-double": clg.DOUBLE, "hop-single": clg.SINGLE, "hop-half": clg.HALF}[args.profile]
-        a = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], precision=prec)
-        a.InitialField(clg.SOURCE_GAUSS, 5, 2)
-        o = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], precision=prec)
+        n = W["nrhs"]  # the workload's right-hand sides in every launch
+        a = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], precision=prec, nrhs=n)
+        for r in range(n):
+            a.InitialField(clg.SOURCE_GAUSS, 5, 2 + r, rhs=r)
+        o = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], precision=prec, nrhs=n)
         for _ in range(args.steps):
             a.apply_to(clg.OP_DEO, o, U)
     elif args.profile == "force":

@@ -40,7 +40,7 @@ GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
  FILE_BRIDGEPP_TXT) = range(6)
 SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT, SOURCE_Z4 = 0, 1, 2, 3, 4
 (SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS, SOLVER_GCRODR, SOLVER_NESTED_MS,
- SOLVER_BICGSTAB_MS) = 0, 1, 2, 3, 4, 5, 6, 7
+ SOLVER_BICGSTAB_MS, SOLVER_GMRESMDR) = 0, 1, 2, 3, 4, 5, 6, 7, 8
 EEDT_SVD, EEDT_REV, EEDT_HEV = 0, 1, 2  # GCRO-DR deflation spaces (EEigenDeflationType)
 
 
@@ -553,6 +553,12 @@ class CSLASolverGCRODR(_Solver):
     def Reset(self):
         """Drop the recycled subspace (the start of a new trajectory)."""
         self.ctx.check(self.ctx.lib.clg_solver_reset(self.h), "clg_solver_reset")
+
+
+class CSLASolverGMRESMDR(CSLASolverGCRODR):
+    """GMRES-MDR (CSolverGMRESMDR.cpp:16-170): GCRO-DR whose solves from a kept
+    U_k start by rotating it to the deflation problem's eigenvectors."""
+    KIND = SOLVER_GMRESMDR
 
 
 # EGammaMatrix (clg_gamma)

@@ -10,8 +10,9 @@
 // structure-of-arrays layout with the chunk stride of the largest checkerboard
 // of the set; the sites past a lattice's own checkerboard are padding that
 // stays zero.  The hop kernels take the lattice of each right-hand side from a
-// device table (HopSeg: geometry and link arrays per right-hand side), the
-// vector kernels run over the padded range unchanged.  So one iteration of the
+// device table (HopSeg: geometry and link arrays per right-hand side), and the
+// vector kernels skip the padding (site_reduce_batch_kernel with the per-rhs
+// checkerboard sizes; the padding is zero either way).  So one iteration of the
 // inner Krylov method is the same fixed number of launches whatever the number
 // of lattices, and it is captured and replayed as a CUDA graph like any other
 // solve.
@@ -32,6 +33,7 @@ struct BatchWork : SolveCacheBase {
   clg_lattice_s vlat;        // the padded batch lattice
   clg_gauge_s vgauge;        // its "gauge field": the per-rhs HopSeg table
   HopSeg* seg_dev = nullptr;
+  int64_t* vh_dev = nullptr;  // per-rhs checkerboard sizes
   void* b_data = nullptr;
   void* x_data = nullptr;
   FieldRef B, X;             // FP64 full fields, padded
@@ -40,6 +42,7 @@ struct BatchWork : SolveCacheBase {
     if (ctx) cudaStreamSynchronize(ctx->stream);
     solve_cache.reset();
     dfree(seg_dev);
+    dfree(vh_dev);
     dfree(b_data);
     dfree(x_data);
   }
@@ -119,6 +122,7 @@ extern "C" clg_status clg_solve_lattices(clg_solver S, int n, clg_field* x, clg_
     nw->vgauge.su3 = true;
     nw->vgauge.dirty_lowp = false;
     std::vector<HopSeg> segs;
+    std::vector<int64_t> vhs;
     for (int i = 0; i < n; ++i)
       for (int r = 0; r < b[i]->nrhs; ++r) {
         HopSeg sg;
@@ -129,15 +133,19 @@ extern "C" clg_status clg_solve_lattices(clg_solver S, int n, clg_field* x, clg_
           sg.u[2][p] = U[i]->u16[p];
         }
         segs.push_back(sg);
+        vhs.push_back(b[i]->lat->g.Vh);
       }
     const size_t fbytes = (size_t)vh_max * nc * 16 * 2 * total;
     clg_status st;
     if ((st = dalloc(ctx, (void**)&nw->seg_dev, sizeof(HopSeg) * segs.size())) ||
+        (st = dalloc(ctx, (void**)&nw->vh_dev, sizeof(int64_t) * vhs.size())) ||
         (st = dalloc(ctx, &nw->b_data, fbytes)) || (st = dalloc(ctx, &nw->x_data, fbytes)))
       return st;
     cudaMemsetAsync(nw->b_data, 0, fbytes, ctx->stream);
     cudaMemsetAsync(nw->x_data, 0, fbytes, ctx->stream);
     if (cudaMemcpyAsync(nw->seg_dev, segs.data(), sizeof(HopSeg) * segs.size(), cudaMemcpyHostToDevice, ctx->stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(nw->vh_dev, vhs.data(), sizeof(int64_t) * vhs.size(), cudaMemcpyHostToDevice, ctx->stream) !=
             cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess)
       return ctx->fail(CLG_ERR_CUDA, "solve_lattices: table upload");
@@ -169,7 +177,14 @@ extern "C" clg_status clg_solve_lattices(clg_solver S, int n, clg_field* x, clg_
   q.b = W->B;
   q.xout.push_back(W->X);
   q.info = info;
+  // the solve's site kernels skip each right-hand side's padding
+  ctx->batch_vh = W->vh_dev;
+  ctx->batch_vh_stride = vh_max;
+  ctx->batch_nrhs = total;
   const clg_status s = solve_core(q);
+  ctx->batch_vh = nullptr;
+  ctx->batch_vh_stride = 0;
+  ctx->batch_nrhs = 0;
   if (s && s != CLG_ERR_NOT_CONVERGED && s != CLG_ERR_BREAKDOWN) return s;
   off = 0;
   for (int i = 0; i < n; ++i) {

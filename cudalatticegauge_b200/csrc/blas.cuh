@@ -37,6 +37,31 @@ __global__ void __launch_bounds__(256)
     grid_reduce_finalize<NRED>(acc, f, rhs, blockIdx.x, gridDim.x, (int)gridDim.y, partials, counter);
 }
 
+// The same over a batch of lattices (clg_solve_lattices): right-hand side r
+// holds rhs_vh[r] sites per checkerboard, the rest of the padded range is
+// skipped (it stays zero).
+template <int NRED, class F>
+__global__ void __launch_bounds__(256)
+    site_reduce_batch_kernel(F f, int64_t nsites, int first_parity, int64_t Vh, double* partials, unsigned* counter,
+                             const int64_t* rhs_vh) {
+  const int rhs = blockIdx.y;
+  pdl_launch_dependents();
+  pdl_wait();
+  double acc[NRED > 0 ? NRED : 1];
+#pragma unroll
+  for (int k = 0; k < (NRED > 0 ? NRED : 1); ++k) acc[k] = 0.0;
+  if (f.active(rhs)) {
+    const int64_t vr = rhs_vh[rhs];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nsites; i += (int64_t)gridDim.x * blockDim.x) {
+      const int pi = (int)(i / Vh);
+      const int64_t h = i - (int64_t)pi * Vh;
+      if (h < vr) f(rhs, first_parity + pi, h, acc);
+    }
+  }
+  if constexpr (NRED > 0)
+    grid_reduce_finalize<NRED>(acc, f, rhs, blockIdx.x, gridDim.x, (int)gridDim.y, partials, counter);
+}
+
 // Launch F over the checkerboards [first_parity, first_parity + nparity) of all nrhs.
 template <int NRED, class F>
 clg_status launch_sites(clg_context_s* ctx, const F& f, int first_parity, int nparity, int64_t Vh, int nrhs) {
@@ -54,8 +79,13 @@ clg_status launch_sites(clg_context_s* ctx, const F& f, int first_parity, int np
     if (st) return st;
   }
   dim3 grid((unsigned)nb, (unsigned)nrhs);
-  cudaError_t e = launch_pdl(ctx, site_reduce_kernel<NRED, F>, grid, dim3(bs), 0, f, nsites, first_parity, Vh,
-                             ctx->red_partials, ctx->red_counter);
+  cudaError_t e;
+  if (ctx->batch_vh && Vh == ctx->batch_vh_stride && nrhs == ctx->batch_nrhs)
+    e = launch_pdl(ctx, site_reduce_batch_kernel<NRED, F>, grid, dim3(bs), 0, f, nsites, first_parity, Vh,
+                   ctx->red_partials, ctx->red_counter, (const int64_t*)ctx->batch_vh);
+  else
+    e = launch_pdl(ctx, site_reduce_kernel<NRED, F>, grid, dim3(bs), 0, f, nsites, first_parity, Vh,
+                   ctx->red_partials, ctx->red_counter);
   if (e != cudaSuccess) return ctx->fail(cuda_status(e), std::string("site kernel: ") + cudaGetErrorString(e));
   return CLG_SUCCESS;
 }

@@ -297,17 +297,22 @@ __device__ __forceinline__ void wilson_hop_store(const HopArgs& a, int rhs, int6
 // The whole stencil for output site (rhs, h): acc = [scale *] (a H in + xa x),
 // on the lattice g with links U_here (parity out_parity) and U_there.  The
 // spinors' chunk stride is a.g.Vh (equal to g.Vh except in a batch of lattices).
-template <int P, int RECON, bool DAGGER, typename AT>
+template <int P, int RECON, bool DAGGER, bool SEG, typename AT>
 __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom& g, const void* U_here,
                                                    const void* U_there, int rhs, int64_t h, cpx<AT> acc[12]) {
   const int64_t Vh = a.g.Vh;
-  const int64_t lVh = g.Vh;
+  const int64_t lVh = SEG ? g.Vh : Vh;  // the links' stride: the lattice's own checkerboard
+  const void* const Uh = SEG ? U_here : a.U_here;
+  const void* const Ut = SEG ? U_there : a.U_there;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
   const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
 
   NbrInfo nb;
   int c[4];
-  neighbours(g, a.out_parity, h, nb, c);
+  if constexpr (SEG)
+    neighbours(g, a.out_parity, h, nb, c);
+  else
+    neighbours(a.g, a.out_parity, h, nb, c);
 
 #pragma unroll
   for (int k = 0; k < 12; ++k) acc[k] = mk<AT>(0, 0);
@@ -327,9 +332,9 @@ __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom&
     Packed16 pf, pb;                                                                    \
     PackedLink16 lf, lb;                                                                \
     load_packed16(in, in_norm, Vh, nb.hf[MU], pf);                                      \
-    load_packed_link16(U_here, MU, lVh, h, lf);                                         \
+    load_packed_link16(Uh, MU, lVh, h, lf);                                             \
     load_packed16(in, in_norm, Vh, nb.hb[MU], pb);                                      \
-    load_packed_link16(U_there, MU, lVh, nb.hb[MU], lb);                                \
+    load_packed_link16(Ut, MU, lVh, nb.hb[MU], lb);                                     \
     wilson_hop_dir16<MU, SF, false>(acc, pf, lf, nb.sf[MU] * pf.n);                     \
     wilson_hop_dir16<MU, SB, true>(acc, pb, lb, nb.sb[MU] * pb.n);                      \
   }
@@ -343,10 +348,10 @@ __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom&
   {                                                                                     \
     cpx<AT> psi[12], u[9];                                                              \
     load_site<P, 12, AT>(in, in_norm, Vh, nb.hf[MU], psi);                              \
-    load_link<P, RECON, AT>(U_here, MU, lVh, h, u);                                     \
+    load_link<P, RECON, AT>(Uh, MU, lVh, h, u);                                         \
     wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (AT)nb.sf[MU]);                      \
     load_site<P, 12, AT>(in, in_norm, Vh, nb.hb[MU], psi);                              \
-    load_link<P, RECON, AT>(U_there, MU, lVh, nb.hb[MU], u);                            \
+    load_link<P, RECON, AT>(Ut, MU, lVh, nb.hb[MU], u);                                 \
     wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (AT)nb.sb[MU]);                       \
   }
     CLG_WILSON_DIR(0)
@@ -360,7 +365,7 @@ __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom&
 
 template <int P, int RECON, bool DAGGER, typename AT>
 __device__ __forceinline__ void wilson_hop_site(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
-  wilson_hop_site_on<P, RECON, DAGGER>(a, a.g, a.U_here, a.U_there, rhs, h, acc);
+  wilson_hop_site_on<P, RECON, DAGGER, false>(a, a.g, a.U_here, a.U_there, rhs, h, acc);
 }
 
 // The precision index of the batch link table (HopSeg::u)
@@ -372,7 +377,7 @@ template <int P, int RECON, bool DAGGER, typename AT>
 __device__ __forceinline__ bool wilson_hop_site_batch(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[12]) {
   const HopSeg& sg = a.seg[rhs];
   if (h >= sg.g.Vh) return false;
-  wilson_hop_site_on<P, RECON, DAGGER>(a, sg.g, sg.u[seg_prec<P>()][a.out_parity], sg.u[seg_prec<P>()][1 - a.out_parity],
+  wilson_hop_site_on<P, RECON, DAGGER, true>(a, sg.g, sg.u[seg_prec<P>()][a.out_parity], sg.u[seg_prec<P>()][1 - a.out_parity],
                                        rhs, h, acc);
   return true;
 }

@@ -94,6 +94,7 @@ clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_g
   if (clg_status st = gauge_prepare(Ug, CLG_PREC_DOUBLE)) return st;
   const int m = S->p.max_dim, k = S->p.kdim > 0 ? S->p.kdim : S->p.max_dim - 2;
   const int defl = S->p.deflation;
+  const bool mdr = S->p.kind == CLG_SOLVER_GMRESMDR;
 
   // workspace (and the recycled U_k) for this lattice / operator / sizes
   auto* Wp = dynamic_cast<GcroWork*>(S->cache_gcro.get());
@@ -182,10 +183,68 @@ clg_status gcrodr_solve(::clg_solver_s* S, clg_field_s* X, clg_field_s* B, clg_g
     return s;
   };
 
+  bool c_ready = false;  // C = A U already (the GMRES-MDR start)
+  if (W.u_valid && mdr) {
+    // GMRES-MDR's start (CSLASolverGMRESMDR::GenerateCUFirstTime,
+    // CSolverGMRESMDR.cpp:16-135): Q R = U (QRFactorizationOfUk, :140-170),
+    // C = A Q, the k x k problem of the deflation type on span Q (REV: Q^+ A Q;
+    // HEV: Q^+ A^+ A Q p = l Q^+ A^+ Q p; SVD: Q^+ A^+ A Q), U = Q P.  The
+    // reference leaves C = A Q there, which breaks A U = C for the cycles that
+    // follow; here C = A Q P (no extra application) and the QR below makes it
+    // orthonormal with U rescaled to match, as the recycled start requires.
+    for (int i = 0; i < k && W.u_valid; ++i) {
+      std::vector<const FieldRef*> prev;
+      for (int j = 0; j < i; ++j) prev.push_back(&W.U[j]);
+      std::vector<Z> h;
+      if (i && (st = g.orthogonalise(W.U[i], prev, h))) return finish(st);
+      const double n = g.norm(W.U[i]);
+      if (!(n > 0)) W.u_valid = false;
+      else if ((st = g.scale(W.U[i], Z(1.0 / n, 0.0)))) return finish(st);
+    }
+    if (W.u_valid) {
+      for (int i = 0; i < k; ++i)
+        if ((st = g.apply(W.C[i], W.U[i]))) return finish(st);
+      Mat M(k, k), B(k, k);
+      for (int j = 0; j < k; ++j) {
+        std::vector<const FieldRef*> vs;
+        for (int i = 0; i < k; ++i) vs.push_back(defl == CLG_DEFLATION_REV ? &W.U[i] : &W.C[i]);
+        std::vector<Z> d;
+        if ((st = g.dots(W.C[j], vs, d))) return finish(st);  // d[i] = <v_i, C_j>
+        for (int i = 0; i < k; ++i) M(i, j) = d[i];
+        if (defl == CLG_DEFLATION_HEV) {
+          std::vector<Z> e;
+          std::vector<const FieldRef*> cs;
+          for (int i = 0; i < k; ++i) cs.push_back(&W.C[i]);
+          if ((st = g.dots(W.U[j], cs, e))) return finish(st);  // <C_i, Q_j>
+          for (int i = 0; i < k; ++i) B(i, j) = e[i];
+        }
+      }
+      std::vector<Z> ev;
+      Mat P;
+      const bool ok = defl == CLG_DEFLATION_HEV ? dense::geig(M, B, ev, P) : dense::eig(M, ev, P);
+      if (ok) {
+        // U = Q P, C = (A Q) P through the Tu / Tc scratch vectors
+        for (int j = 0; j < k; ++j) {
+          std::vector<const FieldRef*> qs, cs;
+          std::vector<Z> c;
+          for (int i = 0; i < k; ++i) {
+            qs.push_back(&W.U[i]);
+            cs.push_back(&W.C[i]);
+            c.push_back(P(i, j));
+          }
+          if ((st = g.lincomb(W.Tu[j], Z(0.0, 0.0), qs, c)) || (st = g.lincomb(W.Tc[j], Z(0.0, 0.0), cs, c)))
+            return finish(st);
+        }
+        for (int j = 0; j < k; ++j)
+          if ((st = g.copy(W.U[j], W.Tu[j])) || (st = g.copy(W.C[j], W.Tc[j]))) return finish(st);
+      }
+      c_ready = true;
+    }
+  }
   if (W.u_valid) {
     // C = A U, QR, U = U R^-1 (GenerateCUFirstTime / QRFactorAY, CSolverGCRODR.cpp:501-539, 817-841)
     Mat R(k, k);
-    for (int i = 0; i < k; ++i)
+    for (int i = 0; i < k && !c_ready; ++i)
       if ((st = g.apply(W.C[i], W.U[i]))) return finish(st);
     for (int i = 0; i < k; ++i) {
       std::vector<const FieldRef*> prev;

@@ -100,6 +100,12 @@ struct clg_context_s {
   // with the right-hand sides interleaved over the blocks (13.6 against 13.4 us
   // per rhs at 8 rhs, 27.2 against 27.5 at 28), whose links are shared through L2
   bool hop_pair = false;
+  // set by clg_solve_lattices for the duration of its solve: the per-rhs
+  // checkerboard sizes (device) of the padded batch, whose site kernels skip
+  // the padding (launches with this stride and right-hand-side count)
+  const int64_t* batch_vh = nullptr;
+  int64_t batch_vh_stride = 0;
+  int batch_nrhs = 0;
   int hop_pair_config = -1;
   // hops and site kernels are launched with programmatic stream serialization
   // (they overlap the previous kernel's drain); CLG_PDL=0 launches them plainly

@@ -88,7 +88,8 @@ typedef enum {
     CLG_SOLVER_FOM_MS = 4,      /* CMultiShiftFOM     SparseLinearAlgebra/CMultiShiftFOM.cpp:97-270   */
     CLG_SOLVER_GCRODR = 5,      /* CSLASolverGCRODR   SparseLinearAlgebra/CSolverGCRODR.cpp:196-911   */
     CLG_SOLVER_NESTED_MS = 6,   /* CMultiShiftNested  SparseLinearAlgebra/CMultiShiftNested.cpp:69-145 */
-    CLG_SOLVER_BICGSTAB_MS = 7  /* CMultiShiftBiCGStab SparseLinearAlgebra/CMultiShiftBiCGStab.cpp:73-437 */
+    CLG_SOLVER_BICGSTAB_MS = 7, /* CMultiShiftBiCGStab SparseLinearAlgebra/CMultiShiftBiCGStab.cpp:73-437 */
+    CLG_SOLVER_GMRESMDR = 8     /* CSLASolverGMRESMDR SparseLinearAlgebra/CSolverGMRESMDR.cpp:16-170  */
 } clg_solver_kind;
 
 /* GCRO-DR deflation space (EEigenDeflationType, CSolverGCRODR.cpp:541-760):
@@ -272,7 +273,11 @@ clg_status clg_solver_reset(clg_solver s);
  * right-hand side reached tol_true_rel.
  * GCRO-DR (CLG_SOLVER_GCRODR): FP64 fields, one right-hand side, max_dim = MDim
  * (5..32), kdim = KDim (2..MDim-2), deflation = DeflateSpace, restart = cycles, x0 = b when no start
- * vector is given (CSolverGCRODR.cpp:216-223); inner_precision is not used. */
+ * vector is given (CSolverGCRODR.cpp:216-223); inner_precision is not used.
+ * GMRES-MDR (CLG_SOLVER_GMRESMDR): the same parameters and cycles; a solve that
+ * starts from a kept U_k first rotates it to the eigenvectors of the deflation
+ * type's k x k problem on span U_k (GenerateCUFirstTime, CSolverGMRESMDR.cpp:16-135),
+ * with C_k = A U_k made orthonormal again (the reference leaves C_k = A Q). */
 clg_status clg_solve(clg_solver s, clg_field x, clg_field b, clg_gauge g, int op, clg_field x0, clg_solve_info* info);
 /* CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47):
  * (op + c_n) x_n = b for n < nshift; shifts_re_im holds nshift complex shifts

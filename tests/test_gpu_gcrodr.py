@@ -122,3 +122,37 @@ def test_gcrodr_rejects_bad_arguments(ctx, clg):
     xs = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, precision=clg.SINGLE)
     with pytest.raises(clg.CLGError):
         S.Solve(xs, bs, U, clg.EFO_F_D)
+
+
+@pytest.mark.parametrize("space", ["EEDT_SVD", "EEDT_REV", "EEDT_HEV"])
+def test_gmres_mdr_recycles(ctx, clg, oracle, space):
+    """GMRES-MDR (CSolverGMRESMDR.cpp:16-170): the solves after the first start
+    by rotating the kept U_k to the eigenvectors of the deflation type's k x k
+    problem (with C_k = A U_k orthonormal again); every solve to the FP64 true
+    residual 1e-10, equal to the oracle's GMRES solution, and the recycled solves
+    as cheap as GCRO-DR's on the same sequence (the same subspace, another basis)."""
+    dims = (8, 8, 8, 8)
+    kappa = 0.124
+    lat = clg.Lattice(ctx, dims)
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60093, 1, 0.1)
+    Uh = U.CopyDataOut()
+    op = oracle.Operator("WILSON_D", dims, Uh, kappa)
+    apps = {}
+    for name, cls in (("mdr", clg.CSLASolverGMRESMDR), ("gcrodr", clg.CSLASolverGCRODR)):
+        S = cls(ctx, MDim=32, KDim=24, Restart=2000, DeflateSpace=getattr(clg, space))
+        apps[name] = []
+        for r in range(3):
+            b = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+            b.InitialField(clg.SOURCE_GAUSS, 0xC1A60094, 2 + r)
+            x = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+            info = S.Solve(x, b, U, clg.EFO_F_D)[0]
+            bh, xh = b.to_numpy(), x.to_numpy()
+            assert info["status"] == 0 and op.true_residual(bh, xh) <= TOL
+            if name == "mdr" and r == 2:
+                xo, _ = oracle.gmres(op, bh, maxdim=12, restart=400, accuracy=1e-26)
+                assert rel(xh, xo) < 1e-8
+            apps[name].append(info["iterations"])
+        S.close()
+    assert apps["mdr"][0] == apps["gcrodr"][0]  # the first solve is the same GMRES cycle
+    assert max(apps["mdr"][1:]) <= 1.25 * max(apps["gcrodr"][1:]), apps
