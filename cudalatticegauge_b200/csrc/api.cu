@@ -361,7 +361,7 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   if (const char* t = std::getenv("CLG_PDL")) ctx->pdl = t[0] != '0';
   if (const char* t = std::getenv("CLG_HOP_CONFIG")) {
     int variant = -1, bs = 0;
-    if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && variant >= 0 && variant <= 2 &&
+    if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && variant >= 0 && variant <= 3 &&
         (bs == 64 || bs == 128 || bs == 256))
       ctx->hop_config = bs | (variant << 16);
   }

@@ -17,11 +17,17 @@ bool idempotent(const HopArgs& a) { return a.x == nullptr || a.x != a.out; }
 template <int P, int RECON>
 cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
   // config = block size | (variant << 16): 0 plain, 1 capped at 80 registers,
-  // 2 capped at 72 registers (64-thread blocks only)
+  // 2 capped at 72 registers (64-thread blocks only), 3 capped at 128 (FP64:
+  // the uncapped FP64 kernel takes 254 registers, 8 warps per SM)
   auto go = [&](int cfg) {
     const int bs = cfg & 0xffff;
     const int variant = cfg >> 16;
     dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
+    if constexpr (P == P64) {
+      if (variant == 3)
+        return dagger ? launch_pdl(ctx, wilson_hop_kernel<P, RECON, true, 256, 2>, grid, dim3(bs), 0, a)
+                      : launch_pdl(ctx, wilson_hop_kernel<P, RECON, false, 256, 2>, grid, dim3(bs), 0, a);
+    }
     if constexpr (P != P64) {
       if (variant == 1)
         return dagger ? launch_pdl(ctx, wilson_hop_kernel<P, RECON, true, 256, 3>, grid, dim3(bs), 0, a)
@@ -39,6 +45,8 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
   if (P != P64)
     for (int bs : {64, 128, 256}) cand.push_back(bs | (1 << 16));
   if (P != P64) cand.push_back(64 | (2 << 16));
+  if (P == P64)
+    for (int bs : {64, 128, 256}) cand.push_back(bs | (3 << 16));
   return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 
@@ -79,11 +87,17 @@ cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagge
 
 template <int P, int RECON>
 cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
-  auto go = [&](int bs) {
+  // config = block size | (variant << 16): 0 uncapped, 1 capped at 80 registers
+  auto go = [&](int cfg) {
+    const int bs = cfg & 0xffff;
     dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
+    if ((cfg >> 16) == 1) return launch_pdl(ctx, staggered_hop_kernel_capped<P, RECON>, grid, dim3(bs), 0, a);
     return launch_pdl(ctx, staggered_hop_kernel<P, RECON>, grid, dim3(bs), 0, a);
   };
-  return go(tune_block(ctx, key, idempotent(a), go));
+  std::vector<int> cand = {64, 128, 256};
+  if (P == P64)
+    for (int bs : {64, 128, 256}) cand.push_back(bs | (1 << 16));
+  return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 
 // FP64 [mu][9][h] double2 -> FP32 12-real [mu][3][h] float4 or 18-real [mu][9][h] float2

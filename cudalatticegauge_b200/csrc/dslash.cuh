@@ -406,8 +406,10 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_kernel(HopArgs a) {
 
 // The hop over a batch of lattices (HopArgs::seg): right-hand side r on its own
 // lattice, the grid spanning the largest checkerboard.
+// (the register caps of the tuned one-lattice kernels: 80 for FP32 / FP16,
+// 128 for FP64)
 template <int P, int RECON, bool DAGGER>
-__global__ void __launch_bounds__(256) wilson_hop_batch_kernel(HopArgs a) {
+__global__ void __launch_bounds__(256, P == P64 ? 2 : 3) wilson_hop_batch_kernel(HopArgs a) {
   using AT = typename AccT<P>::T;
   const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
   const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
@@ -690,7 +692,7 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_epi_kernel(HopArgs
 }
 
 template <int P, int RECON>
-__global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
+__device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
   using AT = typename AccT<P>::T;
   const int64_t Vh = a.g.Vh;
   // right-hand sides are interleaved in blockIdx.x so that the CTAs of all rhs
@@ -750,6 +752,18 @@ __global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
   }
   store_site<P, 3, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
                        a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
+}
+
+// __launch_bounds__(256): the FP64 kernel takes 90 registers (22 warps per
+// SM); the capped form (256, 3) holds it to 80 (24 warps).  The autotuner
+// picks per operator and lattice.
+template <int P, int RECON>
+__global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
+  staggered_hop_body<P, RECON>(a);
+}
+template <int P, int RECON>
+__global__ void __launch_bounds__(256, 3) staggered_hop_kernel_capped(HopArgs a) {
+  staggered_hop_body<P, RECON>(a);
 }
 
 }  // namespace clg

@@ -86,7 +86,7 @@ struct clg_context_s {
   // block size chosen per kernel variant by the autotuner
   std::map<std::string, int> tuned;
   bool tuning_enabled = true;
-  // CLG_HOP_CONFIG="<variant>:<block>" pins the Wilson hop launch (variant
+  // CLG_HOP_CONFIG="<variant>:<block>" pins the Wilson hop launch (variant 3: FP64 capped at 128;
   // 0 plain, 1 register-capped; block 64, 128 or 256); -1 lets the autotuner choose
   int hop_config = -1;
   // CG on the Wilson normal equations fuses its vector work into the Schur

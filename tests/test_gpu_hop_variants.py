@@ -42,8 +42,8 @@ def monkeypatch_module():
     mp.undo()
 
 
-@pytest.mark.parametrize("cfg", CONFIGS)
-@pytest.mark.parametrize("prec,tol", [(1, 2e-6), (2, 5e-3)])
+@pytest.mark.parametrize("cfg", CONFIGS + ["3:64", "3:128", "3:256"])
+@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 2e-6), (2, 5e-3)])
 @pytest.mark.parametrize("dims", [(8, 8, 8, 8), (4, 6, 4, 10)])
 def test_hop_variant(clg, oracle, pinned, cfg, prec, tol, dims):
     ctx = pinned(cfg)
