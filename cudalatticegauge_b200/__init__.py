@@ -40,7 +40,7 @@ GAUGE_IDENTITY, GAUGE_HAAR, GAUGE_EXPH, GAUGE_ZERO = 0, 1, 2, 3
  FILE_BRIDGEPP_TXT) = range(6)
 SOURCE_ZERO, SOURCE_GAUSS, SOURCE_Z2, SOURCE_POINT, SOURCE_Z4 = 0, 1, 2, 3, 4
 (SOLVER_GMRES, SOLVER_BICGSTAB, SOLVER_CG, SOLVER_CGM, SOLVER_FOM_MS, SOLVER_GCRODR, SOLVER_NESTED_MS,
- SOLVER_BICGSTAB_MS, SOLVER_GMRESMDR) = 0, 1, 2, 3, 4, 5, 6, 7, 8
+ SOLVER_BICGSTAB_MS, SOLVER_GMRESMDR, SOLVER_GMRES_MS) = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9
 EEDT_SVD, EEDT_REV, EEDT_HEV = 0, 1, 2  # GCRO-DR deflation spaces (EEigenDeflationType)
 
 
@@ -529,6 +529,16 @@ class CMultiShiftFOM(_MultiShift):
 
     def __init__(self, ctx: Context, **kw):
         kw.setdefault("MaxDim", 30)
+        super().__init__(ctx, **kw)
+
+
+class CMultiShiftGMRES(_MultiShift):
+    """CMultiShiftGMRES (CMultiShiftGMRES.cpp:113-330): restarted GMRES on the seed
+    system, every shift's residual collinear with the seed's; FP64 fields."""
+    KIND = SOLVER_GMRES_MS
+
+    def __init__(self, ctx: Context, **kw):
+        kw.setdefault("MaxDim", 10)
         super().__init__(ctx, **kw)
 
 

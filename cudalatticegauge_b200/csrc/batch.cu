@@ -150,6 +150,7 @@ extern "C" clg_status clg_solve_lattices(clg_solver S, int n, clg_field* x, clg_
         cudaStreamSynchronize(ctx->stream) != cudaSuccess)
       return ctx->fail(CLG_ERR_CUDA, "solve_lattices: table upload");
     nw->vgauge.seg = nw->seg_dev;
+    nw->vgauge.seg_vh = nw->vh_dev;
     nw->B = padded_full(static_cast<char*>(nw->b_data), nc, total, vh_max);
     nw->X = padded_full(static_cast<char*>(nw->x_data), nc, total, vh_max);
     nw->key = key;

@@ -260,6 +260,7 @@ clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec
   a.skip_stride = s.skip_stride;
   a.nrhs = s.nrhs > 0 ? s.nrhs : 1;
   a.seg = U->seg;
+  a.seg_vh = U->seg_vh;
   if (U->seg) {
     if (s.kind != CLG_FERMION_WILSON) return ctx->fail(CLG_ERR_UNSUPPORTED, "a batch of lattices takes Wilson fermions");
     a.U_here = a.U_there = nullptr;

@@ -54,9 +54,11 @@ struct HopArgs {
   int skip_stride;
   int nrhs;                 // right-hand sides (interleaved in blockIdx.x)
   // a batch of lattices (nullable): right-hand side r lives on lattice seg[r]
-  // (geometry and links); g.Vh is then the fields' chunk stride, the largest
-  // checkerboard of the batch, and sites h >= seg[r].g.Vh are padding
+  // (geometry and links, checkerboard size seg_vh[r]); g.Vh is then the
+  // fields' chunk stride, the largest checkerboard of the batch, and sites
+  // h >= seg_vh[r] are padding
   const HopSeg* seg;
+  const int64_t* seg_vh;
 };
 
 // chiral gamma tables (GammaMatrix.h:447-478): row r -> column perm[r] with phase i^z4[r]
@@ -438,7 +440,9 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E
   const int64_t h = (int64_t)slot * blockDim.x + threadIdx.x;
   pdl_launch_dependents();
   pdl_wait();
-  const bool skipped = a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride];
+  // in a batch of lattices a block wholly in this rhs's padding reduces nothing
+  const bool skipped = (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) ||
+                       (BATCH && (int64_t)slot * blockDim.x >= a.seg_vh[rhs]);
   double red[E::NRED];
 #pragma unroll
   for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
@@ -455,7 +459,7 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E
     }
   }
   grid_reduce_finalize<E::NRED>(red, e, rhs, slot, gridDim.x / (unsigned)a.nrhs, a.nrhs, partials, counter,
-                                !skipped);
+                                !skipped, BATCH ? a.seg_vh : nullptr);
 }
 
 // ---------------------------------------------------------------- FP16, two right-hand sides per thread

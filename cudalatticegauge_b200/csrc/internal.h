@@ -139,6 +139,7 @@ struct clg_gauge_s {
   // a batch of lattices (clg_solve_lattices): per right-hand side geometry and
   // link arrays on the device; lat is then the batch's padded virtual lattice
   const clg::HopSeg* seg = nullptr;
+  const int64_t* seg_vh = nullptr;  // per right-hand side checkerboard sizes (device)
   // per parity link arrays [mu][chunk][h]
   void* u64[2] = {nullptr, nullptr};   // FP64, 18 reals
   void* u32[2] = {nullptr, nullptr};   // FP32, 12 reals (SU(3)) or 18

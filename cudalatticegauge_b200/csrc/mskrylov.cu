@@ -1,7 +1,8 @@
 // mskrylov.cu -- the reference's multi-shift solvers that share one Krylov
 // space of A over every shift c_n of (A + c_n) x_n = b: CMultiShiftFOM::Solve
-// (SparseLinearAlgebra/CMultiShiftFOM.cpp:97-270) and CMultiShiftBiCGStab::Solve
-// (CMultiShiftBiCGStab.cpp:73-437, at the end of this file).
+// (SparseLinearAlgebra/CMultiShiftFOM.cpp:97-270), CMultiShiftGMRES::Solve
+// (CMultiShiftGMRES.cpp:113-330) and CMultiShiftBiCGStab::Solve
+// (CMultiShiftBiCGStab.cpp:73-437), the latter two at the end of this file.
 //
 // Restarted FOM(m) (the full orthogonalisation method): the Arnoldi relation
 // A V_m = V_m H_m + h_{m+1,m} v_{m+1} e_m^T holds for A + c_n with H_m + c_n,
@@ -173,6 +174,149 @@ clg_status fom_ms_run(clg_context_s* ctx, std::unique_ptr<SolveCacheBase>& cache
     }
     *apps_out += dim;
     if (worst <= tol * bnorm || dim < m) break;
+  }
+  return CLG_SUCCESS;
+}
+
+// CMultiShiftGMRES::Solve (SparseLinearAlgebra/CMultiShiftGMRES.cpp:113-330;
+// A. Frommer and U. Glaessner, SIAM J. Sci. Comput. 19 (1998) 15): restarted
+// GMRES(m) on the unshifted seed system; every shift keeps its residual
+// collinear with the seed's, r_n = beta_n r_seed: with z = beta e_1 - Hbar y
+// (the seed's residual in the cycle's basis), shift n solves the square system
+// [Hbar + c_n I~ | z] [y_n; beta_n'] = beta_n beta e_1 and adds V y_n to x_n.
+// The next cycle restarts from the seed's true residual b - A x_seed.  Stop
+// when every |beta_n| |z| (the shifted residual norms) is below tol |b|.
+clg_status gmres_ms_run(clg_context_s* ctx, std::unique_ptr<SolveCacheBase>& cache, const clg_gauge_s* U, int kind,
+                        double param, int op, const FieldRef& b, const std::vector<double2>& shifts, int m, int restart,
+                        double tol, const FieldRef** X_out, int* apps_out, int* cycles_out) {
+  const int ns = (int)shifts.size();
+  const int nc = b.nc;
+  const int64_t Vh = b.Vh;
+  const std::string key = "gmres-m/" + std::to_string((uintptr_t)b.data) + "/" + std::to_string(b.nparity) + "/" +
+                          std::to_string(b.first_parity) + "/" + std::to_string(nc) + "/" + std::to_string(Vh) +
+                          "/" + std::to_string(m) + "/" + std::to_string(ns);
+  auto* W = dynamic_cast<FomWork*>(cache.get());
+  if (!W || W->key != key) {
+    cudaStreamSynchronize(ctx->stream);
+    cache.reset();
+    auto nw = std::make_unique<FomWork>();
+    nw->ctx = ctx;
+    nw->proto = b;
+    nw->proto.nrhs = 1;
+    nw->proto.rstride = nw->proto.blk * nw->proto.nparity;
+    nw->V.resize(m + 1);  // V[m] holds the seed solution
+    clg_status st = CLG_SUCCESS;
+    for (FieldRef& f : nw->V)
+      if (!st) st = nw->vec(f);
+    if (!st) st = nw->vec(nw->w);
+    if (!st) st = nw->vec(nw->R);
+    if (!st) st = nw->full_vec(nw->tmp);
+    if (!st) st = nw->out_buffer();
+    if (!st) {
+      void* p = nullptr;
+      st = dalloc(ctx, &p, (size_t)nw->proto.rstride * ns);
+      if (!st) {
+        nw->allocs.push_back(p);
+        nw->X = nw->proto;
+        nw->X.data = static_cast<char*>(p);
+        nw->X.nrhs = ns;
+      }
+    }
+    if (st) return st;
+    nw->key = key;
+    W = nw.get();
+    cache = std::move(nw);
+  }
+  hk::HostKrylov K{ctx, *W, U, kind, op, nc, param, Vh};
+  auto xk = [&](int k) {
+    FieldRef f = W->X;
+    f.data = W->X.data + (int64_t)k * W->X.rstride;
+    f.nrhs = 1;
+    return f;
+  };
+  const Z zero(0.0, 0.0), one(1.0, 0.0);
+  FieldRef& xs = W->V[m];
+  clg_status st;
+  for (int k = 0; k < ns; ++k)
+    if ((st = K.scale(xk(k), zero))) return st;
+  if ((st = K.scale(xs, zero))) return st;
+  *X_out = &W->X;
+  *apps_out = 0;
+  *cycles_out = 0;
+  const double bnorm = K.norm(b);
+  if (bnorm < 0) return ctx->fail(CLG_ERR_CUDA, "multi-shift GMRES: reading |b|");
+  if (bnorm == 0.0) return CLG_SUCCESS;
+  std::vector<Z> beta0(ns, one);
+  for (int cyc = 0; cyc < restart; ++cyc) {
+    ++*cycles_out;
+    // the seed residual: b, then b - A x_seed (CMultiShiftGMRES.cpp:158-172)
+    if (cyc == 0) {
+      if ((st = K.copy(W->R, b))) return st;
+    } else {
+      if ((st = K.apply(W->w, xs)) || (st = K.lincomb(W->R, zero, {&b, &W->w}, {one, -one}))) return st;
+    }
+    const double beta = K.norm(W->R);
+    if (beta < 0) return ctx->fail(CLG_ERR_CUDA, "multi-shift GMRES: reading |r|");
+    if (beta == 0.0) break;
+    if ((st = K.lincomb(W->V[0], zero, {&W->R}, {Z(1.0 / beta, 0.0)}))) return st;
+    Mat H(m + 1, m);
+    int dim = m;
+    for (int j = 0; j < m; ++j) {
+      if ((st = K.apply(W->w, W->V[j]))) return st;
+      std::vector<const FieldRef*> vs;
+      for (int i = 0; i <= j; ++i) vs.push_back(&W->V[i]);
+      std::vector<Z> h;
+      if ((st = K.orthogonalise(W->w, vs, h))) return st;
+      for (int i = 0; i <= j; ++i) H(i, j) = h[i];
+      const double hn = K.norm(W->w);
+      if (hn < 0) return ctx->fail(CLG_ERR_CUDA, "multi-shift GMRES: reading |w|");
+      H(j + 1, j) = Z(hn, 0.0);
+      if (hn <= 1e-300 * bnorm) {
+        dim = j + 1;
+        break;
+      }
+      if (j + 1 < m && (st = K.lincomb(W->V[j + 1], zero, {&W->w}, {Z(1.0 / hn, 0.0)}))) return st;
+    }
+    *apps_out += dim + (cyc > 0 ? 1 : 0);
+    // the seed system: y = argmin |beta e_1 - Hbar y|, z = beta e_1 - Hbar y
+    Mat Hb(dim + 1, dim);
+    for (int r = 0; r <= dim; ++r)
+      for (int c = 0; c < dim; ++c) Hb(r, c) = H(r, c);
+    std::vector<Z> g(dim + 1, zero), y;
+    g[0] = Z(beta, 0.0);
+    if (!dense::lstsq(Hb, g, y)) return ctx->fail(CLG_ERR_BREAKDOWN, "multi-shift GMRES: seed least squares");
+    std::vector<const FieldRef*> vs;
+    for (int i = 0; i < dim; ++i) vs.push_back(&W->V[i]);
+    if ((st = K.lincomb(xs, one, vs, y))) return st;
+    std::vector<Z> z(dim + 1);
+    for (int r = 0; r <= dim; ++r) {
+      Z hy = zero;
+      for (int c = 0; c < dim; ++c) hy += Hb(r, c) * y[c];
+      z[r] = g[r] - hy;
+    }
+    double zn = 0.0;
+    for (const Z& v : z) zn += std::norm(v);
+    zn = std::sqrt(zn);
+    double worst = 0.0;
+    for (int n = 0; n < ns; ++n) {
+      // [Hbar + c_n I~ | z] [y_n; beta_n'] = beta_n beta e_1
+      Mat Hh(dim + 1, dim + 1);
+      for (int r = 0; r <= dim; ++r) {
+        for (int c = 0; c < dim; ++c)
+          Hh(r, c) = Hb(r, c) + (r == c ? Z(shifts[n].x, shifts[n].y) : zero);
+        Hh(r, dim) = z[r];
+      }
+      std::vector<Z> gn(dim + 1, zero), w;
+      gn[0] = beta0[n] * beta;
+      if (!dense::lstsq(Hh, gn, w)) return ctx->fail(CLG_ERR_BREAKDOWN, "multi-shift GMRES: shifted system");
+      std::vector<Z> yn(w.begin(), w.begin() + dim);
+      if ((st = K.lincomb(xk(n), one, vs, yn))) return st;
+      beta0[n] = w[dim];
+      const double e = std::abs(beta0[n]) * zn;
+      if (!(e == e)) return ctx->fail(CLG_ERR_BREAKDOWN, "multi-shift GMRES: NaN in the recurrence");
+      worst = std::max(worst, e);
+    }
+    if (worst <= tol * bnorm) break;
   }
   return CLG_SUCCESS;
 }

@@ -35,6 +35,10 @@ clg_status bicgstab_ms_run(clg_context_s* ctx, std::unique_ptr<SolveCacheBase>& 
                            double param, int op, const FieldRef& b, const std::vector<double2>& shifts, int dev_step,
                            int max_step, double tol, const FieldRef** X_out, int* apps_out, int* iters_out);
 
+clg_status gmres_ms_run(clg_context_s* ctx, std::unique_ptr<SolveCacheBase>& cache, const clg_gauge_s* U, int kind,
+                        double param, int op, const FieldRef& b, const std::vector<double2>& shifts, int m, int restart,
+                        double tol, const FieldRef** X_out, int* apps_out, int* cycles_out);
+
 constexpr int CGM_MAXSHIFT = 64;
 
 struct CgmState {
@@ -376,8 +380,9 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
   for (int k = 0; k < nshift; ++k)
     if (clg_status st = settle(x[k])) return st;
   if (S->p.kind != CLG_SOLVER_CGM && S->p.kind != CLG_SOLVER_FOM_MS && S->p.kind != CLG_SOLVER_NESTED_MS &&
-      S->p.kind != CLG_SOLVER_BICGSTAB_MS)
-    return ctx->fail(CLG_ERR_BAD_ARG, "clg_solve_multishift needs a CGM, FOM_MS, BICGSTAB_MS or NESTED_MS solver");
+      S->p.kind != CLG_SOLVER_BICGSTAB_MS && S->p.kind != CLG_SOLVER_GMRES_MS)
+    return ctx->fail(CLG_ERR_BAD_ARG,
+                     "clg_solve_multishift needs a CGM, FOM_MS, GMRES_MS, BICGSTAB_MS or NESTED_MS solver");
   std::vector<double2> sh(nshift);
   for (int k = 0; k < nshift; ++k) sh[k] = make_double2(shifts[2 * k], shifts[2 * k + 1]);
   const bool hermitian = op == CLG_OP_DDDAG || op == CLG_OP_DDDAG_EE || op == CLG_OP_MEE_MEEDAG;
@@ -431,7 +436,8 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
     if ((s = cgm_run(ctx, *W, g, b->kind, b->param, op, b->ref(), real, itol, prm.max_iterations, &cgm_iters)))
       return s;
     prm.kind = CLG_SOLVER_CG;  // per-shift refinement
-  } else if (S->p.kind == CLG_SOLVER_FOM_MS || S->p.kind == CLG_SOLVER_BICGSTAB_MS) {
+  } else if (S->p.kind == CLG_SOLVER_FOM_MS || S->p.kind == CLG_SOLVER_BICGSTAB_MS ||
+             S->p.kind == CLG_SOLVER_GMRES_MS) {
     if (b->prec != CLG_PREC_DOUBLE)
       return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift FOM / BiCGStab work on FP64 fields");
     for (int k = 0; k < nshift; ++k)
@@ -441,6 +447,9 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
     if (S->p.kind == CLG_SOLVER_FOM_MS)
       s = fom_ms_run(ctx, S->cache_fom, g, b->kind, b->param, op, b->ref(), sh, prm.max_dim, prm.restart,
                      prm.tol_true_rel * 0.5, &fom_x, &fom_apps, &fom_cycles);
+    else if (S->p.kind == CLG_SOLVER_GMRES_MS)
+      s = gmres_ms_run(ctx, S->cache_fom, g, b->kind, b->param, op, b->ref(), sh, prm.max_dim, prm.restart,
+                       prm.tol_true_rel * 0.5, &fom_x, &fom_apps, &fom_cycles);
     else
       s = bicgstab_ms_run(ctx, S->cache_fom, g, b->kind, b->param, op, b->ref(), sh, std::max(1, prm.deviation_step),
                           std::max(1, prm.max_step), prm.tol_true_rel * 0.5, &fom_x, &fom_apps, &fom_cycles);

@@ -17,7 +17,7 @@ namespace clg {
 // every thread of that block (at most 256 threads, 8 warps).
 template <int NRED, class F>
 __device__ __forceinline__ void grid_final_reduce(const F& f, unsigned nslots, int nrhs, const double* partials,
-                                                  unsigned* counter) {
+                                                  unsigned* counter, const int64_t* rhs_sites = nullptr) {
   __shared__ double sm[NRED][8];
   __shared__ double tot[NRED];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -29,13 +29,16 @@ __device__ __forceinline__ void grid_final_reduce(const F& f, unsigned nslots, i
 #pragma unroll
     for (int k = 0; k < NRED; ++k) s[k] = 0.0;
     const double* pr = partials + (int64_t)r * nslots * NRED;
-    for (unsigned b0 = threadIdx.x; b0 < nslots; b0 += U * blockDim.x) {
+    // a batch of lattices: only the slots that hold sites of this rhs's lattice wrote a partial
+    const unsigned ns = rhs_sites ? (unsigned)min((int64_t)nslots, (rhs_sites[r] + blockDim.x - 1) / blockDim.x)
+                                  : nslots;
+    for (unsigned b0 = threadIdx.x; b0 < ns; b0 += U * blockDim.x) {
       double v[U][NRED];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const unsigned b = b0 + u * blockDim.x;
 #pragma unroll
-        for (int k = 0; k < NRED; ++k) v[u][k] = b < nslots ? __ldcg(pr + (int64_t)b * NRED + k) : 0.0;
+        for (int k = 0; k < NRED; ++k) v[u][k] = b < ns ? __ldcg(pr + (int64_t)b * NRED + k) : 0.0;
       }
 #pragma unroll
       for (int u = 0; u < U; ++u)
@@ -69,7 +72,7 @@ __device__ __forceinline__ void grid_final_reduce(const F& f, unsigned nslots, i
 template <int NRED, class F>
 __device__ __forceinline__ void grid_reduce_finalize(double (&acc)[NRED], const F& f, int rhs, unsigned slot,
                                                      unsigned nslots, int nrhs, double* partials, unsigned* counter,
-                                                     bool contribute = true) {
+                                                     bool contribute = true, const int64_t* rhs_sites = nullptr) {
   __shared__ double sm[NRED][8];
   __shared__ bool last;
   if (contribute) {
@@ -99,7 +102,7 @@ __device__ __forceinline__ void grid_reduce_finalize(double (&acc)[NRED], const 
   __syncthreads();
   if (!last) return;
   __threadfence();
-  grid_final_reduce<NRED>(f, nslots, nrhs, partials, counter);
+  grid_final_reduce<NRED>(f, nslots, nrhs, partials, counter, rhs_sites);
 }
 
 // The same for a block that computes two right-hand sides (rhs0 with acc[0,

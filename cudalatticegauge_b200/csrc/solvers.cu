@@ -849,13 +849,14 @@ clg_status clg_solver_default_params(int kind, clg_solver_params* p) {
 
 clg_status clg_solver_create(clg_context ctx, const clg_solver_params* p, clg_solver* out) {
   if (!ctx || !p || !out) return CLG_ERR_BAD_ARG;
-  if (p->kind < 0 || p->kind > CLG_SOLVER_GMRESMDR || p->inner_precision < 0 || p->inner_precision > 2 ||
+  if (p->kind < 0 || p->kind > CLG_SOLVER_GMRES_MS || p->inner_precision < 0 || p->inner_precision > 2 ||
       !(p->tol_true_rel > 0) || p->max_iterations < 1 || p->max_outer < 1)
     return ctx->fail(CLG_ERR_BAD_ARG, "invalid solver parameters");
   if ((p->kind == CLG_SOLVER_GMRES || p->kind == CLG_SOLVER_NESTED_MS) && (p->max_dim < 1 || p->max_dim > GM_MAXK))
     return ctx->fail(CLG_ERR_UNSUPPORTED, "GMRES MaxDim must be in [1, 16] on the device");
-  if (p->kind == CLG_SOLVER_FOM_MS && (p->max_dim < 2 || p->max_dim > 32 || p->restart < 1))
-    return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift FOM: MaxDim in [2, 32], Restart >= 1");
+  if ((p->kind == CLG_SOLVER_FOM_MS || p->kind == CLG_SOLVER_GMRES_MS) &&
+      (p->max_dim < 2 || p->max_dim > 32 || p->restart < 1))
+    return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift FOM / GMRES: MaxDim in [2, 32], Restart >= 1");
   if ((p->kind == CLG_SOLVER_GCRODR || p->kind == CLG_SOLVER_GMRESMDR) &&
       (p->max_dim < 5 || p->max_dim > 32 || p->kdim < 0 || (p->kdim > 0 && (p->kdim < 2 || p->kdim > p->max_dim - 2)) ||
        p->deflation < CLG_DEFLATION_SVD || p->deflation > CLG_DEFLATION_HEV))
@@ -880,7 +881,7 @@ clg_status clg_solve(clg_solver S, clg_field X, clg_field B, clg_gauge U, int op
       (X0 && (X0->lat != B->lat || X0->subset != B->subset || X0->nrhs != B->nrhs || X0->kind != B->kind)))
     return ctx->fail(CLG_ERR_BAD_ARG, "solve: field shapes differ");
   if (S->p.kind == CLG_SOLVER_CGM || S->p.kind == CLG_SOLVER_FOM_MS || S->p.kind == CLG_SOLVER_NESTED_MS ||
-      S->p.kind == CLG_SOLVER_BICGSTAB_MS)
+      S->p.kind == CLG_SOLVER_BICGSTAB_MS || S->p.kind == CLG_SOLVER_GMRES_MS)
     return ctx->fail(CLG_ERR_BAD_ARG, "multi-shift solvers are called through clg_solve_multishift");
   if (S->p.kind == CLG_SOLVER_GCRODR || S->p.kind == CLG_SOLVER_GMRESMDR) return gcrodr_solve(S, X, B, U, op, X0, info);
   for (clg_field f : {X, B, X0})

@@ -89,7 +89,8 @@ typedef enum {
     CLG_SOLVER_GCRODR = 5,      /* CSLASolverGCRODR   SparseLinearAlgebra/CSolverGCRODR.cpp:196-911   */
     CLG_SOLVER_NESTED_MS = 6,   /* CMultiShiftNested  SparseLinearAlgebra/CMultiShiftNested.cpp:69-145 */
     CLG_SOLVER_BICGSTAB_MS = 7, /* CMultiShiftBiCGStab SparseLinearAlgebra/CMultiShiftBiCGStab.cpp:73-437 */
-    CLG_SOLVER_GMRESMDR = 8     /* CSLASolverGMRESMDR SparseLinearAlgebra/CSolverGMRESMDR.cpp:16-170  */
+    CLG_SOLVER_GMRESMDR = 8,    /* CSLASolverGMRESMDR SparseLinearAlgebra/CSolverGMRESMDR.cpp:16-170  */
+    CLG_SOLVER_GMRES_MS = 9     /* CMultiShiftGMRES   SparseLinearAlgebra/CMultiShiftGMRES.cpp:113-330 */
 } clg_solver_kind;
 
 /* GCRO-DR deflation space (EEigenDeflationType, CSolverGCRODR.cpp:541-760):
@@ -288,6 +289,9 @@ clg_status clg_solve(clg_solver s, clg_field x, clg_field b, clg_gauge g, int op
  *     every complex shift, FP64 (b and x FP64), restart = cycles, stop when every
  *     shift's residual |beta_n| <= tol_true_rel |b|; then the true residuals are
  *     checked in FP64 and refined if needed.
+ *   CLG_SOLVER_GMRES_MS: restarted GMRES(max_dim <= 32) on the unshifted seed
+ *     system with every shift's residual kept collinear with the seed's
+ *     (Frommer-Glaessner), FP64, restart = cycles; then checked and refined.
  *   CLG_SOLVER_BICGSTAB_MS: BiCGStab-M (shadow residual conj(b)) over one Krylov
  *     space for every complex shift, FP64, checked every deviation_step
  *     iterations, at most max_step * deviation_step iterations; then checked and

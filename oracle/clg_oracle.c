@@ -970,3 +970,126 @@ int clgo_bicgstab_ms(const clgo_op* op, const double* b, int nshift, const doubl
     free(R); free(W); free(W0); free(S); free(SA); free(WA); free(T);
     return done;
 }
+
+/* ============================================================== multi-shift GMRES
+ * CMultiShiftGMRES::Solve (SparseLinearAlgebra/CMultiShiftGMRES.cpp:113-330;
+ * Frommer & Glaessner 1998): restarted GMRES(m) on the seed system A x = b (x
+ * from the true residual b - A x at every restart), every shift's residual kept
+ * collinear with the seed's: with z = beta e_1 - Hbar y, shift n solves
+ * [Hbar + c_n I~ | z] (y_n; beta0_n') = beta0_n beta e_1 and adds V y_n.
+ * Stop when max |beta0_n| < accuracy * blen (blen = |b|^2, or 1 absolute),
+ * the reference's rule.  The small systems by Gaussian elimination with
+ * partial pivoting (the reference: Givens / QR on the device; same solutions). */
+static int solve_square(int n, cplx* A, cplx* rhs, cplx* out) {   /* A n x n row-major, destroyed */
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < n; ++r) if (cabs(A[r * n + col]) > cabs(A[piv * n + col])) piv = r;
+        if (cabs(A[piv * n + col]) == 0.0) return 0;
+        if (piv != col) {
+            for (int c = 0; c < n; ++c) { cplx t = A[col * n + c]; A[col * n + c] = A[piv * n + c]; A[piv * n + c] = t; }
+            cplx t = rhs[col]; rhs[col] = rhs[piv]; rhs[piv] = t;
+        }
+        for (int r = col + 1; r < n; ++r) {
+            const cplx f = A[r * n + col] / A[col * n + col];
+            if (f == 0) continue;
+            for (int c = col; c < n; ++c) A[r * n + c] -= f * A[col * n + c];
+            rhs[r] -= f * rhs[col];
+        }
+    }
+    for (int r = n - 1; r >= 0; --r) {
+        cplx acc = rhs[r];
+        for (int c = r + 1; c < n; ++c) acc -= A[r * n + c] * out[c];
+        out[r] = acc / A[r * n + r];
+    }
+    return 1;
+}
+
+int clgo_gmres_ms(const clgo_op* op, const double* b, int nshift, const double* shifts_c, double* x,
+                  int maxdim, int restart, double accuracy, int absolute, clgo_info* info) {
+    const long n = clgo_op_len(op);
+    const int m = maxdim;
+    double** v = (double**)malloc(sizeof(double*) * m);
+    for (int i = 0; i < m; ++i) v[i] = valloc(n);
+    double *W = valloc(n), *X = valloc(n), *T = valloc(n);
+    cplx* h = (cplx*)calloc((size_t)(m + 1) * m, sizeof(cplx));
+    cplx* hh = (cplx*)calloc((size_t)(m + 1) * (m + 1), sizeof(cplx));
+    cplx *y = (cplx*)calloc((size_t)m + 1, sizeof(cplx)), *z = (cplx*)calloc((size_t)m + 1, sizeof(cplx)),
+         *g = (cplx*)calloc((size_t)m + 1, sizeof(cplx)), *w = (cplx*)calloc((size_t)m + 1, sizeof(cplx));
+    cplx* beta0 = (cplx*)malloc(sizeof(cplx) * nshift);
+    for (int s = 0; s < nshift; ++s) beta0[s] = 1;
+    const double blen = absolute ? 1.0 : clgo_norm2(n, b);
+    memset(x, 0, sizeof(double) * 2 * n * nshift);
+    memset(X, 0, sizeof(double) * 2 * n);
+    int napply = 0, converged = 0, cycles = 0;
+    double maxerr = 0;
+    for (int it = 0; it < restart; ++it) {
+        ++cycles;
+        if (it == 0) vcopy(n, b, v[0]);
+        else {
+            clgo_apply(op, X, T); ++napply;
+#pragma omp parallel for schedule(static)
+            for (long k = 0; k < 2 * n; ++k) v[0][k] = b[k] - T[k];
+        }
+        const double beta = sqrt(clgo_norm2(n, v[0]));
+        cscale(n, 1.0 / beta, v[0]);
+        for (int j = 0; j < m; ++j) {
+            clgo_apply(op, v[j], W); ++napply;
+            for (int k = 0; k <= j; ++k) {
+                const cplx d = cdot(n, v[k], W);
+                h[k * m + j] = d;
+                caxpy(n, -d, v[k], W);
+            }
+            const double wn = sqrt(clgo_norm2(n, W));
+            h[(j + 1) * m + j] = wn;
+            if (j < m - 1) { cscale(n, 1.0 / wn, W); vcopy(n, W, v[j + 1]); }
+        }
+        /* the seed: least squares min |beta e1 - Hbar y| through the normal
+         * equations of the small problem (Hbar^+ Hbar y = Hbar^+ beta e1) */
+        {
+            cplx* A = (cplx*)calloc((size_t)m * m, sizeof(cplx));
+            for (int r = 0; r < m; ++r) {
+                for (int c = 0; c < m; ++c) {
+                    cplx acc = 0;
+                    for (int k = 0; k <= m; ++k) acc += conj(h[k * m + r]) * h[k * m + c];
+                    A[r * m + c] = acc;
+                }
+                g[r] = conj(h[r]) * beta;   /* (Hbar^+ beta e1)_r = conj(h[0][r]) beta */
+            }
+            solve_square(m, A, g, y);
+            free(A);
+        }
+        for (int j = 0; j < m; ++j) caxpy(n, y[j], v[j], X);
+        for (int r = 0; r <= m; ++r) {
+            cplx hy = 0;
+            for (int c = 0; c < m; ++c) hy += h[r * m + c] * y[c];
+            z[r] = (r == 0 ? beta : 0.0) - hy;
+        }
+        maxerr = 0;
+        for (int s = 0; s < nshift; ++s) {
+            const cplx cs = shifts_c[2 * s] + I * shifts_c[2 * s + 1];
+            for (int r = 0; r <= m; ++r) {
+                for (int c = 0; c < m; ++c) hh[r * (m + 1) + c] = h[r * m + c] + (r == c ? cs : 0.0);
+                hh[r * (m + 1) + m] = z[r];
+                g[r] = (r == 0) ? beta0[s] * beta : 0.0;
+            }
+            solve_square(m + 1, hh, g, w);
+            beta0[s] = w[m];
+            if (cabs(beta0[s]) > maxerr) maxerr = cabs(beta0[s]);
+            for (int j = 0; j < m; ++j) caxpy(n, w[j], v[j], x + 2 * n * s);
+        }
+        if (maxerr < accuracy * blen) { converged = 1; break; }
+    }
+    if (info) {
+        info->iterations = napply; info->restarts = cycles; info->converged = converged;
+        info->last_deviation = maxerr;
+        double worst = 0;
+        for (int s = 0; s < nshift; ++s) {
+            const double t = clgo_true_residual(op, b, x + 2 * n * s, shifts_c[2 * s], shifts_c[2 * s + 1]);
+            if (t > worst) worst = t;
+        }
+        info->true_rel_residual = worst;
+    }
+    for (int i = 0; i < m; ++i) free(v[i]);
+    free(v); free(W); free(X); free(T); free(h); free(hh); free(y); free(z); free(g); free(w); free(beta0);
+    return converged;
+}

@@ -126,6 +126,8 @@ int clgo_fom_ms(const clgo_op* op, const double* b, int nshift, const double* sh
                 int maxdim, int restart, double accuracy, int absolute, clgo_info* info);
 int clgo_bicgstab_ms(const clgo_op* op, const double* b, int nshift, const double* shifts_c, double* x,
                      int dev_step, int max_step, double accuracy, int absolute, clgo_info* info);
+int clgo_gmres_ms(const clgo_op* op, const double* b, int nshift, const double* shifts_c, double* x,
+                  int maxdim, int restart, double accuracy, int absolute, clgo_info* info);
 double clgo_true_residual(const clgo_op* op, const double* b, const double* x, double shift_re, double shift_im);
 
 #ifdef __cplusplus

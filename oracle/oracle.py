@@ -106,6 +106,7 @@ def lib():
             "clgo_cgm": (i, [p, p, i, p, p, d, i, p]),
             "clgo_fom_ms": (i, [p, p, i, p, p, i, i, d, i, p]),
             "clgo_bicgstab_ms": (i, [p, p, i, p, p, i, i, d, i, p]),
+            "clgo_gmres_ms": (i, [p, p, i, p, p, i, i, d, i, p]),
             "clgo_true_residual": (d, [p, p, p, d, d]),
         }
         for name, (res, args) in sig.items():
@@ -403,6 +404,17 @@ def fom_ms(op: Operator, b, shifts, maxdim=12, restart=100, accuracy=1e-10, abso
     info = Info()
     lib().clgo_fom_ms(C.byref(op.op), _ptr(b), len(sh), _ptr(sh.view(np.float64)), _ptr(x), maxdim, restart,
                       accuracy, int(absolute), C.byref(info))
+    return x, info.as_dict()
+
+
+def gmres_ms(op: Operator, b, shifts, maxdim=10, restart=100, accuracy=1e-10, absolute=False):
+    """CMultiShiftGMRES (CMultiShiftGMRES.cpp:113-330) restated: (A + c_n) x_n = b."""
+    b = np.ascontiguousarray(b, np.complex128)
+    sh = np.ascontiguousarray(np.asarray(shifts, np.complex128))
+    x = np.empty((len(sh),) + b.shape, np.complex128)
+    info = Info()
+    lib().clgo_gmres_ms(C.byref(op.op), _ptr(b), len(sh), _ptr(sh.view(np.float64)), _ptr(x), maxdim, restart,
+                        accuracy, int(absolute), C.byref(info))
     return x, info.as_dict()
 
 

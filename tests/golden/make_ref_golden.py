@@ -186,6 +186,8 @@ CASES = [
           "solver": "gmres"},
          {"ops": ["InverseD"], "solver": "bicgstab", "tag": "bicgstab"},
          {"ops": ["MultiShiftD"], "ms_solver": "fom", "shifts": WILSON_SHIFTS},
+         {"ops": ["MultiShiftD"], "ms_solver": "gmres_ms", "shifts": WILSON_SHIFTS, "tag": "gmres"},
+         {"ops": ["MultiShiftD"], "ms_solver": "bicgstab_ms", "shifts": WILSON_SHIFTS, "tag": "bicgstab"},
      ]},
     # the near-ordered exp(i eps H) links of configs 2-4 on 8^3x16
     {"name": "wilson_expH_8x8x8x16", "L": (8, 8, 8, 16), "links": "expH", "seed": 0xC1A60001,
@@ -220,6 +222,14 @@ def solver_block(kind, bnorm):
         return {"SolverName": "CMultiShiftFOM", "SolverForFieldId": 2, "UseCudaForSmallMatrix": 0,
                 "MaxDim": 30, "Restart": 2000, "AbsoluteAccuracy": 1,
                 "Accuracy": repr(1e-12 * bnorm)}
+    if kind == "gmres_ms":
+        # stop when every collinearity factor |beta0_n| < Accuracy (absolute)
+        return {"SolverName": "CMultiShiftGMRES", "SolverForFieldId": 2, "MaxDim": 10, "Restart": 2000,
+                "AbsoluteAccuracy": 1, "Accuracy": repr(1e-12)}
+    if kind == "bicgstab_ms":
+        # stop when |s| and every |s_n| < Accuracy, checked every DiviationStep iterations
+        return {"SolverName": "CMultiShiftBiCGStab", "SolverForFieldId": 2, "DiviationStep": 10, "MaxStep": 500,
+                "AbsoluteAccuracy": 1, "Accuracy": repr(1e-12 * bnorm)}
     raise ValueError(kind)
 
 

@@ -29,7 +29,7 @@ def test_staggered_cgm_12_shifts(ctx, clg, oracle):
 
 @pytest.mark.parametrize("op,name", [("EFO_F_D", "WILSON_D"), ("EFO_F_Ddagger", "WILSON_DDAG"),
                                      ("EFO_F_DDdagger", "WILSON_DDDAG")])
-@pytest.mark.parametrize("method", ["FOM", "BiCGStab"])
+@pytest.mark.parametrize("method", ["FOM", "GMRES", "BiCGStab"])
 def test_wilson_fom_ms_complex_shifts(ctx, clg, oracle, op, name, method):
     """CMultiShiftFOM / CMultiShiftBiCGStab over one Krylov space with the reference test's shifts
     {2, 1, 0.5, i, 0.5+0.5i, 1-i} on D, D^+ and DD^+ (TestMultiShiftSolver.cpp:12-111):
@@ -46,6 +46,8 @@ def test_wilson_fom_ms_complex_shifts(ctx, clg, oracle, op, name, method):
     xs = [clg.CFieldFermionWilsonSquareSU3(lat, kappa) for _ in cs]
     if method == "FOM":
         S = clg.CMultiShiftFOM(ctx, MaxDim=30, Restart=100)
+    elif method == "GMRES":  # CMultiShiftGMRES (CMultiShiftGMRES.cpp:113-330)
+        S = clg.CMultiShiftGMRES(ctx, MaxDim=10, Restart=200)
     else:  # CMultiShiftBiCGStab (CMultiShiftBiCGStab.cpp:73-437)
         S = clg.CMultiShiftBiCGStab(ctx, DiviationStep=10, MaxStep=100)
     infos = S.Solve(xs, cs, b, U, getattr(clg, op))
@@ -54,6 +56,8 @@ def test_wilson_fom_ms_complex_shifts(ctx, clg, oracle, op, name, method):
     bh = b.to_numpy()
     if method == "FOM":
         xo, io = oracle.fom_ms(o, bh, cs, maxdim=30, restart=100, accuracy=1e-12 * np.linalg.norm(bh), absolute=True)
+    elif method == "GMRES":
+        xo, io = oracle.gmres_ms(o, bh, cs, maxdim=10, restart=200, accuracy=1e-13, absolute=True)
     else:
         xo, io = oracle.bicgstab_ms(o, bh, cs, dev_step=10, max_step=100, accuracy=1e-12)
     for k, c in enumerate(cs):

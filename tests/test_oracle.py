@@ -196,6 +196,12 @@ def test_oracle_solvers_small(oracle):
     for k, s in enumerate(cs):
         assert op.true_residual(b, ys[k], complex(s)) < 1e-10
         assert np.linalg.norm(ys[k] - xs[k]) < 1e-9 * np.linalg.norm(xs[k])
+    # GMRES-M (CMultiShiftGMRES.cpp:113-330): the seed's restarted GMRES, residuals kept collinear
+    zs, i7 = oracle.gmres_ms(op, b, cs, maxdim=10, restart=200, accuracy=1e-13, absolute=True)
+    assert i7["converged"]
+    for k, s in enumerate(cs):
+        assert op.true_residual(b, zs[k], complex(s)) < 1e-10
+        assert np.linalg.norm(zs[k] - xs[k]) < 1e-9 * np.linalg.norm(xs[k])
 
 
 def test_wilson_force_is_the_action_derivative(oracle):

@@ -152,6 +152,29 @@ def test_oracle_fom_ms_matches_reference(oracle, name, key, opname):
         assert err(xs[k], fx, "%s.%d" % (key, k)) < 1e-9, (k, c)
 
 
+@pytest.mark.parametrize("key,method", [("MultiShiftD_gmres", "gmres"), ("MultiShiftD_bicgstab", "bicgstab")])
+def test_oracle_gmres_bicgstab_ms_match_reference(oracle, key, method):
+    """CMultiShiftGMRES (CMultiShiftGMRES.cpp:113-330, MaxDim 10, stop on max |beta0_n| < 1e-12) and
+    CMultiShiftBiCGStab (CMultiShiftBiCGStab.cpp:73-437, DiviationStep 10, stop on |s|, |s_n| < 1e-12 |b|)
+    on the config-1 field with the reference test's shifts."""
+    fx = load("wilson_haar_8x8x8x8")
+    if key + ".shifts" not in fx:
+        pytest.skip("fixture without this solver's outputs")
+    L, V, U, b, _ = inputs(oracle, fx)
+    shifts = list(fx[key + ".shifts"])
+    op = oracle.Operator("WILSON_D", L, U, KAPPA)
+    bb = b.reshape(V, 4, 3)
+    if method == "gmres":
+        xs, info = oracle.gmres_ms(op, bb, shifts, maxdim=10, restart=2000, accuracy=1e-12, absolute=True)
+    else:
+        xs, info = oracle.bicgstab_ms(op, bb, shifts, dev_step=10, max_step=500, accuracy=1e-12 * np.linalg.norm(b),
+                                      absolute=True)
+    assert info["converged"] and int(fx[key + ".ok"]) == 1
+    for k in range(len(shifts)):
+        assert float(fx["%s.%d.true_res" % (key, k)]) < 1e-10
+        assert err(xs[k], fx, "%s.%d" % (key, k)) < 1e-9, k
+
+
 # ------------------------------------------------------------------ GPU: the product against the reference
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["wilson_haar_8x8x8x8", "wilson_expH_8x8x8x16"])
