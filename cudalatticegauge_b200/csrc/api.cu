@@ -352,10 +352,10 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
     int variant = -1, bs = 0;
     if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && (variant == 0 || variant == 1) &&
         (bs == 64 || bs == 128 || bs == 256)) {
-      ctx->hop_pair = true;
+      ctx->hop_pair_mode = 1;
       ctx->hop_pair_config = bs | (variant << 16);
     } else {
-      ctx->hop_pair = t[0] == '1';
+      ctx->hop_pair_mode = t[0] == '1' ? 1 : (t[0] == '0' ? 0 : 2);
     }
   }
   if (const char* t = std::getenv("CLG_PDL")) ctx->pdl = t[0] != '0';

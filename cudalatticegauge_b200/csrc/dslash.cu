@@ -85,6 +85,47 @@ cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagge
                 : launch_pdl(ctx, wilson_hop_batch_kernel<P, RECON, false>, grid, dim3(bs), 0, a);
 }
 
+// The autotuner's choice between one and two right-hand sides per thread for
+// the FP16 Wilson hop: single-rhs configurations keep their variant (0..2),
+// paired ones carry variant 8 + the pair variant.  The winner is also recorded
+// under the keys the fused epilogue launches look up.
+cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
+  auto it = ctx->tuned.find(key + "_auto");
+  int cfg;
+  if (it != ctx->tuned.end()) {
+    cfg = it->second;
+  } else {
+    auto go = [&](int c) -> cudaError_t {
+      const int v = c >> 16;
+      if (v >= 8) {
+        ctx->tuned[key + "_pair"] = (c & 0xffff) | ((v - 8) << 16);
+        return launch_wilson_pair(ctx, a, dagger, key);
+      }
+      ctx->tuned[key] = c;
+      return launch_wilson<P16, 12>(ctx, a, dagger, nrhs, key);
+    };
+    std::vector<int> cand;
+    for (int bs : {64, 128, 256}) {
+      cand.push_back(bs);
+      cand.push_back(bs | (1 << 16));
+      cand.push_back(bs | (8 << 16));
+      cand.push_back(bs | (9 << 16));
+    }
+    cand.push_back(64 | (2 << 16));
+    // untuned (inside a capture, or the output aliases the xpay source): the
+    // one-rhs kernel, and nothing is cached
+    if (!ctx->tuning_enabled || !idempotent(a) || stream_capturing(ctx->stream))
+      return launch_wilson<P16, 12>(ctx, a, dagger, nrhs, key);
+    cfg = tune_block(ctx, key + "_auto", true, go, cand);
+    ctx->tuned.erase(key);
+    ctx->tuned.erase(key + "_pair");
+    if ((cfg >> 16) >= 8) ctx->tuned[key + "_pair"] = (cfg & 0xffff) | (((cfg >> 16) - 8) << 16);
+    else ctx->tuned[key] = cfg;
+  }
+  if ((cfg >> 16) >= 8) return launch_wilson_pair(ctx, a, dagger, key);
+  return launch_wilson<P16, 12>(ctx, a, dagger, nrhs, key);
+}
+
 template <int P, int RECON>
 cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
   // config = block size | (variant << 16): 0 uncapped, 1 capped at 80 registers
@@ -316,8 +357,10 @@ clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
       e = wilson ? launch_wilson<P32, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 12>(ctx, a, s.nrhs, key);
     else
       e = wilson ? launch_wilson<P32, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 18>(ctx, a, s.nrhs, key);
-  } else if (wilson && s.nrhs >= 2 && ctx->hop_pair) {
+  } else if (wilson && s.nrhs >= 2 && ctx->hop_pair_mode == 1) {
     e = launch_wilson_pair(ctx, a, s.dagger, key);
+  } else if (wilson && s.nrhs >= 2 && ctx->hop_pair_mode == 2 && ctx->hop_config < 0) {
+    e = launch_wilson_auto(ctx, a, s.dagger, s.nrhs, key);
   } else {
     e = wilson ? launch_wilson<P16, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P16, 12>(ctx, a, s.nrhs, key);
   }

@@ -92,14 +92,16 @@ struct clg_context_s {
   // CG on the Wilson normal equations fuses its vector work into the Schur
   // hops; CLG_FUSED_CG=0 runs the separate kernels instead
   bool fused_cg = true;
-  // CLG_HOP_PAIR=1: FP16 Wilson hops over two or more right-hand sides compute
-  // them in pairs (one link load and reconstruction per pair, planar half2
-  // arithmetic); CLG_HOP_PAIR="<variant>:<block>" pins the paired launch
-  // (variant 0 uncapped, 1 capped at 128 registers).  Off by default: measured
-  // on 32^3x16 / 32^3x32 it is no faster than one right-hand side per thread
-  // with the right-hand sides interleaved over the blocks (13.6 against 13.4 us
-  // per rhs at 8 rhs, 27.2 against 27.5 at 28), whose links are shared through L2
-  bool hop_pair = false;
+  // FP16 Wilson hops over two or more right-hand sides: one right-hand side
+  // per thread (the right-hand sides interleaved over the blocks, links shared
+  // through L2) or two per thread (wilson_hop_pair_kernel: one link load and
+  // reconstruction per pair, planar half2 arithmetic).  hop_pair_mode 2 (the
+  // default) lets the autotuner time both forms per operator and lattice (the
+  // right-hand-side-per-thread axis); CLG_HOP_PAIR=0 keeps one, =1 forces two,
+  // "<variant>:<block>" pins the paired launch (variant 0 uncapped, 1 capped at
+  // 128 registers).  Measured on 32^3x16 / 32^3x32 the two are within a few
+  // per cent (13.6 against 13.4 us per rhs at 8 rhs, 27.2 against 27.5 at 28).
+  int hop_pair_mode = 2;
   // set by clg_solve_lattices for the duration of its solve: the per-rhs
   // checkerboard sizes (device) of the padded batch, whose site kernels skip
   // the padding (launches with this stride and right-hand-side count)

@@ -618,8 +618,10 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
   const int bs = tuned_hop_block(ctx, w.U, plain, P == P64 ? 64 : 128);
   const int64_t nblk = ((w.Vh + bs - 1) / bs) * w.nrhs;
   if constexpr (P == P16) {
-    if (w.nrhs >= 2 && ctx->hop_pair && !a.seg) {
-      const int cfg = tuned_hop_pair_config(ctx, w.U, plain, 128);
+    const int pcfg = tuned_hop_pair_config(ctx, w.U, plain, -1);
+    const bool pair = ctx->hop_pair_mode == 1 || (ctx->hop_pair_mode == 2 && pcfg >= 0);
+    if (w.nrhs >= 2 && pair && !a.seg) {
+      const int cfg = pcfg >= 0 ? pcfg : 128;
       const int pbs = cfg & 0xffff;
       // partials are indexed [rhs][slot]: nslots x nrhs of them
       if (clg_status st = ensure_reduction(ctx, ((w.Vh + pbs - 1) / pbs) * w.nrhs * E::NRED)) return st;

@@ -69,21 +69,34 @@ def test_hop_variant(clg, oracle, pinned, cfg, prec, tol, dims):
     src.close()
 
 
-@pytest.fixture(scope="module")
-def ctx_pair(clg):
-    """A second context whose FP16 Wilson hops compute pairs of right-hand sides
-    (CLG_HOP_PAIR=1; the default context keeps one right-hand side per thread)."""
+def _context_with(clg, name, value):
     import os
 
-    old = os.environ.get("CLG_HOP_PAIR")
-    os.environ["CLG_HOP_PAIR"] = "1"
+    old = os.environ.get(name)
+    os.environ[name] = value
     try:
-        c = clg.Context(0)
+        return clg.Context(0)
     finally:
         if old is None:
-            del os.environ["CLG_HOP_PAIR"]
+            del os.environ[name]
         else:
-            os.environ["CLG_HOP_PAIR"] = old
+            os.environ[name] = old
+
+
+@pytest.fixture(scope="module")
+def ctx_pair(clg):
+    """A context whose FP16 Wilson hops compute pairs of right-hand sides
+    (CLG_HOP_PAIR=1)."""
+    c = _context_with(clg, "CLG_HOP_PAIR", "1")
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def ctx_single(clg):
+    """A context whose FP16 Wilson hops keep one right-hand side per thread
+    (CLG_HOP_PAIR=0; the default context lets the autotuner time both)."""
+    c = _context_with(clg, "CLG_HOP_PAIR", "0")
     yield c
     c.close()
 
@@ -91,11 +104,12 @@ def ctx_pair(clg):
 @pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 10, 14, 12)])
 @pytest.mark.parametrize("nrhs", [2, 3, 5])
 @pytest.mark.parametrize("op", ["MEE", "MEE_DAG"])
-def test_fp16_pair_hop_bit_identical(ctx, ctx_pair, clg, dims, nrhs, op):
+def test_fp16_pair_hop_bit_identical(ctx, ctx_single, ctx_pair, clg, dims, nrhs, op):
     """The paired FP16 hop (two right-hand sides per thread, planar) gives the
-    same bits as the one-rhs kernel; odd counts leave one unpaired member."""
+    same bits as the one-rhs kernel; odd counts leave one unpaired member.  The
+    default context, whose autotuner picks either form, gives them too."""
     outs = []
-    for c in (ctx, ctx_pair):
+    for c in (ctx_single, ctx_pair, ctx):
         lat = clg.Lattice(c, dims)
         U = clg.CFieldGaugeSU3(lat)
         U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
@@ -106,15 +120,17 @@ def test_fp16_pair_hop_bit_identical(ctx, ctx_pair, clg, dims, nrhs, op):
         outs.append([f.to_numpy(r) for r in range(nrhs)])
     for r in range(nrhs):
         np.testing.assert_array_equal(outs[0][r], outs[1][r])
+        np.testing.assert_array_equal(outs[0][r], outs[2][r])
 
 
 @pytest.mark.parametrize("nrhs", [2, 3])
-def test_fp16_pair_cg_epilogues_identical(ctx, ctx_pair, clg, oracle, nrhs):
+def test_fp16_pair_cg_epilogues_identical(ctx, ctx_single, ctx_pair, clg, oracle, nrhs):
     """The fused CGNE iteration with paired hops and epilogues (CgHopAlpha,
     CgHopUpdate over two right-hand sides per block) runs the same iterations
-    and gives the same solutions as the one-rhs kernels."""
+    and gives the same solutions as the one-rhs kernels, and so does the
+    default context with the form its autotuner chose."""
     res = []
-    for c in (ctx, ctx_pair):
+    for c in (ctx_single, ctx_pair, ctx):
         lat = clg.Lattice(c, (8, 8, 8, 16))
         U = clg.CFieldGaugeSU3(lat)
         U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
@@ -126,10 +142,11 @@ def test_fp16_pair_cg_epilogues_identical(ctx, ctx_pair, clg, oracle, nrhs):
         infos = S.Solve(x, b, U, clg.EFO_F_D)
         res.append(([i["iterations"] for i in infos], [x.to_numpy(r) for r in range(nrhs)], U.CopyDataOut(),
                     [b.to_numpy(r) for r in range(nrhs)]))
-    assert res[0][0] == res[1][0]
+    assert res[0][0] == res[1][0] == res[2][0]
     op = oracle.Operator("WILSON_D", (8, 8, 8, 16), res[0][2], KAPPA)
     for r in range(nrhs):
         np.testing.assert_array_equal(res[0][1][r], res[1][1][r])
+        np.testing.assert_array_equal(res[0][1][r], res[2][1][r])
         assert op.true_residual(res[0][3][r], res[0][1][r]) <= 1e-10
 
 
