@@ -231,6 +231,23 @@ def time_hops(clg, ctx, lat, U, prec, stream, reps=60, nrhs=1):
     return t, launches
 
 
+def hop_form(ctx, prec, Vh, nrhs):
+    """The Wilson hop kernel the autotuner chose for D_eo at this size."""
+    key = f"wilson_p{prec}_d0_V{Vh}_n{nrhs}_r{12 if prec == 1 else 0}"
+    tuned = ctx.tuned()
+    pname = {0: "P64", 1: "P32", 2: "P16"}[prec]
+    if key + "_auto" in tuned:
+        bs, v = tuned[key + "_auto"]
+        if v >= 16:
+            return (f"wilson_hop_tile16_kernel (32 sites x {nrhs} rhs per block, links staged once in shared memory; "
+                    f"{bs // 32} warps, {'80-register cap' if v == 17 else 'uncapped'})")
+        if v >= 8:
+            return f"wilson_hop_pair_kernel (2 rhs per thread; block {bs}, variant {v - 8})"
+        return f"wilson_hop_kernel<P16,12-real> (1 rhs per thread; block {bs}, variant {v})"
+    bs, v = tuned.get(key, (None, None))
+    return f"wilson_hop_kernel<{pname},12-real> (block {bs}, variant {v})"
+
+
 def ours(args, world, rank, local):
     import torch
 
@@ -363,7 +380,7 @@ def ours(args, world, rank, local):
             traffic = ent.get("bytes_per_launch")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic,
-            "kernel": f"wilson_hop_kernel<{'P32' if inner == clg.SINGLE else 'P16'},12-real>, {nrhs} rhs per launch",
+            "kernel": hop_form(ctx, inner, Vh, nrhs) + f", {nrhs} rhs per launch",
             "bytes_per_launch": hop_alg, "launch_us": round(t_hop * 1e6, 2), "peak_source": peak_kind,
             "bytes_model": ("one input and one output spinor per rhs and output site, the 8 links once per site "
                             "for all rhs of the launch")}

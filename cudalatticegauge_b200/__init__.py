@@ -81,6 +81,7 @@ SIGNATURES = [
     ("clg_status_string", C.c_char_p, [_S]),
     ("clg_last_error", C.c_char_p, [_P]),
     ("clg_context_kernel_count", _S, [_P, C.POINTER(_I64)]),
+    ("clg_context_tuned", _S, [_P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("clg_lattice_create", _S, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_P)]),
     ("clg_lattice_destroy", _S, [_P]),
     ("clg_gauge_create", _S, [_P, C.POINTER(_P)]),
@@ -181,6 +182,18 @@ class Context:
         n = C.c_int64()
         self.check(self.lib.clg_context_kernel_count(self.h, C.byref(n)), "kernel_count")
         return n.value
+
+    def tuned(self) -> dict:
+        """The autotuner's choices: kernel key -> (block size, variant)."""
+        need = C.c_size_t()
+        self.check(self.lib.clg_context_tuned(self.h, None, 0, C.byref(need)), "clg_context_tuned")
+        buf = C.create_string_buffer(need.value + 1)
+        self.check(self.lib.clg_context_tuned(self.h, buf, need.value + 1, C.byref(need)), "clg_context_tuned")
+        out = {}
+        for line in buf.value.decode().splitlines():
+            k, v = line.rsplit("=", 1)
+            out[k] = (int(v) & 0xFFFF, int(v) >> 16)
+        return out
 
     def close(self):
         if getattr(self, "h", None):

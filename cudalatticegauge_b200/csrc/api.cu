@@ -358,6 +358,13 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
       ctx->hop_pair_mode = t[0] == '1' ? 1 : (t[0] == '0' ? 0 : 2);
     }
   }
+  if (const char* t = std::getenv("CLG_HOP_TILE")) {
+    int warps = 0, variant = -1;
+    if (std::sscanf(t, "%d:%d", &warps, &variant) == 2 && warps >= 1 && warps <= 8 && (variant == 0 || variant == 1)) {
+      ctx->hop_pair_mode = 3;
+      ctx->hop_tile_config = (32 * warps) | ((16 + variant) << 16);
+    }
+  }
   if (const char* t = std::getenv("CLG_PDL")) ctx->pdl = t[0] != '0';
   if (const char* t = std::getenv("CLG_HOP_CONFIG")) {
     int variant = -1, bs = 0;
@@ -374,8 +381,9 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
     }
     ctx->own_stream = true;
   }
-  if (dalloc(ctx, (void**)&ctx->red_counter, sizeof(unsigned)) ||
-      cudaMemset(ctx->red_counter, 0, sizeof(unsigned)) != cudaSuccess || ensure_reduction(ctx, 65536)) {
+  if (dalloc(ctx, (void**)&ctx->red_counter, sizeof(unsigned) * (1 + kRedGroups)) ||
+      cudaMemset(ctx->red_counter, 0, sizeof(unsigned) * (1 + kRedGroups)) != cudaSuccess ||
+      ensure_reduction(ctx, 65536)) {
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     dfree(ctx->red_counter);
     delete ctx;
@@ -436,6 +444,19 @@ const char* clg_last_error(clg_context ctx) { return ctx ? ctx->last_error.c_str
 clg_status clg_context_kernel_count(clg_context ctx, int64_t* count) {
   if (!ctx || !count) return CLG_ERR_BAD_ARG;
   *count = ctx->kernels;
+  return CLG_SUCCESS;
+}
+
+clg_status clg_context_tuned(clg_context ctx, char* buf, size_t len, size_t* needed) {
+  if (!ctx || !needed || (len && !buf)) return CLG_ERR_BAD_ARG;
+  std::string out;
+  for (const auto& kv : ctx->tuned) out += kv.first + "=" + std::to_string(kv.second) + "\n";
+  *needed = out.size();
+  if (len) {
+    const size_t n = std::min(len - 1, out.size());
+    std::memcpy(buf, out.data(), n);
+    buf[n] = 0;
+  }
   return CLG_SUCCESS;
 }
 

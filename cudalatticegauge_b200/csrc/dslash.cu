@@ -85,10 +85,34 @@ cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagge
                 : launch_pdl(ctx, wilson_hop_batch_kernel<P, RECON, false>, grid, dim3(bs), 0, a);
 }
 
-// The autotuner's choice between one and two right-hand sides per thread for
-// the FP16 Wilson hop: single-rhs configurations keep their variant (0..2),
-// paired ones carry variant 8 + the pair variant.  The winner is also recorded
-// under the keys the fused epilogue launches look up.
+// FP16 Wilson hop over a tile of 32 sites for all right-hand sides
+// (wilson_hop_tile16_kernel); config = block size | (16 + v) << 16 with v = 0
+// uncapped, 1 capped at 80 registers
+cudaError_t launch_wilson_tile(clg_context_s* ctx, const HopArgs& a, bool dagger, int cfg) {
+  const int bs = cfg & 0xffff;
+  dim3 grid((unsigned)((a.g.Vh + TILE16 - 1) / TILE16));
+  if ((cfg >> 16) == 17)
+    return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 3>, grid, dim3(bs), 0, a)
+                  : launch_pdl(ctx, wilson_hop_tile16_kernel<false, 3>, grid, dim3(bs), 0, a);
+  return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 2>, grid, dim3(bs), 0, a)
+                : launch_pdl(ctx, wilson_hop_tile16_kernel<false, 2>, grid, dim3(bs), 0, a);
+}
+
+// warps per tile block worth timing for nrhs right-hand sides: 4 and 8, and
+// the divisors of nrhs between 3 and 8 (no warp idles at the end)
+std::vector<int> tile_warps(int nrhs) {
+  std::vector<int> w = {4, 8};
+  for (int d = 3; d <= 8; ++d)
+    if (nrhs % d == 0 && d != 4 && d != 8) w.push_back(d);
+  if (nrhs < 4) w = {nrhs};
+  return w;
+}
+
+// The autotuner's choice of the FP16 Wilson hop's form for two or more
+// right-hand sides: one rhs per thread (config variants 0..2), two per thread
+// (variant 8 + the pair variant) or a tile of sites for all rhs (variants 16,
+// 17).  The winner is recorded under the keys the fused epilogue launches
+// look up (key, key_pair, key_tile).
 cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
   auto it = ctx->tuned.find(key + "_auto");
   int cfg;
@@ -97,6 +121,7 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
   } else {
     auto go = [&](int c) -> cudaError_t {
       const int v = c >> 16;
+      if (v >= 16) return launch_wilson_tile(ctx, a, dagger, c);
       if (v >= 8) {
         ctx->tuned[key + "_pair"] = (c & 0xffff) | ((v - 8) << 16);
         return launch_wilson_pair(ctx, a, dagger, key);
@@ -112,6 +137,10 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
       cand.push_back(bs | (9 << 16));
     }
     cand.push_back(64 | (2 << 16));
+    for (int w : tile_warps(nrhs)) {
+      cand.push_back((32 * w) | (16 << 16));
+      cand.push_back((32 * w) | (17 << 16));
+    }
     // untuned (inside a capture, or the output aliases the xpay source): the
     // one-rhs kernel, and nothing is cached
     if (!ctx->tuning_enabled || !idempotent(a) || stream_capturing(ctx->stream))
@@ -119,9 +148,13 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
     cfg = tune_block(ctx, key + "_auto", true, go, cand);
     ctx->tuned.erase(key);
     ctx->tuned.erase(key + "_pair");
-    if ((cfg >> 16) >= 8) ctx->tuned[key + "_pair"] = (cfg & 0xffff) | (((cfg >> 16) - 8) << 16);
+    ctx->tuned.erase(key + "_tile");
+    const int v = cfg >> 16;
+    if (v >= 16) ctx->tuned[key + "_tile"] = cfg;
+    else if (v >= 8) ctx->tuned[key + "_pair"] = (cfg & 0xffff) | ((v - 8) << 16);
     else ctx->tuned[key] = cfg;
   }
+  if ((cfg >> 16) >= 16) return launch_wilson_tile(ctx, a, dagger, cfg);
   if ((cfg >> 16) >= 8) return launch_wilson_pair(ctx, a, dagger, key);
   return launch_wilson<P16, 12>(ctx, a, dagger, nrhs, key);
 }
@@ -334,6 +367,12 @@ int tuned_hop_pair_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpe
   return it == ctx->tuned.end() ? fallback : it->second;
 }
 
+int tuned_hop_tile_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback) {
+  if (ctx->hop_pair_mode == 3) return ctx->hop_tile_config;
+  auto it = ctx->tuned.find(hop_key(U, s) + "_tile");
+  return it == ctx->tuned.end() ? fallback : it->second;
+}
+
 int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback) {
   auto it = ctx->tuned.find(hop_key(U, s));
   if (it == ctx->tuned.end()) return fallback;
@@ -357,6 +396,8 @@ clg_status hop(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s) {
       e = wilson ? launch_wilson<P32, 12>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 12>(ctx, a, s.nrhs, key);
     else
       e = wilson ? launch_wilson<P32, 18>(ctx, a, s.dagger, s.nrhs, key) : launch_staggered<P32, 18>(ctx, a, s.nrhs, key);
+  } else if (wilson && s.nrhs >= 2 && ctx->hop_pair_mode == 3) {
+    e = launch_wilson_tile(ctx, a, s.dagger, ctx->hop_tile_config);
   } else if (wilson && s.nrhs >= 2 && ctx->hop_pair_mode == 1) {
     e = launch_wilson_pair(ctx, a, s.dagger, key);
   } else if (wilson && s.nrhs >= 2 && ctx->hop_pair_mode == 2 && ctx->hop_config < 0) {

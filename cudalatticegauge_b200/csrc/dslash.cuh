@@ -126,13 +126,45 @@ __device__ __forceinline__ __half2 h2_cmac(__half2 ur, __half2 ui, uint32_t v, _
   return __hfma2(ui, as_h2(UDAG ? h2_mul_i<3>(v) : h2_mul_i<1>(v)), o);
 }
 
-// The FP16 counterpart of wilson_hop_dir: the spin projection, the third link
-// row (conj(row0 x row1)) and the two colour mat-vecs run on half2 words;
-// only the 6 projected products are converted, and they are accumulated in
-// FP32 with the factor s (boundary sign times the neighbour's site norm).
+// The third row of an FP16 12-real link, row2 = conj(row0 x row1), on half2
+// words: u[0..5] are rows 0 and 1 (one complex number per word), u[6..8] are
+// written.
+__device__ __forceinline__ void link16_third_row(uint32_t u[9]) {
+  // u6 = conj(u1 u5 - u2 u4), u7 = conj(u2 u3 - u0 u5), u8 = conj(u0 u4 - u1 u3)
+  const __half2 zero = __float2half2_rn(0.f);
+  auto cross = [&](int a, int b, int c, int d) -> uint32_t {
+    __half2 t = h2_cmac<false>(__low2half2(as_h2(u[a])), __high2half2(as_h2(u[a])), u[b], zero);
+    const uint32_t nd = u[d] ^ 0x80008000u;  // -u[d]
+    t = h2_cmac<false>(__low2half2(as_h2(u[c])), __high2half2(as_h2(u[c])), nd, t);
+    return as_u32(t) ^ 0x80000000u;  // conjugate
+  };
+  // u6 and u7 together, "planar" across the two: lane 0 carries u1 u5 - u2 u4,
+  // lane 1 u2 u3 - u0 u5, so the products need no broadcasts or swaps
+  const __half2 X = as_h2(__byte_perm(u[1], u[2], 0x5410)), Xi = as_h2(__byte_perm(u[1], u[2], 0x7632));
+  const __half2 Y = as_h2(__byte_perm(u[5], u[3], 0x5410)), Yi = as_h2(__byte_perm(u[5], u[3], 0x7632));
+  const __half2 Z = as_h2(__byte_perm(u[2], u[0], 0x5410)), Zi = as_h2(__byte_perm(u[2], u[0], 0x7632));
+  const __half2 W = as_h2(__byte_perm(u[4], u[5], 0x5410)), Wi = as_h2(__byte_perm(u[4], u[5], 0x7632));
+  __half2 re = __hmul2(X, Y);
+  re = __hfma2(__hneg2(Xi), Yi, re);
+  re = __hfma2(__hneg2(Z), W, re);
+  re = __hfma2(Zi, Wi, re);
+  __half2 nim = __hmul2(Z, Wi);  // minus the imaginary parts: the conjugate directly
+  nim = __hfma2(Zi, W, nim);
+  nim = __hfma2(__hneg2(X), Yi, nim);
+  nim = __hfma2(__hneg2(Xi), Y, nim);
+  u[6] = __byte_perm(as_u32(re), as_u32(nim), 0x5410);
+  u[7] = __byte_perm(as_u32(re), as_u32(nim), 0x7632);
+  u[8] = cross(0, 4, 1, 3);
+}
+
+// The FP16 counterpart of wilson_hop_dir with the whole link given (u[9], one
+// complex number per half2 word): the spin projection and the two colour
+// mat-vecs run on half2 words; only the 6 projected products are converted,
+// and they are accumulated in FP32 with the factor s (boundary sign times the
+// neighbour's site norm).
 template <int MU, int SGN, bool UDAG>
-__device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packed16& p, const PackedLink16& l,
-                                                 float s) {
+__device__ __forceinline__ void wilson_hop_dir16_u(cpx<float> acc[12], const Packed16& p, const uint32_t (&u)[9],
+                                                   float s) {
   constexpr int add = SGN < 0 ? 2 : 0;
   uint32_t w[12];
 #pragma unroll
@@ -147,34 +179,6 @@ __device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packe
   for (int c = 0; c < 3; ++c) {
     h0[c] = as_u32(__hadd2(as_h2(w[c]), as_h2(h2_mul_i<gz4(MU, 0) + add>(w[3 * gperm(MU, 0) + c]))));
     h1[c] = as_u32(__hadd2(as_h2(w[3 + c]), as_h2(h2_mul_i<gz4(MU, 1) + add>(w[3 * gperm(MU, 1) + c]))));
-  }
-  uint32_t u[9] = {l.a.x, l.a.y, l.a.z, l.a.w, l.b.x, l.b.y, 0u, 0u, 0u};
-  {
-    // row2 = conj(row0 x row1): u6 = conj(u1 u5 - u2 u4), u7 = conj(u2 u3 - u0 u5), u8 = conj(u0 u4 - u1 u3)
-    const __half2 zero = __float2half2_rn(0.f);
-    auto cross = [&](int a, int b, int c, int d) -> uint32_t {
-      __half2 t = h2_cmac<false>(__low2half2(as_h2(u[a])), __high2half2(as_h2(u[a])), u[b], zero);
-      const uint32_t nd = u[d] ^ 0x80008000u;  // -u[d]
-      t = h2_cmac<false>(__low2half2(as_h2(u[c])), __high2half2(as_h2(u[c])), nd, t);
-      return as_u32(t) ^ 0x80000000u;  // conjugate
-    };
-    // u6 and u7 together, "planar" across the two: lane 0 carries u1 u5 - u2 u4,
-    // lane 1 u2 u3 - u0 u5, so the products need no broadcasts or swaps
-    const __half2 X = as_h2(__byte_perm(u[1], u[2], 0x5410)), Xi = as_h2(__byte_perm(u[1], u[2], 0x7632));
-    const __half2 Y = as_h2(__byte_perm(u[5], u[3], 0x5410)), Yi = as_h2(__byte_perm(u[5], u[3], 0x7632));
-    const __half2 Z = as_h2(__byte_perm(u[2], u[0], 0x5410)), Zi = as_h2(__byte_perm(u[2], u[0], 0x7632));
-    const __half2 W = as_h2(__byte_perm(u[4], u[5], 0x5410)), Wi = as_h2(__byte_perm(u[4], u[5], 0x7632));
-    __half2 re = __hmul2(X, Y);
-    re = __hfma2(__hneg2(Xi), Yi, re);
-    re = __hfma2(__hneg2(Z), W, re);
-    re = __hfma2(Zi, Wi, re);
-    __half2 nim = __hmul2(Z, Wi);  // minus the imaginary parts: the conjugate directly
-    nim = __hfma2(Zi, W, nim);
-    nim = __hfma2(__hneg2(X), Yi, nim);
-    nim = __hfma2(__hneg2(Xi), Y, nim);
-    u[6] = __byte_perm(as_u32(re), as_u32(nim), 0x5410);
-    u[7] = __byte_perm(as_u32(re), as_u32(nim), 0x7632);
-    u[8] = cross(0, 4, 1, 3);
   }
   const __half2 zero = __float2half2_rn(0.f);
   __half2 g0[3] = {zero, zero, zero}, g1[3] = {zero, zero, zero};
@@ -211,6 +215,15 @@ __device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packe
       }
     }
   }
+}
+
+// The same with the link as stored (12-real): the third row is rebuilt first.
+template <int MU, int SGN, bool UDAG>
+__device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packed16& p, const PackedLink16& l,
+                                                 float s) {
+  uint32_t u[9] = {l.a.x, l.a.y, l.a.z, l.a.w, l.b.x, l.b.y, 0u, 0u, 0u};
+  link16_third_row(u);
+  wilson_hop_dir16_u<MU, SGN, UDAG>(acc, p, u, s);
 }
 
 struct NbrInfo {
@@ -426,14 +439,15 @@ __global__ void __launch_bounds__(256, P == P64 ? 2 : 3) wilson_hop_batch_kernel
 // The hop with a fused epilogue E (used by the Krylov solvers):
 //   E::STORE      the result is stored to a.out (else it only feeds E::site)
 //   E::NRED       doubles reduced over the grid per rhs, E::finalize(rhs, tot)
-//                 runs on the device in the last block (grid_reduce_finalize)
+//                 runs on the device in the last block (grid_reduce_finalize2)
 //   E::site(rhs, h, acc, red)   per-site work on the result in registers
 // Every thread reaches the block reduction: out-of-range sites contribute
 // zero; a block of a skipped (finished) right-hand side only takes its ticket,
 // and E::finalize ignores such right-hand sides.
 template <int P, int RECON, bool DAGGER, int MAXT, int MINB, class E, bool BATCH = false>
 __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E e, double* partials,
-                                                                    unsigned* counter) {
+                                                                    double* gpart, unsigned* counter,
+                                                                    unsigned group) {
   using AT = typename AccT<P>::T;
   const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
   const unsigned slot = blockIdx.x / (unsigned)a.nrhs;
@@ -458,8 +472,11 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_epi_kernel(HopArgs a, E
       e.site(rhs, h, acc, red);
     }
   }
-  grid_reduce_finalize<E::NRED>(red, e, rhs, slot, gridDim.x / (unsigned)a.nrhs, a.nrhs, partials, counter,
-                                !skipped, BATCH ? a.seg_vh : nullptr);
+  const int rr[1] = {rhs};
+  const bool cc[1] = {!skipped}, hh[1] = {true};
+  grid_reduce_finalize2<E::NRED, 1>(red, e, rr, cc, hh, (unsigned)rhs, (unsigned)a.nrhs, slot,
+                                    gridDim.x / (unsigned)a.nrhs, a.nrhs, group, partials, gpart, counter,
+                                    BATCH ? a.seg_vh : nullptr);
 }
 
 // ---------------------------------------------------------------- FP16, two right-hand sides per thread
@@ -665,7 +682,8 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_kernel(HopArgs a) 
 // side of the pair; the block reduces both right-hand sides' values.
 template <bool DAGGER, int MAXT, int MINB, class E>
 __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_epi_kernel(HopArgs a, E e, double* partials,
-                                                                         unsigned* counter) {
+                                                                         double* gpart, unsigned* counter,
+                                                                         unsigned group) {
   const unsigned npairs = (unsigned)(a.nrhs + 1) / 2u;
   int rhs0, rhs1;
   bool has1;
@@ -691,8 +709,180 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_epi_kernel(HopArgs
       e.site(rhs1, h, acc1, red + E::NRED);
     }
   }
-  grid_reduce_finalize_pair<E::NRED>(red, e, rhs0, rhs1, run0, run1, slot, gridDim.x / npairs, gridDim.x, a.nrhs,
-                                     partials, counter);
+  const int rr[2] = {rhs0, rhs1};
+  const bool cc[2] = {run0, run1}, hh[2] = {true, has1};
+  grid_reduce_finalize2<E::NRED, 2>(red, e, rr, cc, hh, (unsigned)(rhs0 / 2), npairs, slot, gridDim.x / npairs,
+                                    a.nrhs, group, partials, gpart, counter);
+}
+
+// ---------------------------------------------------------------- FP16, a tile of sites for every right-hand side
+// The multi-right-hand-side FP16 hop with the links of a tile of 32 output
+// sites loaded and completed (third row) once for all right-hand sides.  The
+// block first stages, for its 32 sites, the neighbour indices with the
+// boundary signs and the 8 links of each site (U_mu(x), U_mu(x - mu)) as
+// 18-real half2 words in shared memory; then its warps loop over the
+// right-hand sides (warp w takes rhs w, w + nwarps, ...), each lane computing
+// one output site per right-hand side with the links read from shared memory.
+// Per site and rhs this drops the link loads from global memory, the third-row
+// rebuild and the neighbour arithmetic of the one-rhs kernel, and each link
+// crosses DRAM once per launch whatever the L2 holds.  The arithmetic per site
+// and rhs is wilson_hop_dir16_u's, so the results are bit-identical to the
+// one-rhs kernel.
+constexpr int TILE16 = 32;
+struct Tile16 {
+  uint4 la[8][TILE16];     // link words 0-3; direction d < 4: U_d(x), d >= 4: U_(d-4)(x - mu)
+  uint4 lb[8][TILE16];     // words 4-7
+  uint32_t lc[8][TILE16];  // word 8
+  int nb[8][TILE16];       // checkerboard index of x + mu (d < 4), of x - mu (d >= 4)
+  uint32_t neg[TILE16];    // bit d: the boundary sign of direction d is -1
+};
+
+// The neighbours of the tile's sites (geometry only: no memory is read, so
+// this runs before the wait on the previous kernel)
+__device__ __forceinline__ void tile16_neighbours(const HopArgs& a, int64_t h0, Tile16& t) {
+  for (int i = threadIdx.x; i < TILE16; i += blockDim.x) {
+    const int64_t h = h0 + i;
+    uint32_t neg = 0;
+    if (h < a.g.Vh) {
+      NbrInfo nb;
+      int c[4];
+      neighbours(a.g, a.out_parity, h, nb, c);
+#pragma unroll
+      for (int mu = 0; mu < 4; ++mu) {
+        t.nb[mu][i] = nb.hf[mu];
+        t.nb[4 + mu][i] = nb.hb[mu];
+        neg |= (nb.sf[mu] < 0.f ? 1u : 0u) << mu;
+        neg |= (nb.sb[mu] < 0.f ? 1u : 0u) << (4 + mu);
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 8; ++d) t.nb[d][i] = 0;
+    }
+    t.neg[i] = neg;
+  }
+}
+
+// The tile's links, third row rebuilt (after tile16_neighbours and a barrier)
+__device__ __forceinline__ void tile16_links(const HopArgs& a, int64_t h0, Tile16& t) {
+  for (int k = threadIdx.x; k < 8 * TILE16; k += blockDim.x) {
+    const int d = k / TILE16, i = k % TILE16;
+    const int64_t h = h0 + i;
+    uint32_t u[9] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    if (h < a.g.Vh) {
+      PackedLink16 l;
+      if (d < 4)
+        load_packed_link16(a.U_here, d, a.g.Vh, h, l);
+      else
+        load_packed_link16(a.U_there, d - 4, a.g.Vh, t.nb[d][i], l);
+      u[0] = l.a.x; u[1] = l.a.y; u[2] = l.a.z; u[3] = l.a.w; u[4] = l.b.x; u[5] = l.b.y;
+      link16_third_row(u);
+    }
+    t.la[d][i] = make_uint4(u[0], u[1], u[2], u[3]);
+    t.lb[d][i] = make_uint4(u[4], u[5], u[6], u[7]);
+    t.lc[d][i] = u[8];
+  }
+}
+
+__device__ __forceinline__ void tile16_link(const Tile16& t, int d, int i, uint32_t (&u)[9]) {
+  const uint4 x = t.la[d][i], y = t.lb[d][i];
+  u[0] = x.x; u[1] = x.y; u[2] = x.z; u[3] = x.w;
+  u[4] = y.x; u[5] = y.y; u[6] = y.z; u[7] = y.w;
+  u[8] = t.lc[d][i];
+}
+
+// H in at tile site i (output site h) of right-hand side rhs, then the finish
+template <bool DAGGER>
+__device__ __forceinline__ void wilson_hop_site_tile16(const HopArgs& a, const Tile16& t, int i, int rhs, int64_t h,
+                                                       cpx<float> acc[12]) {
+  const int64_t Vh = a.g.Vh;
+  const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
+  const float* in_norm = a.in_norm + rhs * a.in_nstride;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = mk<float>(0.f, 0.f);
+  const uint32_t neg = t.neg[i];
+  constexpr int SF = DAGGER ? 1 : -1;
+  constexpr int SB = -SF;
+#define CLG_TILE_DIR16(MU)                                                   \
+  {                                                                          \
+    Packed16 pf, pb;                                                         \
+    load_packed16(in, in_norm, Vh, t.nb[MU][i], pf);                         \
+    load_packed16(in, in_norm, Vh, t.nb[4 + MU][i], pb);                     \
+    uint32_t u[9];                                                           \
+    tile16_link(t, MU, i, u);                                                \
+    wilson_hop_dir16_u<MU, SF, false>(acc, pf, u, (neg >> MU) & 1u ? -pf.n : pf.n);       \
+    tile16_link(t, 4 + MU, i, u);                                            \
+    wilson_hop_dir16_u<MU, SB, true>(acc, pb, u, (neg >> (4 + MU)) & 1u ? -pb.n : pb.n);  \
+  }
+  CLG_TILE_DIR16(0)
+  CLG_TILE_DIR16(1)
+  CLG_TILE_DIR16(2)
+  CLG_TILE_DIR16(3)
+#undef CLG_TILE_DIR16
+  wilson_hop_finish<P16>(a, rhs, h, acc);
+}
+
+// One block per tile of 32 output sites, blockDim = 32 x (warps sharing the
+// right-hand sides); MINB 2 leaves the registers uncapped (128), 3 caps at 80.
+template <bool DAGGER, int MINB>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_kernel(HopArgs a) {
+  __shared__ Tile16 t;
+  const int64_t h0 = (int64_t)blockIdx.x * TILE16;
+  pdl_launch_dependents();
+  tile16_neighbours(a, h0, t);
+  pdl_wait();
+  __syncthreads();
+  tile16_links(a, h0, t);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int64_t h = h0 + lane;
+  if (h >= a.g.Vh) return;  // no barrier follows
+  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+    if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
+    cpx<float> acc[12];
+    wilson_hop_site_tile16<DAGGER>(a, t, lane, rhs, h, acc);
+    wilson_hop_store<P16>(a, rhs, h, acc);
+  }
+}
+
+// The tile form of wilson_hop_epi_kernel: per right-hand side the warp
+// reduces its 32 sites and writes the tile's partial (slot = tile); the tiles
+// then reduce in two levels (tile_reduce_finalize).
+template <bool DAGGER, int MINB, class E>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_epi_kernel(HopArgs a, E e, double* partials,
+                                                                          double* gpart, unsigned* counter,
+                                                                          unsigned group) {
+  __shared__ Tile16 t;
+  const int64_t h0 = (int64_t)blockIdx.x * TILE16;
+  pdl_launch_dependents();
+  tile16_neighbours(a, h0, t);
+  pdl_wait();
+  __syncthreads();
+  tile16_links(a, h0, t);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int64_t h = h0 + lane;
+  const unsigned nslots = gridDim.x;
+  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+    if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
+    double red[E::NRED];
+#pragma unroll
+    for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
+    if (h < a.g.Vh) {
+      cpx<float> acc[12];
+      wilson_hop_site_tile16<DAGGER>(a, t, lane, rhs, h, acc);
+      if constexpr (E::STORE) wilson_hop_store<P16>(a, rhs, h, acc);
+      e.site(rhs, h, acc, red);
+    }
+#pragma unroll
+    for (int k = 0; k < E::NRED; ++k) {
+      double v = red[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) partials[((int64_t)rhs * nslots + blockIdx.x) * E::NRED + k] = v;
+    }
+    if (lane == 0) __threadfence();
+  }
+  tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
 }
 
 template <int P, int RECON>

@@ -65,6 +65,9 @@ struct clg_context_s {
   int num_sms = 148;
   int64_t kernels = 0;
   // reduction scratch (device): partial sums and the arrival counter
+  // reduction scratch: block partials (and the group totals of the two-level
+  // reductions) in red_partials; red_counter[0] is the grid ticket, and
+  // red_counter[1 .. kRedGroups] the group tickets (grid_reduce_finalize2)
   double* red_partials = nullptr;
   int64_t red_capacity = 0;  // doubles
   unsigned int* red_counter = nullptr;
@@ -94,14 +97,20 @@ struct clg_context_s {
   bool fused_cg = true;
   // FP16 Wilson hops over two or more right-hand sides: one right-hand side
   // per thread (the right-hand sides interleaved over the blocks, links shared
-  // through L2) or two per thread (wilson_hop_pair_kernel: one link load and
-  // reconstruction per pair, planar half2 arithmetic).  hop_pair_mode 2 (the
-  // default) lets the autotuner time both forms per operator and lattice (the
-  // right-hand-side-per-thread axis); CLG_HOP_PAIR=0 keeps one, =1 forces two,
+  // through L2), two per thread (wilson_hop_pair_kernel: one link load and
+  // reconstruction per pair, planar half2 arithmetic) or a tile of 32 sites
+  // for all right-hand sides (wilson_hop_tile16_kernel: links staged once per
+  // tile in shared memory).  hop_pair_mode 2 (the default) lets the autotuner
+  // time the three forms per operator and lattice (the right-hand-side-per-
+  // thread and site-tiling axes); CLG_HOP_PAIR=0 keeps one, =1 forces two,
   // "<variant>:<block>" pins the paired launch (variant 0 uncapped, 1 capped at
   // 128 registers).  Measured on 32^3x16 / 32^3x32 the two are within a few
   // per cent (13.6 against 13.4 us per rhs at 8 rhs, 27.2 against 27.5 at 28).
+  // CLG_HOP_TILE="<warps>:<variant>" forces the tile form (mode 3;
+  // wilson_hop_tile16_kernel, variant 0 uncapped, 1 capped at 80 registers);
+  // the autotuner of mode 2 times it with the other two
   int hop_pair_mode = 2;
+  int hop_tile_config = -1;
   // set by clg_solve_lattices for the duration of its solve: the per-rhs
   // checkerboard sizes (device) of the padded batch, whose site kernels skip
   // the padding (launches with this stride and right-hand-side count)
@@ -203,6 +212,19 @@ clg_status noalloc_prepare(clg_context_s* ctx);
 clg_status dalloc(clg_context_s* ctx, void** p, size_t bytes);
 void dfree(void* p);
 clg_status ensure_reduction(clg_context_s* ctx, int64_t doubles);
+// Group tickets of the two-level reductions, and the group size for nunits x
+// nslots blocks (at least 64 slots, doubled until the tickets fit)
+constexpr int64_t kRedGroups = 65536;
+inline unsigned red_group(int64_t nslots, int64_t nunits) {
+  int64_t g = 64;
+  while (((nslots + g - 1) / g) * nunits > kRedGroups) g *= 2;
+  return (unsigned)g;
+}
+// scratch doubles of a two-level reduction: block partials then group totals
+inline int64_t red2_doubles(int64_t nslots, int nrhs, int nunits, int nred) {
+  const int64_t ng = (nslots + red_group(nslots, nunits) - 1) / red_group(nslots, nunits);
+  return (nslots + ng) * nrhs * nred;
+}
 
 // ------------------------------------------------------------ launch helpers
 bool stream_capturing(cudaStream_t s);
@@ -288,6 +310,9 @@ clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec
 int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
 // the tuned launch configuration (block | variant << 16) of the paired FP16 hop
 int tuned_hop_pair_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
+// the tile form's configuration (block | variant << 16), when the tile form is
+// forced or was the autotuner's choice for this hop
+int tuned_hop_tile_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
 clg_status gauge_prepare(clg_gauge_s* U, int prec);  // builds the FP32 / FP16 copies on first use
 // address range of the link copy the hops of precision `prec` read (nullptr, 0 if none)
 void gauge_link_range(const clg_gauge_s* U, int prec, const void** base, size_t* bytes);

@@ -569,23 +569,43 @@ template <bool DAG, class E>
 cudaError_t launch_hop_pair_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int cfg) {
   const int bs = cfg & 0xffff;
   const unsigned npairs = (unsigned)(a.nrhs + 1) / 2u;
-  dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * npairs));
+  const int64_t nslots = (a.g.Vh + bs - 1) / bs;
+  dim3 grid((unsigned)(nslots * npairs));
+  const unsigned group = red_group(nslots, npairs);
+  double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
   if ((cfg >> 16) == 1)
     return launch_pdl(ctx, wilson_hop_pair_epi_kernel<DAG, 256, 2, E>, grid, dim3(bs), 0, a, e, ctx->red_partials,
-                      ctx->red_counter);
+                      gpart, ctx->red_counter, group);
   return launch_pdl(ctx, wilson_hop_pair_epi_kernel<DAG, 256, 1, E>, grid, dim3(bs), 0, a, e, ctx->red_partials,
-                    ctx->red_counter);
+                    gpart, ctx->red_counter, group);
+}
+
+// the tile form (wilson_hop_tile16_epi_kernel): config as in launch_wilson_tile
+template <bool DAG, class E>
+cudaError_t launch_hop_tile_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int cfg) {
+  const int bs = cfg & 0xffff;
+  const int64_t nslots = (a.g.Vh + TILE16 - 1) / TILE16;
+  const unsigned group = red_group(nslots, 1);
+  double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
+  if ((cfg >> 16) == 17)
+    return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 3, E>, dim3((unsigned)nslots), dim3(bs), 0, a, e,
+                      ctx->red_partials, gpart, ctx->red_counter, group);
+  return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 2, E>, dim3((unsigned)nslots), dim3(bs), 0, a, e,
+                    ctx->red_partials, gpart, ctx->red_counter, group);
 }
 
 template <int P, int RECON, bool DAG, class E>
 cudaError_t launch_hop_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int bs) {
-  dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * a.nrhs));
+  const int64_t nslots = (a.g.Vh + bs - 1) / bs;
+  dim3 grid((unsigned)(nslots * a.nrhs));
+  const unsigned group = red_group(nslots, a.nrhs);
+  double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
   constexpr int MINB = P == P64 ? 1 : 3;
   if (a.seg)  // a batch of lattices
     return launch_pdl(ctx, wilson_hop_epi_kernel<P, RECON, DAG, 256, MINB, E, true>, grid, dim3(bs), 0, a, e,
-                      ctx->red_partials, ctx->red_counter);
+                      ctx->red_partials, gpart, ctx->red_counter, group);
   return launch_pdl(ctx, wilson_hop_epi_kernel<P, RECON, DAG, 256, MINB, E>, grid, dim3(bs), 0, a, e,
-                    ctx->red_partials, ctx->red_counter);
+                    ctx->red_partials, gpart, ctx->red_counter, group);
 }
 
 // out_e = in_e - kappa^2 H_eo^(dag) t_o with epilogue e (E::STORE decides
@@ -616,21 +636,29 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
   HopSpec plain = s;
   plain.x = nullptr;
   const int bs = tuned_hop_block(ctx, w.U, plain, P == P64 ? 64 : 128);
-  const int64_t nblk = ((w.Vh + bs - 1) / bs) * w.nrhs;
   if constexpr (P == P16) {
+    const int tcfg = w.nrhs >= 2 && !a.seg ? tuned_hop_tile_config(ctx, w.U, plain, -1) : -1;
+    if (tcfg >= 0) {
+      const int64_t nslots = (w.Vh + TILE16 - 1) / TILE16;
+      if (clg_status st = ensure_reduction(ctx, red2_doubles(nslots, w.nrhs, 1, E::NRED))) return st;
+      const cudaError_t terr = dag ? launch_hop_tile_epi<true>(ctx, a, e, tcfg) : launch_hop_tile_epi<false>(ctx, a, e, tcfg);
+      if (terr != cudaSuccess) return ctx->fail(cuda_status(terr), std::string("fused hop: ") + cudaGetErrorString(terr));
+      return CLG_SUCCESS;
+    }
     const int pcfg = tuned_hop_pair_config(ctx, w.U, plain, -1);
     const bool pair = ctx->hop_pair_mode == 1 || (ctx->hop_pair_mode == 2 && pcfg >= 0);
     if (w.nrhs >= 2 && pair && !a.seg) {
       const int cfg = pcfg >= 0 ? pcfg : 128;
       const int pbs = cfg & 0xffff;
       // partials are indexed [rhs][slot]: nslots x nrhs of them
-      if (clg_status st = ensure_reduction(ctx, ((w.Vh + pbs - 1) / pbs) * w.nrhs * E::NRED)) return st;
+      if (clg_status st = ensure_reduction(ctx, red2_doubles((w.Vh + pbs - 1) / pbs, w.nrhs, (w.nrhs + 1) / 2, E::NRED)))
+        return st;
       const cudaError_t perr = dag ? launch_hop_pair_epi<true>(ctx, a, e, cfg) : launch_hop_pair_epi<false>(ctx, a, e, cfg);
       if (perr != cudaSuccess) return ctx->fail(cuda_status(perr), std::string("fused hop: ") + cudaGetErrorString(perr));
       return CLG_SUCCESS;
     }
   }
-  if (clg_status st = ensure_reduction(ctx, nblk * E::NRED)) return st;
+  if (clg_status st = ensure_reduction(ctx, red2_doubles((w.Vh + bs - 1) / bs, w.nrhs, w.nrhs, E::NRED))) return st;
   cudaError_t err;
   if constexpr (P == P64) {
     err = dag ? launch_hop_epi<P, 18, true>(ctx, a, e, bs) : launch_hop_epi<P, 18, false>(ctx, a, e, bs);

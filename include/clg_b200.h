@@ -120,6 +120,12 @@ const char* clg_status_string(clg_status s);
 const char* clg_last_error(clg_context ctx);
 /* number of kernels this context has launched (all kinds), for accounting */
 clg_status clg_context_kernel_count(clg_context ctx, int64_t* count);
+/* the autotuner's choices so far, one "<kernel key>=<config>" per line (config
+ * = block size | variant << 16); writes at most len bytes including the
+ * terminating zero and stores the full length (without it) in *needed.  No
+ * reference counterpart: the reference launches with fixed block sizes
+ * (Core/CudaHelper.cu). */
+clg_status clg_context_tuned(clg_context ctx, char* buf, size_t len, size_t* needed);
 
 /* ------------------------------------------------------------------ lattice
  * Replaces InitialLatticeAndConstant (Core/CLGLibManager.cpp:52-348) and the

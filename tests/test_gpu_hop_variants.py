@@ -181,3 +181,71 @@ def test_fp16_pair_variants_vs_oracle(clg, oracle, cfg):
             assert rel(f.to_numpy(r)[pm == 0], want) < 5e-3
     finally:
         c.close()
+
+
+TILE_CONFIGS = ["8:0", "8:1", "4:1", "3:1"]
+
+
+@pytest.fixture(scope="module")
+def ctx_tiles(clg):
+    """Contexts whose FP16 Wilson hops over two or more right-hand sides use
+    the tile form (CLG_HOP_TILE="<warps>:<variant>": 32 sites per block, the
+    links staged once in shared memory for all right-hand sides)."""
+    made = {}
+
+    def get(cfg):
+        if cfg not in made:
+            made[cfg] = _context_with(clg, "CLG_HOP_TILE", cfg)
+        return made[cfg]
+
+    yield get
+    for c in made.values():
+        c.close()
+
+
+@pytest.mark.parametrize("cfg", TILE_CONFIGS)
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 10, 14, 12)])
+@pytest.mark.parametrize("nrhs", [2, 5, 9])
+@pytest.mark.parametrize("op", ["MEE", "MEE_DAG"])
+def test_fp16_tile_hop_bit_identical(ctx_single, ctx_tiles, clg, cfg, dims, nrhs, op):
+    """The tile form gives the same bits as the one-rhs kernel, with a partial
+    last tile (6x10x14x12: 2520 sites per checkerboard) and more right-hand
+    sides than warps."""
+    outs = []
+    for c in (ctx_single, ctx_tiles(cfg)):
+        lat = clg.Lattice(c, dims)
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+        f = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF, nrhs=nrhs)
+        for r in range(nrhs):
+            f.InitialField(clg.SOURCE_GAUSS, 600 + r, 2, rhs=r)
+        f.ApplyOperator(getattr(clg, "OP_" + op), U)
+        outs.append([f.to_numpy(r) for r in range(nrhs)])
+    for r in range(nrhs):
+        np.testing.assert_array_equal(outs[0][r], outs[1][r])
+
+
+@pytest.mark.parametrize("cfg", ["8:1", "3:0"])
+def test_fp16_tile_cg_epilogues(ctx_single, ctx_tiles, clg, oracle, cfg):
+    """The fused CGNE iteration with the tile form's epilogues (CgHopAlpha,
+    CgHopUpdate reduced per tile and in two levels) converges like the one-rhs
+    kernels, to 1e-10 by the oracle's residual, on five right-hand sides that
+    finish at different iterations (the finished ones are skipped)."""
+    nrhs = 5
+    res = []
+    for c in (ctx_single, ctx_tiles(cfg)):
+        lat = clg.Lattice(c, (8, 8, 8, 16))
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+        b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=nrhs)
+        for r in range(nrhs):
+            b.InitialField(clg.SOURCE_GAUSS if r % 2 else clg.SOURCE_Z2, 700 + r, 2, rhs=r)
+        x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=nrhs)
+        S = clg.CSLASolverCG(c, inner_precision=clg.HALF, tol_true_rel=1e-10)
+        infos = S.Solve(x, b, U, clg.EFO_F_D)
+        res.append(([i["iterations"] for i in infos], [x.to_numpy(r) for r in range(nrhs)], U.CopyDataOut(),
+                    [b.to_numpy(r) for r in range(nrhs)]))
+    op = oracle.Operator("WILSON_D", (8, 8, 8, 16), res[1][2], KAPPA)
+    for r in range(nrhs):
+        assert abs(res[0][0][r] - res[1][0][r]) <= max(3, res[0][0][r] // 20), (res[0][0], res[1][0])
+        assert op.true_residual(res[1][3][r], res[1][1][r]) <= 1e-10
