@@ -85,13 +85,33 @@ cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagge
                 : launch_pdl(ctx, wilson_hop_batch_kernel<P, RECON, false>, grid, dim3(bs), 0, a);
 }
 
+}  // namespace
+
+// The y-rows per chunk of the tile hops' blocked order (0: site order): the
+// largest divisor of L_y whose three x-slabs of input spinors, over all
+// right-hand sides, take at most 24 MB of L2; 0 when the z-t planes are not a
+// whole number of tiles or no chunk smaller than L_y qualifies.
+int tile_rows(const Geom& g, int nrhs) {
+  const int64_t plane = (int64_t)g.L[2] * g.L[3];
+  if (plane % (2 * TILE16)) return 0;
+  const int64_t slab_row = plane / 2 * nrhs * 52;  // FP16 spinor + norm bytes of one y-row, all rhs
+  int best = 0;
+  for (int by = 1; by < g.L[1]; ++by)
+    if (g.L[1] % by == 0 && 3 * by * slab_row <= (int64_t)24 << 20) best = by;
+  return best;
+}
+
+namespace {
+
 // FP16 Wilson hop over a tile of 32 sites for all right-hand sides
-// (wilson_hop_tile16_kernel); config = block size | (16 + v) << 16 with v = 0
-// uncapped, 1 capped at 80 registers
-cudaError_t launch_wilson_tile(clg_context_s* ctx, const HopArgs& a, bool dagger, int cfg) {
+// (wilson_hop_tile16_kernel); config = block size | (16 + v) << 16 with v & 1
+// = the 80-register cap and v & 2 = the blocked tile order (tile_rows)
+cudaError_t launch_wilson_tile(clg_context_s* ctx, const HopArgs& a0, bool dagger, int cfg) {
   const int bs = cfg & 0xffff;
+  HopArgs a = a0;
+  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
   dim3 grid((unsigned)((a.g.Vh + TILE16 - 1) / TILE16));
-  if ((cfg >> 16) == 17)
+  if ((cfg >> 16) & 1)
     return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 3>, grid, dim3(bs), 0, a)
                   : launch_pdl(ctx, wilson_hop_tile16_kernel<false, 3>, grid, dim3(bs), 0, a);
   return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 2>, grid, dim3(bs), 0, a)
@@ -137,10 +157,8 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
       cand.push_back(bs | (9 << 16));
     }
     cand.push_back(64 | (2 << 16));
-    for (int w : tile_warps(nrhs)) {
-      cand.push_back((32 * w) | (16 << 16));
-      cand.push_back((32 * w) | (17 << 16));
-    }
+    for (int w : tile_warps(nrhs))
+      for (int v = 0; v < (tile_rows(a.g, nrhs) ? 4 : 2); ++v) cand.push_back((32 * w) | ((16 + v) << 16));
     // untuned (inside a capture, or the output aliases the xpay source): the
     // one-rhs kernel, and nothing is cached
     if (!ctx->tuning_enabled || !idempotent(a) || stream_capturing(ctx->stream))
@@ -335,6 +353,7 @@ clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec
   a.nrhs = s.nrhs > 0 ? s.nrhs : 1;
   a.seg = U->seg;
   a.seg_vh = U->seg_vh;
+  a.tile_rows = 0;
   if (U->seg) {
     if (s.kind != CLG_FERMION_WILSON) return ctx->fail(CLG_ERR_UNSUPPORTED, "a batch of lattices takes Wilson fermions");
     a.U_here = a.U_there = nullptr;

@@ -59,6 +59,9 @@ struct HopArgs {
   // h >= seg_vh[r] are padding
   const HopSeg* seg;
   const int64_t* seg_vh;
+  // the tile hops' block order (wilson_hop_tile16_kernel): 0 = tiles in site
+  // order, else the rows y are walked in chunks of tile_rows (tile16_index)
+  int tile_rows;
 };
 
 // chiral gamma tables (GammaMatrix.h:447-478): row r -> column perm[r] with phase i^z4[r]
@@ -157,15 +160,60 @@ __device__ __forceinline__ void link16_third_row(uint32_t u[9]) {
   u[8] = cross(0, 4, 1, 3);
 }
 
+// FP16 hop accumulators, "planar" over pairs of spin rows: r[c] holds the real
+// parts of rows (0, 1) of colour c, r[3 + c] those of rows (2, 3); i[] the
+// imaginary parts.  acc16_out gives the usual interleaved acc[12].
+struct Acc16 {
+  float2 r[6], i[6];
+};
+__device__ __forceinline__ void acc16_zero(Acc16& A) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    A.r[k] = make_float2(0.f, 0.f);
+    A.i[k] = make_float2(0.f, 0.f);
+  }
+}
+__device__ __forceinline__ void acc16_out(const Acc16& A, cpx<float> acc[12]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    acc[c] = mk<float>(A.r[c].x, A.i[c].x);
+    acc[3 + c] = mk<float>(A.r[c].y, A.i[c].y);
+    acc[6 + c] = mk<float>(A.r[3 + c].x, A.i[3 + c].x);
+    acc[9 + c] = mk<float>(A.r[3 + c].y, A.i[3 + c].y);
+  }
+}
+
+// a + (P0 ? +b.lo : -b.lo, P1 ? +b.hi : -b.hi), one half2 instruction
+template <bool P0, bool P1>
+__device__ __forceinline__ __half2 h2_add_signed(__half2 a, __half2 b) {
+  if constexpr (P0 && P1) return __hadd2(a, b);
+  else if constexpr (!P0 && !P1) return __hsub2(a, b);
+  else return __hfma2(__floats2half2_rn(P0 ? 1.f : -1.f, P1 ? 1.f : -1.f), b, a);
+}
+// acc + (S0 ? s : -s, S1 ? s : -s) * f, one packed f32x2 FMA
+template <bool S0, bool S1>
+__device__ __forceinline__ float2 f2_fma_signed(float s, float2 f, float2 acc) {
+  return __ffma2_rn(make_float2(S0 ? s : -s, S1 ? s : -s), f, acc);
+}
+
 // The FP16 counterpart of wilson_hop_dir with the whole link given (u[9], one
-// complex number per half2 word): the spin projection and the two colour
-// mat-vecs run on half2 words; only the 6 projected products are converted,
-// and they are accumulated in FP32 with the factor s (boundary sign times the
-// neighbour's site norm).
+// complex number per half2 word), planar over the two projected spin rows:
+// the spin projection forms, per colour, one half2 of the real parts of both
+// projected rows and one of the imaginary parts; every HFMA2 of the colour
+// mat-vec then serves both rows with no swap or sign flip of its operands
+// (the link element's real / imaginary part is the broadcast operand), and
+// the phases of the rebuilt rows 2, 3 are per-lane signs of one packed f32x2
+// FMA.  The accumulation is in FP32 with the factor s (boundary sign times
+// the neighbour's site norm).  Every rounding step is the one of the
+// interleaved formulation (projection a + i^z b, U h as (re, im) pairs,
+// s * g + acc per real component), so results are bit-identical to it.
+// Both projected rows' phases i^z have the same parity for every direction
+// of the chiral basis (gz4), which is what lets one plane select serve both.
 template <int MU, int SGN, bool UDAG>
-__device__ __forceinline__ void wilson_hop_dir16_u(cpx<float> acc[12], const Packed16& p, const uint32_t (&u)[9],
-                                                   float s) {
+__device__ __forceinline__ void wilson_hop_dir16_u(Acc16& A, const Packed16& p, const uint32_t (&u)[9], float s) {
   constexpr int add = SGN < 0 ? 2 : 0;
+  constexpr int z0 = (gz4(MU, 0) + add) & 3, z1 = (gz4(MU, 1) + add) & 3;
+  static_assert(((z0 ^ z1) & 1) == 0, "projected rows with phases of different parity");
   uint32_t w[12];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -174,14 +222,25 @@ __device__ __forceinline__ void wilson_hop_dir16_u(cpx<float> acc[12], const Pac
     w[4 * k + 2] = p.c[k].z;
     w[4 * k + 3] = p.c[k].w;
   }
-  uint32_t h0[3], h1[3];
+  // projected rows j = 0, 1:  h_j[c] = psi_j[c] + i^z_j psi_perm(j)[c]
+  __half2 hR[3], hI[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    h0[c] = as_u32(__hadd2(as_h2(w[c]), as_h2(h2_mul_i<gz4(MU, 0) + add>(w[3 * gperm(MU, 0) + c]))));
-    h1[c] = as_u32(__hadd2(as_h2(w[3 + c]), as_h2(h2_mul_i<gz4(MU, 1) + add>(w[3 * gperm(MU, 1) + c]))));
+    const uint32_t a0 = w[c], a1 = w[3 + c];
+    const uint32_t b0 = w[3 * gperm(MU, 0) + c], b1 = w[3 * gperm(MU, 1) + c];
+    const __half2 Ar = as_h2(__byte_perm(a0, a1, 0x5410)), Ai = as_h2(__byte_perm(a0, a1, 0x7632));
+    const __half2 Br = as_h2(__byte_perm(b0, b1, 0x5410)), Bi = as_h2(__byte_perm(b0, b1, 0x7632));
+    if constexpr ((z0 & 1) == 0) {  // i^z = +-1
+      hR[c] = h2_add_signed<z0 == 0, z1 == 0>(Ar, Br);
+      hI[c] = h2_add_signed<z0 == 0, z1 == 0>(Ai, Bi);
+    } else {  // i^z b = (-b.im, b.re) for z = 1, (b.im, -b.re) for z = 3
+      hR[c] = h2_add_signed<z0 == 3, z1 == 3>(Ar, Bi);
+      hI[c] = h2_add_signed<z0 == 1, z1 == 1>(Ai, Br);
+    }
   }
+  // g_j = U h_j (UDAG: U^+ h_j), both rows per instruction
   const __half2 zero = __float2half2_rn(0.f);
-  __half2 g0[3] = {zero, zero, zero}, g1[3] = {zero, zero, zero};
+  __half2 gR[3] = {zero, zero, zero}, gI[3] = {zero, zero, zero};
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -189,41 +248,45 @@ __device__ __forceinline__ void wilson_hop_dir16_u(cpx<float> acc[12], const Pac
       // U: row r, column k;  U^+: conj of row k, column r
       const uint32_t e = UDAG ? u[3 * k + r] : u[3 * r + k];
       const __half2 er = __low2half2(as_h2(e)), ei = __high2half2(as_h2(e));
-      g0[r] = h2_cmac<UDAG>(er, ei, h0[k], g0[r]);
-      g1[r] = h2_cmac<UDAG>(er, ei, h1[k], g1[r]);
+      gR[r] = __hfma2(er, hR[k], gR[r]);
+      gI[r] = __hfma2(er, hI[k], gI[r]);
+      if constexpr (UDAG) {  // conj(e) h: re += ei h.im, im -= ei h.re
+        gR[r] = __hfma2(ei, hI[k], gR[r]);
+        gI[r] = __hfma2(__hneg2(ei), hR[k], gI[r]);
+      } else {               // e h: re -= ei h.im, im += ei h.re
+        gR[r] = __hfma2(__hneg2(ei), hI[k], gR[r]);
+        gI[r] = __hfma2(ei, hR[k], gI[r]);
+      }
     }
-  // accumulation in FP32: rows whose phase is real (+-1) take one packed
-  // f32x2 FMA per complex number (sm_100 FFMA2); rows with an imaginary phase
-  // need the swapped pair and stay on two scalar FMAs
-  const float2 ss = make_float2(s, s), sn = make_float2(-s, -s);
+  // FP32 accumulation.  Rows 0, 1 take s g_0, s g_1; rows 2, 3 take
+  // s i^z_r g_perm(r), perm = (1, 0) for mu < 2 (the lanes swapped) and (0, 1)
+  // for mu >= 2, with z_2, z_3 of equal parity as well.
+  constexpr int z2 = (gz4(MU, 2) + add) & 3, z3 = (gz4(MU, 3) + add) & 3;
+  static_assert(((z2 ^ z3) & 1) == 0, "rebuilt rows with phases of different parity");
+  constexpr bool swp = gperm(MU, 2) == 1;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float2 f0 = __half22float2(g0[c]), f1 = __half22float2(g1[c]);
-    float2* av = reinterpret_cast<float2*>(acc);
-    av[c] = __ffma2_rn(ss, f0, av[c]);
-    av[3 + c] = __ffma2_rn(ss, f1, av[3 + c]);
-#pragma unroll
-    for (int row = 2; row < 4; ++row) {
-      const int z = (gz4(MU, row) + add) & 3;
-      const float2 f = gperm(MU, row) == 0 ? f0 : f1;
-      if (z == 0) {
-        av[3 * row + c] = __ffma2_rn(ss, f, av[3 * row + c]);
-      } else if (z == 2) {
-        av[3 * row + c] = __ffma2_rn(sn, f, av[3 * row + c]);
-      } else {
-        acc[3 * row + c] = cfma(s, mul_i(mk<float>(f.x, f.y), z), acc[3 * row + c]);
-      }
+    const float2 fr = __half22float2(gR[c]), fi = __half22float2(gI[c]);
+    A.r[c] = f2_fma_signed<true, true>(s, fr, A.r[c]);
+    A.i[c] = f2_fma_signed<true, true>(s, fi, A.i[c]);
+    const float2 gr = swp ? make_float2(fr.y, fr.x) : fr;
+    const float2 gi = swp ? make_float2(fi.y, fi.x) : fi;
+    if constexpr ((z2 & 1) == 0) {
+      A.r[3 + c] = f2_fma_signed<z2 == 0, z3 == 0>(s, gr, A.r[3 + c]);
+      A.i[3 + c] = f2_fma_signed<z2 == 0, z3 == 0>(s, gi, A.i[3 + c]);
+    } else {
+      A.r[3 + c] = f2_fma_signed<z2 == 3, z3 == 3>(s, gi, A.r[3 + c]);
+      A.i[3 + c] = f2_fma_signed<z2 == 1, z3 == 1>(s, gr, A.i[3 + c]);
     }
   }
 }
 
 // The same with the link as stored (12-real): the third row is rebuilt first.
 template <int MU, int SGN, bool UDAG>
-__device__ __forceinline__ void wilson_hop_dir16(cpx<float> acc[12], const Packed16& p, const PackedLink16& l,
-                                                 float s) {
+__device__ __forceinline__ void wilson_hop_dir16(Acc16& A, const Packed16& p, const PackedLink16& l, float s) {
   uint32_t u[9] = {l.a.x, l.a.y, l.a.z, l.a.w, l.b.x, l.b.y, 0u, 0u, 0u};
   link16_third_row(u);
-  wilson_hop_dir16_u<MU, SGN, UDAG>(acc, p, u, s);
+  wilson_hop_dir16_u<MU, SGN, UDAG>(A, p, u, s);
 }
 
 struct NbrInfo {
@@ -342,6 +405,8 @@ __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom&
     // (wilson_hop_dir16); the projection and the link product are linear, so
     // the neighbour's site norm is applied with the boundary sign to the 6
     // projected products when they are accumulated in FP32.
+    Acc16 A;
+    acc16_zero(A);
 #define CLG_WILSON_DIR16(MU)                                                            \
   {                                                                                     \
     Packed16 pf, pb;                                                                    \
@@ -350,14 +415,15 @@ __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom&
     load_packed_link16(Uh, MU, lVh, h, lf);                                             \
     load_packed16(in, in_norm, Vh, nb.hb[MU], pb);                                      \
     load_packed_link16(Ut, MU, lVh, nb.hb[MU], lb);                                     \
-    wilson_hop_dir16<MU, SF, false>(acc, pf, lf, nb.sf[MU] * pf.n);                     \
-    wilson_hop_dir16<MU, SB, true>(acc, pb, lb, nb.sb[MU] * pb.n);                      \
+    wilson_hop_dir16<MU, SF, false>(A, pf, lf, nb.sf[MU] * pf.n);                       \
+    wilson_hop_dir16<MU, SB, true>(A, pb, lb, nb.sb[MU] * pb.n);                        \
   }
     CLG_WILSON_DIR16(0)
     CLG_WILSON_DIR16(1)
     CLG_WILSON_DIR16(2)
     CLG_WILSON_DIR16(3)
 #undef CLG_WILSON_DIR16
+    acc16_out(A, acc);
   } else {
 #define CLG_WILSON_DIR(MU)                                                              \
   {                                                                                     \
@@ -729,6 +795,8 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_epi_kernel(HopArgs
 // and rhs is wilson_hop_dir16_u's, so the results are bit-identical to the
 // one-rhs kernel.
 constexpr int TILE16 = 32;
+// the y-rows per chunk of the blocked tile order for this lattice and rhs count (dslash.cu)
+int tile_rows(const Geom& g, int nrhs);
 struct Tile16 {
   uint4 la[8][TILE16];     // link words 0-3; direction d < 4: U_d(x), d >= 4: U_(d-4)(x - mu)
   uint4 lb[8][TILE16];     // words 4-7
@@ -736,6 +804,24 @@ struct Tile16 {
   int nb[8][TILE16];       // checkerboard index of x + mu (d < 4), of x - mu (d >= 4)
   uint32_t neg[TILE16];    // bit d: the boundary sign of direction d is -1
 };
+
+// The tile of block blockIdx.x.  In site order a spinor is read by the tiles
+// of its x-neighbours a whole (y, z, t) volume apart, so the L2 would have to
+// hold about three such slabs of every right-hand side.  With tile_rows > 0
+// (the lattice's z-t planes a whole number of tiles, L_y a multiple of
+// tile_rows) the blocks instead walk chunk after chunk of tile_rows y-rows,
+// x slowest within a chunk: the slabs shrink by L_y / tile_rows, and only the
+// y-neighbours across a chunk's edge are read from DRAM a second time.
+__device__ __forceinline__ int64_t tile16_index(const HopArgs& a) {
+  const int64_t b = blockIdx.x;
+  if (a.tile_rows <= 0) return b;
+  const int64_t np = (int64_t)a.g.L[2] * a.g.L[3] / (2 * TILE16);  // tiles per (x, y) plane
+  const int64_t per_x = a.tile_rows * np, per_chunk = a.g.L[0] * per_x;
+  const int64_t yc = b / per_chunk, r = b - yc * per_chunk;
+  const int64_t x = r / per_x, r2 = r - x * per_x;
+  const int64_t yi = r2 / np, k = r2 - yi * np;
+  return (x * a.g.L[1] + yc * a.tile_rows + yi) * np + k;
+}
 
 // The neighbours of the tile's sites (geometry only: no memory is read, so
 // this runs before the wait on the previous kernel)
@@ -797,8 +883,8 @@ __device__ __forceinline__ void wilson_hop_site_tile16(const HopArgs& a, const T
   const int64_t Vh = a.g.Vh;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
   const float* in_norm = a.in_norm + rhs * a.in_nstride;
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = mk<float>(0.f, 0.f);
+  Acc16 A;
+  acc16_zero(A);
   const uint32_t neg = t.neg[i];
   constexpr int SF = DAGGER ? 1 : -1;
   constexpr int SB = -SF;
@@ -809,15 +895,16 @@ __device__ __forceinline__ void wilson_hop_site_tile16(const HopArgs& a, const T
     load_packed16(in, in_norm, Vh, t.nb[4 + MU][i], pb);                     \
     uint32_t u[9];                                                           \
     tile16_link(t, MU, i, u);                                                \
-    wilson_hop_dir16_u<MU, SF, false>(acc, pf, u, (neg >> MU) & 1u ? -pf.n : pf.n);       \
+    wilson_hop_dir16_u<MU, SF, false>(A, pf, u, (neg >> MU) & 1u ? -pf.n : pf.n);         \
     tile16_link(t, 4 + MU, i, u);                                            \
-    wilson_hop_dir16_u<MU, SB, true>(acc, pb, u, (neg >> (4 + MU)) & 1u ? -pb.n : pb.n);  \
+    wilson_hop_dir16_u<MU, SB, true>(A, pb, u, (neg >> (4 + MU)) & 1u ? -pb.n : pb.n);    \
   }
   CLG_TILE_DIR16(0)
   CLG_TILE_DIR16(1)
   CLG_TILE_DIR16(2)
   CLG_TILE_DIR16(3)
 #undef CLG_TILE_DIR16
+  acc16_out(A, acc);
   wilson_hop_finish<P16>(a, rhs, h, acc);
 }
 
@@ -826,7 +913,7 @@ __device__ __forceinline__ void wilson_hop_site_tile16(const HopArgs& a, const T
 template <bool DAGGER, int MINB>
 __global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_kernel(HopArgs a) {
   __shared__ Tile16 t;
-  const int64_t h0 = (int64_t)blockIdx.x * TILE16;
+  const int64_t h0 = tile16_index(a) * TILE16;
   pdl_launch_dependents();
   tile16_neighbours(a, h0, t);
   pdl_wait();
@@ -852,7 +939,7 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_epi_kernel(HopArg
                                                                           double* gpart, unsigned* counter,
                                                                           unsigned group) {
   __shared__ Tile16 t;
-  const int64_t h0 = (int64_t)blockIdx.x * TILE16;
+  const int64_t h0 = tile16_index(a) * TILE16;
   pdl_launch_dependents();
   tile16_neighbours(a, h0, t);
   pdl_wait();

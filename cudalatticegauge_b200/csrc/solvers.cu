@@ -582,12 +582,14 @@ cudaError_t launch_hop_pair_epi(clg_context_s* ctx, const HopArgs& a, const E& e
 
 // the tile form (wilson_hop_tile16_epi_kernel): config as in launch_wilson_tile
 template <bool DAG, class E>
-cudaError_t launch_hop_tile_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int cfg) {
+cudaError_t launch_hop_tile_epi(clg_context_s* ctx, const HopArgs& a0, const E& e, int cfg) {
   const int bs = cfg & 0xffff;
+  HopArgs a = a0;
+  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
   const int64_t nslots = (a.g.Vh + TILE16 - 1) / TILE16;
   const unsigned group = red_group(nslots, 1);
   double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
-  if ((cfg >> 16) == 17)
+  if ((cfg >> 16) & 1)
     return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 3, E>, dim3((unsigned)nslots), dim3(bs), 0, a, e,
                       ctx->red_partials, gpart, ctx->red_counter, group);
   return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 2, E>, dim3((unsigned)nslots), dim3(bs), 0, a, e,

@@ -183,14 +183,15 @@ def test_fp16_pair_variants_vs_oracle(clg, oracle, cfg):
         c.close()
 
 
-TILE_CONFIGS = ["8:0", "8:1", "4:1", "3:1"]
+TILE_CONFIGS = ["8:0", "8:1", "4:1", "3:1", "4:3", "7:2"]
 
 
 @pytest.fixture(scope="module")
 def ctx_tiles(clg):
     """Contexts whose FP16 Wilson hops over two or more right-hand sides use
     the tile form (CLG_HOP_TILE="<warps>:<variant>": 32 sites per block, the
-    links staged once in shared memory for all right-hand sides)."""
+    links staged once in shared memory for all right-hand sides; variant bit
+    0 caps the registers, bit 1 walks the tiles in chunks of y-rows)."""
     made = {}
 
     def get(cfg):
@@ -209,8 +210,8 @@ def ctx_tiles(clg):
 @pytest.mark.parametrize("op", ["MEE", "MEE_DAG"])
 def test_fp16_tile_hop_bit_identical(ctx_single, ctx_tiles, clg, cfg, dims, nrhs, op):
     """The tile form gives the same bits as the one-rhs kernel, with a partial
-    last tile (6x10x14x12: 2520 sites per checkerboard) and more right-hand
-    sides than warps."""
+    last tile (6x10x14x12: 2520 sites per checkerboard, site order) and more
+    right-hand sides than warps; on 8^4 the blocked order covers every tile."""
     outs = []
     for c in (ctx_single, ctx_tiles(cfg)):
         lat = clg.Lattice(c, dims)
@@ -225,7 +226,7 @@ def test_fp16_tile_hop_bit_identical(ctx_single, ctx_tiles, clg, cfg, dims, nrhs
         np.testing.assert_array_equal(outs[0][r], outs[1][r])
 
 
-@pytest.mark.parametrize("cfg", ["8:1", "3:0"])
+@pytest.mark.parametrize("cfg", ["8:1", "3:0", "4:3"])
 def test_fp16_tile_cg_epilogues(ctx_single, ctx_tiles, clg, oracle, cfg):
     """The fused CGNE iteration with the tile form's epilogues (CgHopAlpha,
     CgHopUpdate reduced per tile and in two levels) converges like the one-rhs
