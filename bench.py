@@ -238,9 +238,12 @@ def hop_form(ctx, prec, Vh, nrhs):
     pname = {0: "P64", 1: "P32", 2: "P16"}[prec]
     if key + "_auto" in tuned:
         bs, v = tuned[key + "_auto"]
+        if v >= 24:
+            return f"wilson_hop_mma16_kernel (tensor-core colour products; variant {v - 24})"
         if v >= 16:
             return (f"wilson_hop_tile16_kernel (32 sites x {nrhs} rhs per block, links staged once in shared memory; "
-                    f"{bs // 32} warps, {'80-register cap' if v == 17 else 'uncapped'})")
+                    f"{bs // 32} warps, {'80-register cap' if v & 1 else 'uncapped'}, "
+                    f"{'blocked' if v & 2 else 'site'} tile order)")
         if v >= 8:
             return f"wilson_hop_pair_kernel (2 rhs per thread; block {bs}, variant {v - 8})"
         return f"wilson_hop_kernel<P16,12-real> (1 rhs per thread; block {bs}, variant {v})"
@@ -464,6 +467,11 @@ def ours(args, world, rank, local):
         "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": launches,
         "iterations_per_solve": max(i["iterations"] for i in infos) if infos else None,
         "oracle_check": oracle_check,
+        # the Wilson hop forms the autotuner chose for this lattice
+        # ([block, variant]: variant 0-3 one rhs per thread, 8-9 two, 16-19 the
+        # tile form, 24-27 the tensor-core form; see clg_context_tuned)
+        "autotuner": {k: list(v) for k, v in ctx.tuned().items()
+                      if k.startswith("wilson") and f"_V{Vh}_n{nrhs}_" in k},
     }
     result.update(extra)
     if "cpu_baseline" not in result:
@@ -1243,6 +1251,11 @@ def profile_driver(args):
         for _ in range(args.steps):
             print(s.Solve(x, b, U, clg.EFO_F_D)[0], flush=True)
     ctx.synchronize()
+    tf = os.environ.get("CLG_TUNE_FILE")
+    if tf and not os.path.exists(tf):  # the autotuner's choices for a later (profiled) run of the same command
+        with open(tf, "w") as f:
+            for k, (bs, v) in ctx.tuned().items():
+                f.write(f"{k}={bs | (v << 16)}\n")
     print("profile driver done, kernels", ctx.kernel_count())
 
 

@@ -363,6 +363,27 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
     if (std::sscanf(t, "%d:%d", &warps, &variant) == 2 && warps >= 1 && warps <= 8 && variant >= 0 && variant <= 3) {
       ctx->hop_pair_mode = 3;
       ctx->hop_tile_config = (32 * warps) | ((16 + variant) << 16);
+    } else if (std::sscanf(t, "%d:%d", &warps, &variant) == 2 && warps == 8 && variant >= 8 && variant <= 11) {
+      ctx->hop_pair_mode = 3;
+      ctx->hop_tile_config = 256 | ((24 + variant - 8) << 16);
+    }
+  }
+  if (const char* t = std::getenv("CLG_HOP_MMA")) ctx->hop_mma = t[0] != '0';
+  // CLG_TUNE_FILE: the autotuner's choices ("<key>=<config>" lines) are read
+  // from this file when the context is created and written back when it is
+  // destroyed, so a later run (a profiler's, whose timings would mislead the
+  // autotuner) launches exactly the kernels an earlier run chose
+  if (const char* t = std::getenv("CLG_TUNE_FILE")) {
+    ctx->tune_file = t;
+    if (FILE* f = std::fopen(t, "r")) {
+      char line[512];
+      while (std::fgets(line, sizeof line, f)) {
+        char* eq = std::strrchr(line, '=');
+        if (!eq) continue;
+        *eq = 0;
+        ctx->tuned[line] = std::atoi(eq + 1);
+      }
+      std::fclose(f);
     }
   }
   if (const char* t = std::getenv("CLG_PDL")) ctx->pdl = t[0] != '0';
@@ -370,6 +391,10 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
     int variant = -1, bs = 0;
     if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && variant >= 0 && variant <= 3 &&
         (bs == 64 || bs == 128 || bs == 256))
+      ctx->hop_config = bs | (variant << 16);
+    // the FP64 / FP32 tile form: variants 16..19, 32 x (1..8) threads
+    else if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && variant >= 16 && variant <= 19 && bs >= 32 &&
+             bs <= 256 && bs % 32 == 0)
       ctx->hop_config = bs | (variant << 16);
   }
   if (stream) {
@@ -403,6 +428,12 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
 clg_status clg_context_destroy(clg_context ctx) {
   if (!ctx) return CLG_ERR_BAD_ARG;
   cudaStreamSynchronize(ctx->stream);
+  if (!ctx->tune_file.empty()) {
+    if (FILE* f = std::fopen(ctx->tune_file.c_str(), "w")) {
+      for (const auto& kv : ctx->tuned) std::fprintf(f, "%s=%d\n", kv.first.c_str(), kv.second);
+      std::fclose(f);
+    }
+  }
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);

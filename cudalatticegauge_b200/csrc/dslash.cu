@@ -14,6 +14,25 @@ namespace {
 // the output aliases the xpay source
 bool idempotent(const HopArgs& a) { return a.x == nullptr || a.x != a.out; }
 
+// FP64 / FP32 Wilson hop over a tile of 32 sites for all right-hand sides
+// (wilson_hop_tileN_kernel); config = block size | (16 + v) << 16, v & 1 =
+// the register cap (128 for FP64, 80 for FP32), v & 2 = the blocked tile order
+template <int P, int RECON>
+cudaError_t launch_wilson_tileN(clg_context_s* ctx, const HopArgs& a0, bool dagger, int cfg) {
+  constexpr int CAP = P == P64 ? 2 : 3;
+  const int bs = cfg & 0xffff;
+  HopArgs a = a0;
+  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
+  dim3 grid((unsigned)((a.g.Vh + TILE16 - 1) / TILE16));
+  if ((cfg >> 16) & 1)
+    return dagger ? launch_pdl(ctx, wilson_hop_tileN_kernel<P, RECON, true, CAP>, grid, dim3(bs), 0, a)
+                  : launch_pdl(ctx, wilson_hop_tileN_kernel<P, RECON, false, CAP>, grid, dim3(bs), 0, a);
+  return dagger ? launch_pdl(ctx, wilson_hop_tileN_kernel<P, RECON, true, 1>, grid, dim3(bs), 0, a)
+                : launch_pdl(ctx, wilson_hop_tileN_kernel<P, RECON, false, 1>, grid, dim3(bs), 0, a);
+}
+
+std::vector<int> tile_warps(int nrhs);
+
 template <int P, int RECON>
 cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int nrhs, const std::string& key) {
   // config = block size | (variant << 16): 0 plain, 1 capped at 80 registers,
@@ -22,6 +41,9 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
   auto go = [&](int cfg) {
     const int bs = cfg & 0xffff;
     const int variant = cfg >> 16;
+    if constexpr (P != P16) {
+      if (variant >= 16) return launch_wilson_tileN<P, RECON>(ctx, a, dagger, cfg);
+    }
     dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
     if constexpr (P == P64) {
       if (variant == 3)
@@ -39,7 +61,10 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
     return dagger ? launch_pdl(ctx, wilson_hop_kernel<P, RECON, true>, grid, dim3(bs), 0, a)
                   : launch_pdl(ctx, wilson_hop_kernel<P, RECON, false>, grid, dim3(bs), 0, a);
   };
-  if (ctx->hop_config >= 0) return go(ctx->hop_config);
+  if (ctx->hop_config >= 0) {
+    ctx->tuned[key] = ctx->hop_config;  // the fused epilogue launches follow the pinned form
+    return go(ctx->hop_config);
+  }
   // __launch_bounds__(256, ...) caps the block at 256 threads
   std::vector<int> cand = {64, 128, 256};
   if (P != P64)
@@ -47,6 +72,10 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
   if (P != P64) cand.push_back(64 | (2 << 16));
   if (P == P64)
     for (int bs : {64, 128, 256}) cand.push_back(bs | (3 << 16));
+  // several right-hand sides: the tile form (links staged once per tile)
+  if (P != P16 && nrhs >= 2)
+    for (int w : tile_warps(nrhs))
+      for (int v = 0; v < (tile_rows(a.g, nrhs) ? 4 : 2); ++v) cand.push_back((32 * w) | ((16 + v) << 16));
   return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 
@@ -91,9 +120,9 @@ cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagge
 // largest divisor of L_y whose three x-slabs of input spinors, over all
 // right-hand sides, take at most 24 MB of L2; 0 when the z-t planes are not a
 // whole number of tiles or no chunk smaller than L_y qualifies.
-int tile_rows(const Geom& g, int nrhs) {
+int tile_rows(const Geom& g, int nrhs, int ts) {
   const int64_t plane = (int64_t)g.L[2] * g.L[3];
-  if (plane % (2 * TILE16)) return 0;
+  if (plane % (2 * ts)) return 0;
   const int64_t slab_row = plane / 2 * nrhs * 52;  // FP16 spinor + norm bytes of one y-row, all rhs
   int best = 0;
   for (int by = 1; by < g.L[1]; ++by)
@@ -103,10 +132,30 @@ int tile_rows(const Geom& g, int nrhs) {
 
 namespace {
 
+// FP16 Wilson hop with the colour products on the tensor cores
+// (wilson_hop_mma16_kernel, 256 threads, a tile of MMA_TS sites); config
+// variant 24 + v, v & 1 = at most 128 registers (two blocks per SM), v & 2 =
+// the blocked tile order
+cudaError_t launch_wilson_mma(clg_context_s* ctx, const HopArgs& a0, bool dagger, int cfg) {
+  HopArgs a = a0;
+  const int v = (cfg >> 16) - 24;
+  a.tile_rows = (v & 2) ? tile_rows(a.g, a.nrhs, MMA_TS) : 0;
+  dim3 grid((unsigned)((a.g.Vh + MMA_TS - 1) / MMA_TS));
+  const size_t smem = sizeof(Mma16Smem);
+  auto go = [&](void (*kernel)(HopArgs)) {
+    if (const cudaError_t e = opt_in_smem((const void*)kernel, smem)) return e;
+    return launch_pdl(ctx, kernel, grid, dim3(256), smem, a);
+  };
+  if (v & 1) return dagger ? go(wilson_hop_mma16_kernel<true, 2>) : go(wilson_hop_mma16_kernel<false, 2>);
+  return dagger ? go(wilson_hop_mma16_kernel<true, 1>) : go(wilson_hop_mma16_kernel<false, 1>);
+}
+
 // FP16 Wilson hop over a tile of 32 sites for all right-hand sides
 // (wilson_hop_tile16_kernel); config = block size | (16 + v) << 16 with v & 1
-// = the 80-register cap and v & 2 = the blocked tile order (tile_rows)
+// = the 80-register cap and v & 2 = the blocked tile order (tile_rows);
+// variants from 24 on are the tensor-core form (launch_wilson_mma)
 cudaError_t launch_wilson_tile(clg_context_s* ctx, const HopArgs& a0, bool dagger, int cfg) {
+  if ((cfg >> 16) >= 24) return launch_wilson_mma(ctx, a0, dagger, cfg);
   const int bs = cfg & 0xffff;
   HopArgs a = a0;
   a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
@@ -159,6 +208,8 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
     cand.push_back(64 | (2 << 16));
     for (int w : tile_warps(nrhs))
       for (int v = 0; v < (tile_rows(a.g, nrhs) ? 4 : 2); ++v) cand.push_back((32 * w) | ((16 + v) << 16));
+    if (ctx->hop_mma)
+      for (int v = 0; v < (tile_rows(a.g, nrhs, MMA_TS) ? 4 : 2); ++v) cand.push_back(256 | ((24 + v) << 16));
     // untuned (inside a capture, or the output aliases the xpay source): the
     // one-rhs kernel, and nothing is cached
     if (!ctx->tuning_enabled || !idempotent(a) || stream_capturing(ctx->stream))
@@ -389,6 +440,11 @@ int tuned_hop_pair_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpe
 int tuned_hop_tile_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback) {
   if (ctx->hop_pair_mode == 3) return ctx->hop_tile_config;
   auto it = ctx->tuned.find(hop_key(U, s) + "_tile");
+  return it == ctx->tuned.end() ? fallback : it->second;
+}
+
+int tuned_hop_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback) {
+  auto it = ctx->tuned.find(hop_key(U, s));
   return it == ctx->tuned.end() ? fallback : it->second;
 }
 

@@ -795,8 +795,9 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_epi_kernel(HopArgs
 // and rhs is wilson_hop_dir16_u's, so the results are bit-identical to the
 // one-rhs kernel.
 constexpr int TILE16 = 32;
-// the y-rows per chunk of the blocked tile order for this lattice and rhs count (dslash.cu)
-int tile_rows(const Geom& g, int nrhs);
+// the y-rows per chunk of the blocked tile order for this lattice, rhs count
+// and tile size (dslash.cu)
+int tile_rows(const Geom& g, int nrhs, int ts = TILE16);
 struct Tile16 {
   uint4 la[8][TILE16];     // link words 0-3; direction d < 4: U_d(x), d >= 4: U_(d-4)(x - mu)
   uint4 lb[8][TILE16];     // words 4-7
@@ -812,20 +813,23 @@ struct Tile16 {
 // tile_rows) the blocks instead walk chunk after chunk of tile_rows y-rows,
 // x slowest within a chunk: the slabs shrink by L_y / tile_rows, and only the
 // y-neighbours across a chunk's edge are read from DRAM a second time.
-__device__ __forceinline__ int64_t tile16_index(const HopArgs& a) {
+template <int TS>
+__device__ __forceinline__ int64_t tile_index(const HopArgs& a) {
   const int64_t b = blockIdx.x;
   if (a.tile_rows <= 0) return b;
-  const int64_t np = (int64_t)a.g.L[2] * a.g.L[3] / (2 * TILE16);  // tiles per (x, y) plane
+  const int64_t np = (int64_t)a.g.L[2] * a.g.L[3] / (2 * TS);  // tiles per (x, y) plane
   const int64_t per_x = a.tile_rows * np, per_chunk = a.g.L[0] * per_x;
   const int64_t yc = b / per_chunk, r = b - yc * per_chunk;
   const int64_t x = r / per_x, r2 = r - x * per_x;
   const int64_t yi = r2 / np, k = r2 - yi * np;
   return (x * a.g.L[1] + yc * a.tile_rows + yi) * np + k;
 }
+__device__ __forceinline__ int64_t tile16_index(const HopArgs& a) { return tile_index<TILE16>(a); }
 
 // The neighbours of the tile's sites (geometry only: no memory is read, so
 // this runs before the wait on the previous kernel)
-__device__ __forceinline__ void tile16_neighbours(const HopArgs& a, int64_t h0, Tile16& t) {
+template <class T>
+__device__ __forceinline__ void tile16_neighbours(const HopArgs& a, int64_t h0, T& t) {
   for (int i = threadIdx.x; i < TILE16; i += blockDim.x) {
     const int64_t h = h0 + i;
     uint32_t neg = 0;
@@ -968,6 +972,440 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_epi_kernel(HopArg
       if (lane == 0) partials[((int64_t)rhs * nslots + blockIdx.x) * E::NRED + k] = v;
     }
     if (lane == 0) __threadfence();
+  }
+  tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
+}
+
+// ---------------------------------------------------------------- FP64 / FP32, a tile of sites for every right-hand side
+// The tile form of the FP64 and FP32 hops: the block stages the 8 links of its
+// 32 sites once (complete, as load_link gives them: 18-real, or 12-real with
+// the third row rebuilt) as complex numbers in shared memory, then loops over
+// the right-hand sides like wilson_hop_tile16_kernel.  The FP64 hop of a
+// batched solve's outer residual re-reads 1152 link bytes per site and rhs
+// through L2 in the one-rhs form; here each link crosses DRAM once per
+// launch.  Arithmetic per site and rhs is wilson_hop_dir's (bit-identical).
+template <typename AT>
+struct TileN {
+  cpx<AT> u[8][9][TILE16];  // direction d < 4: U_d(x), d >= 4: U_(d-4)(x - mu)
+  int nb[8][TILE16];
+  uint32_t neg[TILE16];
+};
+
+template <int P, int RECON, typename AT>
+__device__ __forceinline__ void tileN_links(const HopArgs& a, int64_t h0, TileN<AT>& t) {
+  for (int k = threadIdx.x; k < 8 * TILE16; k += blockDim.x) {
+    const int d = k / TILE16, i = k % TILE16;
+    const int64_t h = h0 + i;
+    cpx<AT> u[9];
+    if (h < a.g.Vh) {
+      if (d < 4)
+        load_link<P, RECON, AT>(a.U_here, d, a.g.Vh, h, u);
+      else
+        load_link<P, RECON, AT>(a.U_there, d - 4, a.g.Vh, t.nb[d][i], u);
+    } else {
+#pragma unroll
+      for (int w = 0; w < 9; ++w) u[w] = mk<AT>(0, 0);
+    }
+#pragma unroll
+    for (int w = 0; w < 9; ++w) t.u[d][w][i] = u[w];
+  }
+}
+
+template <int P, bool DAGGER, typename AT>
+__device__ __forceinline__ void wilson_hop_site_tileN(const HopArgs& a, const TileN<AT>& t, int i, int rhs, int64_t h,
+                                                      cpx<AT> acc[12]) {
+  const int64_t Vh = a.g.Vh;
+  const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
+  const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = mk<AT>(0, 0);
+  const uint32_t neg = t.neg[i];
+  constexpr int SF = DAGGER ? 1 : -1;
+  constexpr int SB = -SF;
+#define CLG_TILEN_DIR(MU)                                                              \
+  {                                                                                    \
+    cpx<AT> psi[12], u[9];                                                             \
+    load_site<P, 12, AT>(in, in_norm, Vh, t.nb[MU][i], psi);                           \
+    _Pragma("unroll") for (int w = 0; w < 9; ++w) u[w] = t.u[MU][w][i];                \
+    wilson_hop_dir<AT, MU, SF, false>(acc, psi, u, (neg >> MU) & 1u ? (AT)-1 : (AT)1); \
+    load_site<P, 12, AT>(in, in_norm, Vh, t.nb[4 + MU][i], psi);                       \
+    _Pragma("unroll") for (int w = 0; w < 9; ++w) u[w] = t.u[4 + MU][w][i];            \
+    wilson_hop_dir<AT, MU, SB, true>(acc, psi, u, (neg >> (4 + MU)) & 1u ? (AT)-1 : (AT)1); \
+  }
+  CLG_TILEN_DIR(0)
+  CLG_TILEN_DIR(1)
+  CLG_TILEN_DIR(2)
+  CLG_TILEN_DIR(3)
+#undef CLG_TILEN_DIR
+  wilson_hop_finish<P>(a, rhs, h, acc);
+}
+
+template <int P, int RECON, bool DAGGER, int MINB>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_kernel(HopArgs a) {
+  using AT = typename AccT<P>::T;
+  __shared__ TileN<AT> t;
+  const int64_t h0 = tile16_index(a) * TILE16;
+  pdl_launch_dependents();
+  tile16_neighbours(a, h0, t);
+  pdl_wait();
+  __syncthreads();
+  tileN_links<P, RECON>(a, h0, t);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int64_t h = h0 + lane;
+  if (h >= a.g.Vh) return;  // no barrier follows
+  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+    if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
+    cpx<AT> acc[12];
+    wilson_hop_site_tileN<P, DAGGER>(a, t, lane, rhs, h, acc);
+    wilson_hop_store<P>(a, rhs, h, acc);
+  }
+}
+
+template <int P, int RECON, bool DAGGER, int MINB, class E>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_epi_kernel(HopArgs a, E e, double* partials,
+                                                                         double* gpart, unsigned* counter,
+                                                                         unsigned group) {
+  using AT = typename AccT<P>::T;
+  __shared__ TileN<AT> t;
+  const int64_t h0 = tile16_index(a) * TILE16;
+  pdl_launch_dependents();
+  tile16_neighbours(a, h0, t);
+  pdl_wait();
+  __syncthreads();
+  tileN_links<P, RECON>(a, h0, t);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int64_t h = h0 + lane;
+  const unsigned nslots = gridDim.x;
+  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+    if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
+    double red[E::NRED];
+#pragma unroll
+    for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
+    if (h < a.g.Vh) {
+      cpx<AT> acc[12];
+      wilson_hop_site_tileN<P, DAGGER>(a, t, lane, rhs, h, acc);
+      if constexpr (E::STORE) wilson_hop_store<P>(a, rhs, h, acc);
+      e.site(rhs, h, acc, red);
+    }
+#pragma unroll
+    for (int k = 0; k < E::NRED; ++k) {
+      double v = red[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) partials[((int64_t)rhs * nslots + blockIdx.x) * E::NRED + k] = v;
+    }
+    if (lane == 0) __threadfence();
+  }
+  tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
+}
+
+// ---------------------------------------------------------------- FP16 with the colour products on the tensor cores
+// The multi-right-hand-side FP16 hop as small matrix products (mma.sync
+// m16n8k16, FP16 operands, FP32 accumulation).  For output site x, with
+// directions d = 2 mu + (0 forward, 1 backward), the hop is
+//   out_s = sum_d U_d ( c_{d,s} h_d^(j_{d,s}) ),   s = 0..3,
+// where h_d^(0,1) are the two spin-projected rows of the neighbour's spinor,
+// rows 0, 1 take c = 1, j = s, and the rebuilt rows 2, 3 take the phase
+// i^z and row perm of the chiral basis (linearity moves the phase before the
+// link).  So per site, with one column per (right-hand side, output row s)
+// holding the 8 directions' 3 colours (re, im) of c h (K = 8 x 8, 6 used), the
+// whole hop of all right-hand sides is one product
+//   OUT^T [columns x (colour, re/im)] = COL^T [columns x K] . E^T [K x 6]
+// with E the real 6 x 6 embedding of each direction's link (U, or U^+
+// backward).  A block takes a tile of MMA_TS sites and the right-hand sides in
+// groups of MMA_G:
+//   1. staging (all threads, lanes over sites: coalesced): for each (site,
+//      rhs) the 8 neighbour norms give nmax; each neighbour spinor is
+//      projected, scaled by sign * norm / nmax (<= 1, so FP16 cannot overflow)
+//      and its four columns' K-blocks are stored to shared memory;
+//   2. products (warp w = site w): per mu one k-step; the A fragments
+//      (columns) by ldmatrix, the B fragment (the link embedding) built in
+//      registers from the staged links; the FP32 accumulators hold the sums
+//      over all 8 directions;
+//   3. finish (thread per (site, rhs)): times nmax, then the usual epilogue
+//      and store.
+// The FP16 rounding differs from wilson_hop_kernel's (the projected rows are
+// rounded once more when scaled; the colour sums are exact products summed in
+// FP32 instead of HFMA2 chains), within the FP16 storage's precision.
+constexpr int MMA_TS = 8;                       // sites per tile
+constexpr int MMA_G = 16;                       // right-hand sides per group
+constexpr int MMA_CS = 72;                      // halves per column: 8 x 8 + 8 pad (144 B: ldmatrix rows conflict-free)
+constexpr int MMA_SS = 4 * MMA_G * MMA_CS + 8;  // halves per site (+16 B: staging stores conflict-free)
+constexpr int MMA_CB = MMA_G * 12 + 2;          // float2 per site of the result buffer (+16 B)
+struct Mma16Smem {
+  __half col[MMA_TS * MMA_SS];  // per site: column (rhs_local * 4 + s), K = d * 8 + colour * 2 + re/im
+  float2 res[MMA_TS * MMA_CB];  // per site: [rhs_local][s * 3 + colour] / nmax
+  uint32_t u[8][9][MMA_TS];     // links as 9 half2 words, direction d = 2 mu + backward
+  int nb[8][MMA_TS];            // neighbour checkerboard index per direction
+  uint32_t neg[MMA_TS];         // bit d: boundary sign -1
+  float nmax[MMA_TS][MMA_G];
+};
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+__device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// the tile's geometry and links (staged once per tile)
+__device__ __forceinline__ void mma16_stage_geometry(const HopArgs& a, int64_t h0, Mma16Smem& t) {
+  for (int i = threadIdx.x; i < MMA_TS; i += blockDim.x) {
+    const int64_t h = h0 + i;
+    uint32_t neg = 0;
+    if (h < a.g.Vh) {
+      NbrInfo nb;
+      int c[4];
+      neighbours(a.g, a.out_parity, h, nb, c);
+#pragma unroll
+      for (int mu = 0; mu < 4; ++mu) {
+        t.nb[2 * mu][i] = nb.hf[mu];
+        t.nb[2 * mu + 1][i] = nb.hb[mu];
+        neg |= (nb.sf[mu] < 0.f ? 1u : 0u) << (2 * mu);
+        neg |= (nb.sb[mu] < 0.f ? 1u : 0u) << (2 * mu + 1);
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 8; ++d) t.nb[d][i] = 0;
+    }
+    t.neg[i] = neg;
+  }
+}
+__device__ __forceinline__ void mma16_stage_links(const HopArgs& a, int64_t h0, Mma16Smem& t) {
+  for (int k = threadIdx.x; k < 8 * MMA_TS; k += blockDim.x) {
+    const int d = k / MMA_TS, i = k % MMA_TS;
+    const int64_t h = h0 + i;
+    uint32_t u[9] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    if (h < a.g.Vh) {
+      PackedLink16 l;
+      if ((d & 1) == 0)
+        load_packed_link16(a.U_here, d >> 1, a.g.Vh, h, l);
+      else
+        load_packed_link16(a.U_there, d >> 1, a.g.Vh, t.nb[d][i], l);
+      u[0] = l.a.x; u[1] = l.a.y; u[2] = l.a.z; u[3] = l.a.w; u[4] = l.b.x; u[5] = l.b.y;
+      link16_third_row(u);
+    }
+#pragma unroll
+    for (int w = 0; w < 9; ++w) t.u[d][w][i] = u[w];
+  }
+}
+
+// One direction's four columns for (site i, rhs_local rl): the projected rows
+// of the neighbour spinor p, scaled by r2, with the rebuilt rows' phases.
+template <int MU, int SGN>
+__device__ __forceinline__ void mma16_columns(__half* colsite, int rl, int d, const Packed16& p, __half2 r2) {
+  constexpr int add = SGN < 0 ? 2 : 0;
+  uint32_t w[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    w[4 * k + 0] = p.c[k].x;
+    w[4 * k + 1] = p.c[k].y;
+    w[4 * k + 2] = p.c[k].z;
+    w[4 * k + 3] = p.c[k].w;
+  }
+  uint32_t h[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    h[0][c] = as_u32(__hmul2(__hadd2(as_h2(w[c]), as_h2(h2_mul_i<gz4(MU, 0) + add>(w[3 * gperm(MU, 0) + c]))), r2));
+    h[1][c] = as_u32(__hmul2(__hadd2(as_h2(w[3 + c]), as_h2(h2_mul_i<gz4(MU, 1) + add>(w[3 * gperm(MU, 1) + c]))), r2));
+  }
+  constexpr int j2 = gperm(MU, 2), j3 = gperm(MU, 3);
+  uint4* base = reinterpret_cast<uint4*>(colsite + (rl * 4) * MMA_CS + d * 8);
+  constexpr int CS4 = MMA_CS / 8;  // uint4 per column
+  base[0] = make_uint4(h[0][0], h[0][1], h[0][2], 0u);
+  base[CS4] = make_uint4(h[1][0], h[1][1], h[1][2], 0u);
+  base[2 * CS4] = make_uint4(h2_mul_i<gz4(MU, 2) + add>(h[j2][0]), h2_mul_i<gz4(MU, 2) + add>(h[j2][1]),
+                             h2_mul_i<gz4(MU, 2) + add>(h[j2][2]), 0u);
+  base[3 * CS4] = make_uint4(h2_mul_i<gz4(MU, 3) + add>(h[j3][0]), h2_mul_i<gz4(MU, 3) + add>(h[j3][1]),
+                             h2_mul_i<gz4(MU, 3) + add>(h[j3][2]), 0u);
+}
+
+// Phase 1 for right-hand sides [r0, r0 + MMA_G): thread t stages site t % 8,
+// rhs_local (t / 8) % 16, directions mu in {0, 1} (t < 128) or {2, 3}.
+template <bool DAGGER>
+__device__ __forceinline__ void mma16_stage_columns(const HopArgs& a, int64_t h0, int r0, Mma16Smem& t) {
+  const int i = threadIdx.x % MMA_TS, rl = (threadIdx.x / MMA_TS) % MMA_G, dh = threadIdx.x / (MMA_TS * MMA_G);
+  const int rhs = r0 + rl;
+  const int64_t h = h0 + i;
+  const bool valid = h < a.g.Vh && rhs < a.nrhs && !(a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]);
+  __half* colsite = t.col + i * MMA_SS;
+  if (!valid) {
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        reinterpret_cast<uint4*>(colsite + (rl * 4 + s) * MMA_CS + (4 * dh + d) * 8)[0] = z;
+    if (dh == 0) t.nmax[i][rl] = 0.f;
+    return;
+  }
+  const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
+  const float* in_norm = a.in_norm + rhs * a.in_nstride;
+  float nm = 0.f;
+#pragma unroll
+  for (int d = 0; d < 8; ++d) nm = fmaxf(nm, __ldg(in_norm + t.nb[d][i]));
+  if (dh == 0) t.nmax[i][rl] = nm;
+  const float inv = nm > 0.f ? 1.f / nm : 0.f;
+  const uint32_t neg = t.neg[i];
+  constexpr int SF = DAGGER ? 1 : -1;
+  constexpr int SB = -SF;
+#define CLG_MMA_DIR(MU)                                                                          \
+  {                                                                                              \
+    Packed16 pf, pb;                                                                             \
+    load_packed16(in, in_norm, a.g.Vh, t.nb[2 * MU][i], pf);                                     \
+    load_packed16(in, in_norm, a.g.Vh, t.nb[2 * MU + 1][i], pb);                                 \
+    const float rf = ((neg >> (2 * MU)) & 1u ? -pf.n : pf.n) * inv;                              \
+    const float rb = ((neg >> (2 * MU + 1)) & 1u ? -pb.n : pb.n) * inv;                          \
+    mma16_columns<MU, SF>(colsite, rl, 2 * MU, pf, __float2half2_rn(rf));                        \
+    mma16_columns<MU, SB>(colsite, rl, 2 * MU + 1, pb, __float2half2_rn(rb));                    \
+  }
+  if (dh == 0) {
+    CLG_MMA_DIR(0)
+    CLG_MMA_DIR(1)
+  } else {
+    CLG_MMA_DIR(2)
+    CLG_MMA_DIR(3)
+  }
+#undef CLG_MMA_DIR
+}
+
+// Phase 2: warp w multiplies site w's columns (ncols_tiles m-tiles of 16
+// columns) by its links' embedding; results to t.res.
+__device__ __forceinline__ void mma16_products(Mma16Smem& t, int mtiles) {
+  const int lane = threadIdx.x & 31, i = threadIdx.x >> 5;
+  if (i >= MMA_TS) return;
+  const int g = lane >> 2, q = lane & 3;
+  // the B fragment (E^T): lane holds E[n = g][k = 2q, 2q + 1] (forward link,
+  // k < 8) and E[g][2q + 8, 2q + 9] (backward), n = colour a * 2 + re/im of
+  // the output, k = colour b = q of the input (re, im)
+  uint32_t bf[4][2];
+  const int ca = g >> 1, ri = g & 1;
+  const bool live = g < 6 && q < 3;
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu) {
+    const uint32_t m = live ? t.u[2 * mu][3 * ca + q][i] : 0u;      // U[a][b]
+    const uint32_t w = live ? t.u[2 * mu + 1][3 * q + ca][i] : 0u;  // U^+[a][b] = conj(U[b][a])
+    bf[mu][0] = ri == 0 ? (m ^ 0x80000000u) : h2_swap(m);             // (Re M, -Im M) | (Im M, Re M)
+    bf[mu][1] = ri == 0 ? w : (h2_swap(w) ^ 0x00008000u);            // M = conj(W): (Re W, Im W) | (-Im W, Re W)
+  }
+  const __half* colsite = t.col + i * MMA_SS;
+  float2* res = t.res + i * MMA_CB;
+  // ldmatrix.x4 rows: lanes 0-7 matrix 0 (columns 0-7, k 0-7), 8-15 matrix 1
+  // (columns 8-15, k 0-7), 16-23 matrix 2 (columns 0-7, k 8-15), 24-31 matrix 3
+  const int lrow = (lane & 7) + ((lane >> 3) & 1) * 8, lk = (lane >> 4) * 8;
+  for (int mt = 0; mt < mtiles; ++mt) {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const __half* cp = colsite + (mt * 16 + lrow) * MMA_CS + lk;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+      uint32_t af[4];
+      ldsm_x4(af, cp + mu * 16);
+      mma_16816(acc, af, bf[mu][0], bf[mu][1]);
+    }
+    // acc[0, 1]: column mt * 16 + g, output colour q (re, im); acc[2, 3]: column + 8
+    if (q < 3) {
+      const int c0 = mt * 16 + g, c1 = c0 + 8;  // column = rhs_local * 4 + s
+      res[(c0 >> 2) * 12 + (c0 & 3) * 3 + q] = make_float2(acc[0], acc[1]);
+      res[(c1 >> 2) * 12 + (c1 & 3) * 3 + q] = make_float2(acc[2], acc[3]);
+    }
+  }
+}
+
+template <bool DAGGER, int MINB>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_mma16_kernel(HopArgs a) {
+  extern __shared__ __align__(16) unsigned char mma_smem[];
+  Mma16Smem& t = *reinterpret_cast<Mma16Smem*>(mma_smem);
+  const int64_t h0 = tile_index<MMA_TS>(a) * MMA_TS;
+  pdl_launch_dependents();
+  mma16_stage_geometry(a, h0, t);
+  pdl_wait();
+  __syncthreads();
+  mma16_stage_links(a, h0, t);
+  for (int r0 = 0; r0 < a.nrhs; r0 += MMA_G) {
+    mma16_stage_columns<DAGGER>(a, h0, r0, t);
+    __syncthreads();
+    mma16_products(t, (min(MMA_G, a.nrhs - r0) + 3) / 4);
+    __syncthreads();
+    if (threadIdx.x < MMA_TS * MMA_G) {
+      const int i = threadIdx.x % MMA_TS, rl = threadIdx.x / MMA_TS, rhs = r0 + rl;
+      const int64_t h = h0 + i;
+      if (h < a.g.Vh && rhs < a.nrhs && !(a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride])) {
+        const float nm = t.nmax[i][rl];
+        const float2* rp = t.res + i * MMA_CB + rl * 12;
+        cpx<float> acc[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+          const float2 v = rp[k];
+          acc[k] = mk<float>(v.x * nm, v.y * nm);
+        }
+        wilson_hop_finish<P16>(a, rhs, h, acc);
+        wilson_hop_store<P16>(a, rhs, h, acc);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// The epilogue form: per right-hand side the 8 sites of the tile reduce in
+// groups of 8 lanes and write the tile's partial; tile_reduce_finalize after.
+template <bool DAGGER, int MINB, class E>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_mma16_epi_kernel(HopArgs a, E e, double* partials,
+                                                                         double* gpart, unsigned* counter,
+                                                                         unsigned group) {
+  extern __shared__ __align__(16) unsigned char mma_smem[];
+  Mma16Smem& t = *reinterpret_cast<Mma16Smem*>(mma_smem);
+  const int64_t h0 = tile_index<MMA_TS>(a) * MMA_TS;
+  pdl_launch_dependents();
+  mma16_stage_geometry(a, h0, t);
+  pdl_wait();
+  __syncthreads();
+  mma16_stage_links(a, h0, t);
+  const unsigned nslots = gridDim.x;
+  for (int r0 = 0; r0 < a.nrhs; r0 += MMA_G) {
+    mma16_stage_columns<DAGGER>(a, h0, r0, t);
+    __syncthreads();
+    mma16_products(t, (min(MMA_G, a.nrhs - r0) + 3) / 4);
+    __syncthreads();
+    if (threadIdx.x < MMA_TS * MMA_G) {
+      const int i = threadIdx.x % MMA_TS, rl = threadIdx.x / MMA_TS, rhs = r0 + rl;
+      const int64_t h = h0 + i;
+      // uniform over the 8 lanes of (rl): rhs and its skip flag
+      const bool live = rhs < a.nrhs && !(a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]);
+      double red[E::NRED];
+#pragma unroll
+      for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
+      if (live && h < a.g.Vh) {
+        const float nm = t.nmax[i][rl];
+        const float2* rp = t.res + i * MMA_CB + rl * 12;
+        cpx<float> acc[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+          const float2 v = rp[k];
+          acc[k] = mk<float>(v.x * nm, v.y * nm);
+        }
+        wilson_hop_finish<P16>(a, rhs, h, acc);
+        if constexpr (E::STORE) wilson_hop_store<P16>(a, rhs, h, acc);
+        e.site(rhs, h, acc, red);
+      }
+#pragma unroll
+      for (int k = 0; k < E::NRED; ++k) {
+        double v = red[k];
+#pragma unroll
+        for (int o = MMA_TS / 2; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o, MMA_TS);
+        if (live && i == 0) partials[((int64_t)rhs * nslots + blockIdx.x) * E::NRED + k] = v;
+      }
+      if (live && i == 0) __threadfence();
+    }
+    __syncthreads();
   }
   tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
 }

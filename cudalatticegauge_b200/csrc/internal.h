@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -112,6 +113,14 @@ struct clg_context_s {
   // the autotuner of mode 2 times it with the other two
   int hop_pair_mode = 2;
   int hop_tile_config = -1;
+  // the tensor-core form of the FP16 hop (wilson_hop_mma16_kernel) among the
+  // autotuner's candidates: CLG_HOP_MMA=1 (off by default: measured 1.91 ms
+  // against 0.63 ms for the tile form on 28 rhs of 32^3x32, bound by the
+  // latency of its three barrier-separated phases at 16 warps per SM).
+  // CLG_HOP_TILE variants 8..11 force it (variant bit 0: two blocks per SM,
+  // bit 1: the blocked tile order)
+  bool hop_mma = false;
+  std::string tune_file;  // CLG_TUNE_FILE (empty: none)
   // set by clg_solve_lattices for the duration of its solve: the per-rhs
   // checkerboard sizes (device) of the padded batch, whose site kernels skip
   // the padding (launches with this stride and right-hand-side count)
@@ -253,6 +262,21 @@ cudaError_t launch_pdl(clg_context_s* ctx, void (*kernel)(KArgs...), dim3 grid, 
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
+// Opt kernel fn into `bytes` of dynamic shared memory (above the 48 KB
+// default), once per kernel and device.
+inline cudaError_t opt_in_smem(const void* fn, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  if (cudaError_t e = cudaGetDevice(&dev)) return e;
+  std::lock_guard<std::mutex> lk(m);
+  auto it = done.find({fn, dev});
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done[{fn, dev}] = bytes;
+  return e;
+}
+
 // Autotuner: the launch configuration for kernel variant `key`.  On first use
 // (outside stream capture, when the launch is idempotent) each candidate
 // (a block size, optionally combined with a register-capped kernel variant) is
@@ -311,6 +335,9 @@ clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec
 int tuned_hop_block(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
 // the tuned launch configuration (block | variant << 16) of the paired FP16 hop
 int tuned_hop_pair_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
+// the autotuner's configuration (block | variant << 16) of this hop (FP64 /
+// FP32: variants from 16 on are the tile form)
+int tuned_hop_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);
 // the tile form's configuration (block | variant << 16), when the tile form is
 // forced or was the autotuner's choice for this hop
 int tuned_hop_tile_config(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec& s, int fallback);

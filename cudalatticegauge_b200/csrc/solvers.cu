@@ -581,8 +581,28 @@ cudaError_t launch_hop_pair_epi(clg_context_s* ctx, const HopArgs& a, const E& e
 }
 
 // the tile form (wilson_hop_tile16_epi_kernel): config as in launch_wilson_tile
+// the tensor-core form (wilson_hop_mma16_epi_kernel): config as in launch_wilson_mma
+template <bool DAG, class E>
+cudaError_t launch_hop_mma_epi(clg_context_s* ctx, const HopArgs& a0, const E& e, int cfg) {
+  HopArgs a = a0;
+  const int v = (cfg >> 16) - 24;
+  a.tile_rows = (v & 2) ? tile_rows(a.g, a.nrhs, MMA_TS) : 0;
+  const int64_t nslots = (a.g.Vh + MMA_TS - 1) / MMA_TS;
+  const unsigned group = red_group(nslots, 1);
+  double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
+  const size_t smem = sizeof(Mma16Smem);
+  auto go = [&](void (*kernel)(HopArgs, E, double*, double*, unsigned*, unsigned)) {
+    if (const cudaError_t err = opt_in_smem((const void*)kernel, smem)) return err;
+    return launch_pdl(ctx, kernel, dim3((unsigned)nslots), dim3(256), smem, a, e, ctx->red_partials, gpart,
+                      ctx->red_counter, group);
+  };
+  if (v & 1) return go(wilson_hop_mma16_epi_kernel<DAG, 2, E>);
+  return go(wilson_hop_mma16_epi_kernel<DAG, 1, E>);
+}
+
 template <bool DAG, class E>
 cudaError_t launch_hop_tile_epi(clg_context_s* ctx, const HopArgs& a0, const E& e, int cfg) {
+  if ((cfg >> 16) >= 24) return launch_hop_mma_epi<DAG>(ctx, a0, e, cfg);
   const int bs = cfg & 0xffff;
   HopArgs a = a0;
   a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
@@ -594,6 +614,23 @@ cudaError_t launch_hop_tile_epi(clg_context_s* ctx, const HopArgs& a0, const E& 
                       ctx->red_partials, gpart, ctx->red_counter, group);
   return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 2, E>, dim3((unsigned)nslots), dim3(bs), 0, a, e,
                     ctx->red_partials, gpart, ctx->red_counter, group);
+}
+
+// the FP64 / FP32 tile form (wilson_hop_tileN_epi_kernel): config as in launch_wilson_tileN
+template <int P, int RECON, bool DAG, class E>
+cudaError_t launch_hop_tileN_epi(clg_context_s* ctx, const HopArgs& a0, const E& e, int cfg) {
+  constexpr int CAP = P == P64 ? 2 : 3;
+  const int bs = cfg & 0xffff;
+  HopArgs a = a0;
+  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
+  const int64_t nslots = (a.g.Vh + TILE16 - 1) / TILE16;
+  const unsigned group = red_group(nslots, 1);
+  double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
+  if ((cfg >> 16) & 1)
+    return launch_pdl(ctx, wilson_hop_tileN_epi_kernel<P, RECON, DAG, CAP, E>, dim3((unsigned)nslots), dim3(bs), 0,
+                      a, e, ctx->red_partials, gpart, ctx->red_counter, group);
+  return launch_pdl(ctx, wilson_hop_tileN_epi_kernel<P, RECON, DAG, 1, E>, dim3((unsigned)nslots), dim3(bs), 0, a,
+                    e, ctx->red_partials, gpart, ctx->red_counter, group);
 }
 
 template <int P, int RECON, bool DAG, class E>
@@ -641,7 +678,7 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
   if constexpr (P == P16) {
     const int tcfg = w.nrhs >= 2 && !a.seg ? tuned_hop_tile_config(ctx, w.U, plain, -1) : -1;
     if (tcfg >= 0) {
-      const int64_t nslots = (w.Vh + TILE16 - 1) / TILE16;
+      const int64_t nslots = (w.Vh + ((tcfg >> 16) >= 24 ? MMA_TS : TILE16) - 1) / ((tcfg >> 16) >= 24 ? MMA_TS : TILE16);
       if (clg_status st = ensure_reduction(ctx, red2_doubles(nslots, w.nrhs, 1, E::NRED))) return st;
       const cudaError_t terr = dag ? launch_hop_tile_epi<true>(ctx, a, e, tcfg) : launch_hop_tile_epi<false>(ctx, a, e, tcfg);
       if (terr != cudaSuccess) return ctx->fail(cuda_status(terr), std::string("fused hop: ") + cudaGetErrorString(terr));
@@ -657,6 +694,23 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
         return st;
       const cudaError_t perr = dag ? launch_hop_pair_epi<true>(ctx, a, e, cfg) : launch_hop_pair_epi<false>(ctx, a, e, cfg);
       if (perr != cudaSuccess) return ctx->fail(cuda_status(perr), std::string("fused hop: ") + cudaGetErrorString(perr));
+      return CLG_SUCCESS;
+    }
+  }
+  if constexpr (P != P16) {
+    // the tile form, when the autotuner chose it for the plain hop
+    const int pc = w.nrhs >= 2 && !a.seg ? tuned_hop_config(ctx, w.U, plain, -1) : -1;
+    if (pc >= 0 && (pc >> 16) >= 16) {
+      const int64_t nslots = (w.Vh + TILE16 - 1) / TILE16;
+      if (clg_status st = ensure_reduction(ctx, red2_doubles(nslots, w.nrhs, 1, E::NRED))) return st;
+      cudaError_t terr;
+      if constexpr (P == P64)
+        terr = dag ? launch_hop_tileN_epi<P, 18, true>(ctx, a, e, pc) : launch_hop_tileN_epi<P, 18, false>(ctx, a, e, pc);
+      else if (w.U->recon32 == 12)
+        terr = dag ? launch_hop_tileN_epi<P, 12, true>(ctx, a, e, pc) : launch_hop_tileN_epi<P, 12, false>(ctx, a, e, pc);
+      else
+        terr = dag ? launch_hop_tileN_epi<P, 18, true>(ctx, a, e, pc) : launch_hop_tileN_epi<P, 18, false>(ctx, a, e, pc);
+      if (terr != cudaSuccess) return ctx->fail(cuda_status(terr), std::string("fused hop: ") + cudaGetErrorString(terr));
       return CLG_SUCCESS;
     }
   }

@@ -3,7 +3,9 @@
 The autotuner picks one variant per operator and lattice, so the tuned runs
 of the other tests exercise only the winner.  Here each variant is pinned
 through CLG_HOP_CONFIG ("<variant>:<block>", read when a context is created):
-0 = plain, 1 = capped at 80 registers, 2 = capped at 72.  Lattices with a partial last
+0 = plain, 1 = capped at 80 registers, 2 = capped at 72, 3 = FP64 capped at
+128; 16..19 the FP64 / FP32 tile form (32 sites per block, links staged once
+for all right-hand sides; bit 0 the register cap, bit 1 the blocked order).  Lattices with a partial last
 block per checkerboard and two right-hand sides (the rhs strides and FP16
 norms) are included.  Tolerances as in test_gpu_dslash: FP32 2e-6, FP16 storage 5e-3.
 """
@@ -42,7 +44,7 @@ def monkeypatch_module():
     mp.undo()
 
 
-@pytest.mark.parametrize("cfg", CONFIGS + ["3:64", "3:128", "3:256"])
+@pytest.mark.parametrize("cfg", CONFIGS + ["3:64", "3:128", "3:256", "16:128", "17:96", "18:256", "19:64"])
 @pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 2e-6), (2, 5e-3)])
 @pytest.mark.parametrize("dims", [(8, 8, 8, 8), (4, 6, 4, 10)])
 def test_hop_variant(clg, oracle, pinned, cfg, prec, tol, dims):
@@ -250,3 +252,101 @@ def test_fp16_tile_cg_epilogues(ctx_single, ctx_tiles, clg, oracle, cfg):
     for r in range(nrhs):
         assert abs(res[0][0][r] - res[1][0][r]) <= max(3, res[0][0][r] // 20), (res[0][0], res[1][0])
         assert op.true_residual(res[1][3][r], res[1][1][r]) <= 1e-10
+
+
+MMA_CONFIGS = ["8:8", "8:11"]
+
+
+@pytest.mark.parametrize("cfg", MMA_CONFIGS)
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 10, 14, 12)])
+@pytest.mark.parametrize("nrhs", [2, 5, 17])
+@pytest.mark.parametrize("dagger", [False, True])
+def test_fp16_mma_hop_vs_oracle(ctx_tiles, clg, oracle, cfg, dims, nrhs, dagger):
+    """The tensor-core form (CLG_HOP_TILE="8:8", "8:11": mma.sync colour
+    products, 8 sites per block, right-hand sides in groups of 16) against the
+    FP64 oracle's M_ee (and M_ee^+) within the FP16 tolerance, with a partial
+    last tile (6x10x14x12) and a partial last group (17 rhs)."""
+    c = ctx_tiles(cfg)
+    lat = clg.Lattice(c, dims)
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+    Uh = U.CopyDataOut()
+    pm = clg.eo_parity(dims)
+    f = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF, nrhs=nrhs)
+    src = []
+    for r in range(nrhs):
+        g = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN)
+        g.InitialField(clg.SOURCE_GAUSS, 800 + r, 2)
+        src.append(g.to_numpy())
+        f.from_numpy(src[-1], rhs=r)
+    f.ApplyOperator(clg.OP_MEE_DAG if dagger else clg.OP_MEE, U)
+    for r in range(nrhs):
+        want = oracle.wilson_mee(dims, Uh, src[r], KAPPA, dagger=dagger)[pm == 0]
+        assert rel(f.to_numpy(r)[pm == 0], want) < 5e-3, (cfg, dims, nrhs, dagger, r)
+
+
+@pytest.mark.parametrize("cfg", MMA_CONFIGS)
+def test_fp16_mma_cg_epilogues(ctx_tiles, clg, oracle, cfg):
+    """CGNE with the tensor-core form's fused epilogues converges to 1e-10 by
+    the oracle's residual on five right-hand sides that finish at different
+    iterations."""
+    nrhs = 5
+    c = ctx_tiles(cfg)
+    lat = clg.Lattice(c, (8, 8, 8, 16))
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=nrhs)
+    for r in range(nrhs):
+        b.InitialField(clg.SOURCE_GAUSS if r % 2 else clg.SOURCE_Z2, 700 + r, 2, rhs=r)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=nrhs)
+    S = clg.CSLASolverCG(c, inner_precision=clg.HALF, tol_true_rel=1e-10)
+    infos = S.Solve(x, b, U, clg.EFO_F_D)
+    op = oracle.Operator("WILSON_D", (8, 8, 8, 16), U.CopyDataOut(), KAPPA)
+    for r in range(nrhs):
+        assert infos[r]["status"] == 0
+        assert op.true_residual(b.to_numpy(r), x.to_numpy(r)) <= 1e-10
+
+
+@pytest.mark.parametrize("cfg", ["16:128", "19:256"])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_tileN_bit_identical(clg, pinned, cfg, prec):
+    """The FP64 tile form gives the same bits as the one-rhs kernel (pinned
+    "0:128") on 5 right-hand sides, in D and D^+; FP32 agrees to its rounding
+    (the compiler contracts the products of the rebuilt third link row into
+    FMAs differently in the two kernels)."""
+    outs = []
+    for c in (pinned("0:128"), pinned(cfg)):
+        lat = clg.Lattice(c, (8, 8, 8, 16))
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+        f = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, precision=prec, nrhs=5)
+        for r in range(5):
+            f.InitialField(clg.SOURCE_GAUSS, 900 + r, 2, rhs=r)
+        f.D(U)
+        f.Ddagger(U)
+        outs.append([f.to_numpy(r) for r in range(5)])
+    for r in range(5):
+        if prec == 0:
+            np.testing.assert_array_equal(outs[0][r], outs[1][r])
+        else:
+            assert rel(outs[1][r], outs[0][r]) < 2e-6
+
+
+@pytest.mark.parametrize("cfg", ["17:128", "18:224"])
+def test_tileN_cg_fp64(clg, oracle, pinned, cfg):
+    """FP64 CGNE with the tile form's fused epilogues (four right-hand sides,
+    7 warps for 4 rhs in "18:224") converges to 1e-10 by the oracle."""
+    c = pinned(cfg)
+    lat = clg.Lattice(c, (8, 8, 8, 16))
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=4)
+    for r in range(4):
+        b.InitialField(clg.SOURCE_GAUSS, 950 + r, 2, rhs=r)
+    x = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, nrhs=4)
+    S = clg.CSLASolverCG(c, inner_precision=clg.DOUBLE, tol_true_rel=1e-10)
+    infos = S.Solve(x, b, U, clg.EFO_F_D)
+    op = oracle.Operator("WILSON_D", (8, 8, 8, 16), U.CopyDataOut(), KAPPA)
+    for r in range(4):
+        assert infos[r]["status"] == 0
+        assert op.true_residual(b.to_numpy(r), x.to_numpy(r)) <= 1e-10
