@@ -231,6 +231,18 @@ def time_hops(clg, ctx, lat, U, prec, stream, reps=60, nrhs=1):
     return t, launches
 
 
+def hop_form_id(ctx, prec, Vh, nrhs):
+    """Short name of the autotuner's Wilson hop form for D_eo at this size."""
+    key = f"wilson_p{prec}_d0_V{Vh}_n{nrhs}_r{12 if prec == 1 else 0}"
+    tuned = ctx.tuned()
+    bs, v = tuned.get(key + "_auto", tuned.get(key, (0, 0)))
+    if v >= 24:
+        return "mma"
+    if v >= 16:
+        return "tile_blocked" if v & 2 else "tile_site"
+    return "pair" if v >= 8 else "one"
+
+
 def hop_form(ctx, prec, Vh, nrhs):
     """The Wilson hop kernel the autotuner chose for D_eo at this size."""
     key = f"wilson_p{prec}_d0_V{Vh}_n{nrhs}_r{12 if prec == 1 else 0}"
@@ -378,7 +390,8 @@ def ours(args, world, rank, local):
     tp = os.path.join(ROOT, "profiles", "hop_traffic.json")
     if os.path.exists(tp):
         d = json.load(open(tp))
-        ent = d.get(pname + ("" if nrhs == 1 else f"_{nrhs}rhs"), {})
+        form = hop_form_id(ctx, inner, Vh, nrhs)
+        ent = d.get(pname + ("" if nrhs == 1 else f"_{nrhs}rhs" + ("" if form in ("one", "pair") else "_" + form)), {})
         if tuple(ent.get("dims", d.get("dims", ()))) == tuple(W["dims"]):
             traffic = ent.get("bytes_per_launch")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
