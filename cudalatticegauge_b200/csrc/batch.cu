@@ -10,7 +10,10 @@
 // structure-of-arrays layout with the chunk stride of the largest checkerboard
 // of the set; the sites past a lattice's own checkerboard are padding that
 // stays zero.  The hop kernels take the lattice of each right-hand side from a
-// device table (HopSeg: geometry and link arrays per right-hand side), and the
+// device table (HopSeg: geometry and link arrays per right-hand side; the tile
+// form's blocks are the tiles of 32 sites of each lattice in turn, BatchTile,
+// so no block works on padding and each lattice's links are staged once per
+// tile for all its right-hand sides), and the
 // vector kernels skip the padding (site_reduce_batch_kernel with the per-rhs
 // checkerboard sizes; the padding is zero either way).  So one iteration of the
 // inner Krylov method is the same fixed number of launches whatever the number
@@ -34,6 +37,7 @@ struct BatchWork : SolveCacheBase {
   clg_gauge_s vgauge;        // its "gauge field": the per-rhs HopSeg table
   HopSeg* seg_dev = nullptr;
   int64_t* vh_dev = nullptr;  // per-rhs checkerboard sizes
+  BatchTile* tile_dev = nullptr;  // per lattice: its tiles of 32 sites and right-hand sides
   void* b_data = nullptr;
   void* x_data = nullptr;
   FieldRef B, X;             // FP64 full fields, padded
@@ -43,6 +47,7 @@ struct BatchWork : SolveCacheBase {
     solve_cache.reset();
     dfree(seg_dev);
     dfree(vh_dev);
+    dfree(tile_dev);
     dfree(b_data);
     dfree(x_data);
   }
@@ -123,7 +128,16 @@ extern "C" clg_status clg_solve_lattices(clg_solver S, int n, clg_field* x, clg_
     nw->vgauge.dirty_lowp = false;
     std::vector<HopSeg> segs;
     std::vector<int64_t> vhs;
-    for (int i = 0; i < n; ++i)
+    std::vector<BatchTile> tiles;
+    int64_t ntiles = 0;
+    for (int i = 0; i < n; ++i) {
+      BatchTile bt;
+      bt.tile0 = ntiles;
+      bt.rhs0 = (int)segs.size();
+      bt.nrhs = b[i]->nrhs;
+      bt.seg = (int)segs.size();
+      tiles.push_back(bt);
+      ntiles += (b[i]->lat->g.Vh + TILE16 - 1) / TILE16;
       for (int r = 0; r < b[i]->nrhs; ++r) {
         HopSeg sg;
         sg.g = b[i]->lat->g;
@@ -135,10 +149,12 @@ extern "C" clg_status clg_solve_lattices(clg_solver S, int n, clg_field* x, clg_
         segs.push_back(sg);
         vhs.push_back(b[i]->lat->g.Vh);
       }
+    }
     const size_t fbytes = (size_t)vh_max * nc * 16 * 2 * total;
     clg_status st;
     if ((st = dalloc(ctx, (void**)&nw->seg_dev, sizeof(HopSeg) * segs.size())) ||
         (st = dalloc(ctx, (void**)&nw->vh_dev, sizeof(int64_t) * vhs.size())) ||
+        (st = dalloc(ctx, (void**)&nw->tile_dev, sizeof(BatchTile) * tiles.size())) ||
         (st = dalloc(ctx, &nw->b_data, fbytes)) || (st = dalloc(ctx, &nw->x_data, fbytes)))
       return st;
     cudaMemsetAsync(nw->b_data, 0, fbytes, ctx->stream);
@@ -147,10 +163,15 @@ extern "C" clg_status clg_solve_lattices(clg_solver S, int n, clg_field* x, clg_
             cudaSuccess ||
         cudaMemcpyAsync(nw->vh_dev, vhs.data(), sizeof(int64_t) * vhs.size(), cudaMemcpyHostToDevice, ctx->stream) !=
             cudaSuccess ||
+        cudaMemcpyAsync(nw->tile_dev, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess)
       return ctx->fail(CLG_ERR_CUDA, "solve_lattices: table upload");
     nw->vgauge.seg = nw->seg_dev;
     nw->vgauge.seg_vh = nw->vh_dev;
+    nw->vgauge.btile = nw->tile_dev;
+    nw->vgauge.nbtile = (int)tiles.size();
+    nw->vgauge.btiles = ntiles;
     nw->B = padded_full(static_cast<char*>(nw->b_data), nc, total, vh_max);
     nw->X = padded_full(static_cast<char*>(nw->x_data), nc, total, vh_max);
     nw->key = key;

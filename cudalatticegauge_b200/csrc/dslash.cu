@@ -108,6 +108,18 @@ cudaError_t launch_wilson_pair(clg_context_s* ctx, const HopArgs& a, bool dagger
 // a batch of lattices: one right-hand side per lattice segment, untuned
 template <int P, int RECON>
 cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagger) {
+  if (a.btile) {
+    // the tile form, one block per tile of 32 sites of one lattice (4 warps;
+    // FP16 / FP32 capped at 80 registers, FP64 at 128)
+    constexpr int CAP = P == P64 ? 2 : 3;
+    const dim3 grid((unsigned)a.btiles), block(128);
+    if constexpr (P == P16)
+      return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, CAP, true>, grid, block, 0, a)
+                    : launch_pdl(ctx, wilson_hop_tile16_kernel<false, CAP, true>, grid, block, 0, a);
+    else
+      return dagger ? launch_pdl(ctx, wilson_hop_tileN_kernel<P, RECON, true, CAP, true>, grid, block, 0, a)
+                    : launch_pdl(ctx, wilson_hop_tileN_kernel<P, RECON, false, CAP, true>, grid, block, 0, a);
+  }
   const int bs = P == P64 ? 64 : 128;
   dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * a.nrhs));
   return dagger ? launch_pdl(ctx, wilson_hop_batch_kernel<P, RECON, true>, grid, dim3(bs), 0, a)
@@ -405,6 +417,9 @@ clg_status make_hop_args(clg_context_s* ctx, const clg_gauge_s* U, const HopSpec
   a.seg = U->seg;
   a.seg_vh = U->seg_vh;
   a.tile_rows = 0;
+  a.btile = U->btile;
+  a.nbtile = U->nbtile;
+  a.btiles = U->btiles;
   if (U->seg) {
     if (s.kind != CLG_FERMION_WILSON) return ctx->fail(CLG_ERR_UNSUPPORTED, "a batch of lattices takes Wilson fermions");
     a.U_here = a.U_there = nullptr;

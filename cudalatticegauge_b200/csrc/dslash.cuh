@@ -62,7 +62,23 @@ struct HopArgs {
   // the tile hops' block order (wilson_hop_tile16_kernel): 0 = tiles in site
   // order, else the rows y are walked in chunks of tile_rows (tile16_index)
   int tile_rows;
+  // a batch of lattices, tile form: lattice l's tiles are the blocks
+  // [btile[l].tile0, btile[l + 1].tile0), its right-hand sides
+  // [rhs0, rhs0 + nrhs), its geometry and links those of seg[btile[l].seg]
+  const struct BatchTile* btile;
+  int nbtile;
+  int64_t btiles;  // blocks of the batch (all lattices' tiles)
 };
+struct BatchTile {
+  int64_t tile0;
+  int rhs0, nrhs, seg;
+};
+// the lattice of batch block b (a handful of lattices: a linear scan)
+__device__ __forceinline__ BatchTile batch_tile(const HopArgs& a) {
+  int l = 0;
+  while (l + 1 < a.nbtile && a.btile[l + 1].tile0 <= (int64_t)blockIdx.x) ++l;
+  return a.btile[l];
+}
 
 // chiral gamma tables (GammaMatrix.h:447-478): row r -> column perm[r] with phase i^z4[r]
 __device__ __forceinline__ constexpr int gperm(int mu, int r) {
@@ -829,14 +845,14 @@ __device__ __forceinline__ int64_t tile16_index(const HopArgs& a) { return tile_
 // The neighbours of the tile's sites (geometry only: no memory is read, so
 // this runs before the wait on the previous kernel)
 template <class T>
-__device__ __forceinline__ void tile16_neighbours(const HopArgs& a, int64_t h0, T& t) {
+__device__ __forceinline__ void tile16_neighbours(const Geom& g, int parity, int64_t h0, T& t) {
   for (int i = threadIdx.x; i < TILE16; i += blockDim.x) {
     const int64_t h = h0 + i;
     uint32_t neg = 0;
-    if (h < a.g.Vh) {
+    if (h < g.Vh) {
       NbrInfo nb;
       int c[4];
-      neighbours(a.g, a.out_parity, h, nb, c);
+      neighbours(g, parity, h, nb, c);
 #pragma unroll
       for (int mu = 0; mu < 4; ++mu) {
         t.nb[mu][i] = nb.hf[mu];
@@ -852,18 +868,20 @@ __device__ __forceinline__ void tile16_neighbours(const HopArgs& a, int64_t h0, 
   }
 }
 
-// The tile's links, third row rebuilt (after tile16_neighbours and a barrier)
-__device__ __forceinline__ void tile16_links(const HopArgs& a, int64_t h0, Tile16& t) {
+// The tile's links, third row rebuilt (after tile16_neighbours and a barrier);
+// Uh / Ut the link arrays of the output / input parity, Vh the lattice's
+// checkerboard size (their stride)
+__device__ __forceinline__ void tile16_links(const void* Uh, const void* Ut, int64_t Vh, int64_t h0, Tile16& t) {
   for (int k = threadIdx.x; k < 8 * TILE16; k += blockDim.x) {
     const int d = k / TILE16, i = k % TILE16;
     const int64_t h = h0 + i;
     uint32_t u[9] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-    if (h < a.g.Vh) {
+    if (h < Vh) {
       PackedLink16 l;
       if (d < 4)
-        load_packed_link16(a.U_here, d, a.g.Vh, h, l);
+        load_packed_link16(Uh, d, Vh, h, l);
       else
-        load_packed_link16(a.U_there, d - 4, a.g.Vh, t.nb[d][i], l);
+        load_packed_link16(Ut, d - 4, Vh, t.nb[d][i], l);
       u[0] = l.a.x; u[1] = l.a.y; u[2] = l.a.z; u[3] = l.a.w; u[4] = l.b.x; u[5] = l.b.y;
       link16_third_row(u);
     }
@@ -912,22 +930,22 @@ __device__ __forceinline__ void wilson_hop_site_tile16(const HopArgs& a, const T
   wilson_hop_finish<P16>(a, rhs, h, acc);
 }
 
-// One block per tile of 32 output sites, blockDim = 32 x (warps sharing the
-// right-hand sides); MINB 2 leaves the registers uncapped (128), 3 caps at 80.
-template <bool DAGGER, int MINB>
-__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_kernel(HopArgs a) {
-  __shared__ Tile16 t;
-  const int64_t h0 = tile16_index(a) * TILE16;
+// The work of one tile block: lattice g (links Uh, Ut), output sites
+// [h0, h0 + 32), right-hand sides [r0, r1).  In a batch of lattices g is one
+// lattice of the batch and a.g.Vh the fields' (padded) chunk stride.
+template <bool DAGGER>
+__device__ __forceinline__ void tile16_body(const HopArgs& a, Tile16& t, const Geom& g, const void* Uh,
+                                            const void* Ut, int64_t h0, int r0, int r1) {
   pdl_launch_dependents();
-  tile16_neighbours(a, h0, t);
+  tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
   __syncthreads();
-  tile16_links(a, h0, t);
+  tile16_links(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int64_t h = h0 + lane;
-  if (h >= a.g.Vh) return;  // no barrier follows
-  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+  if (h >= g.Vh) return;  // no barrier follows
+  for (int rhs = r0 + (threadIdx.x >> 5); rhs < r1; rhs += nw) {
     if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
     cpx<float> acc[12];
     wilson_hop_site_tile16<DAGGER>(a, t, lane, rhs, h, acc);
@@ -935,30 +953,47 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_kernel(HopArgs a)
   }
 }
 
-// The tile form of wilson_hop_epi_kernel: per right-hand side the warp
-// reduces its 32 sites and writes the tile's partial (slot = tile); the tiles
-// then reduce in two levels (tile_reduce_finalize).
-template <bool DAGGER, int MINB, class E>
-__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_epi_kernel(HopArgs a, E e, double* partials,
-                                                                          double* gpart, unsigned* counter,
-                                                                          unsigned group) {
+// One block per tile of 32 output sites, blockDim = 32 x (warps sharing the
+// right-hand sides); MINB 2 leaves the registers uncapped (128), 3 caps at 80.
+// BATCH: a batch of lattices, one block per tile of one lattice (btile).
+template <bool DAGGER, int MINB, bool BATCH = false>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_kernel(HopArgs a) {
   __shared__ Tile16 t;
-  const int64_t h0 = tile16_index(a) * TILE16;
+  if constexpr (BATCH) {
+    const BatchTile bt = batch_tile(a);
+    const HopSeg& sg = a.seg[bt.seg];
+    const Geom g = sg.g;
+    tile16_body<DAGGER>(a, t, g, sg.u[2][a.out_parity], sg.u[2][1 - a.out_parity],
+                        ((int64_t)blockIdx.x - bt.tile0) * TILE16, bt.rhs0, bt.rhs0 + bt.nrhs);
+  } else {
+    tile16_body<DAGGER>(a, t, a.g, a.U_here, a.U_there, tile16_index(a) * TILE16, 0, a.nrhs);
+  }
+}
+
+// The epilogue form of tile16_body: per right-hand side the warp reduces its
+// 32 sites and writes the tile's partial (slot = block); in a batch the block
+// writes zero partials for the other lattices' right-hand sides.  The blocks
+// then reduce in two levels (tile_reduce_finalize).
+template <bool DAGGER, class E>
+__device__ __forceinline__ void tile16_epi_body(const HopArgs& a, const E& e, Tile16& t, const Geom& g,
+                                                const void* Uh, const void* Ut, int64_t h0, int r0, int r1,
+                                                double* partials, double* gpart, unsigned* counter,
+                                                unsigned group) {
   pdl_launch_dependents();
-  tile16_neighbours(a, h0, t);
+  tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
   __syncthreads();
-  tile16_links(a, h0, t);
+  tile16_links(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int64_t h = h0 + lane;
   const unsigned nslots = gridDim.x;
-  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+  for (int rhs = r0 + (threadIdx.x >> 5); rhs < r1; rhs += nw) {
     if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
     double red[E::NRED];
 #pragma unroll
     for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
-    if (h < a.g.Vh) {
+    if (h < g.Vh) {
       cpx<float> acc[12];
       wilson_hop_site_tile16<DAGGER>(a, t, lane, rhs, h, acc);
       if constexpr (E::STORE) wilson_hop_store<P16>(a, rhs, h, acc);
@@ -973,7 +1008,32 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_epi_kernel(HopArg
     }
     if (lane == 0) __threadfence();
   }
+  if (r0 > 0 || r1 < a.nrhs) {
+    for (int q = threadIdx.x; q < a.nrhs * E::NRED; q += blockDim.x) {
+      const int rhs = q / E::NRED;
+      if (rhs < r0 || rhs >= r1) partials[((int64_t)rhs * nslots + blockIdx.x) * E::NRED + q % E::NRED] = 0.0;
+    }
+    __threadfence();
+  }
   tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
+}
+
+template <bool DAGGER, int MINB, class E, bool BATCH = false>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_epi_kernel(HopArgs a, E e, double* partials,
+                                                                          double* gpart, unsigned* counter,
+                                                                          unsigned group) {
+  __shared__ Tile16 t;
+  if constexpr (BATCH) {
+    const BatchTile bt = batch_tile(a);
+    const HopSeg& sg = a.seg[bt.seg];
+    const Geom g = sg.g;
+    tile16_epi_body<DAGGER>(a, e, t, g, sg.u[2][a.out_parity], sg.u[2][1 - a.out_parity],
+                            ((int64_t)blockIdx.x - bt.tile0) * TILE16, bt.rhs0, bt.rhs0 + bt.nrhs, partials,
+                            gpart, counter, group);
+  } else {
+    tile16_epi_body<DAGGER>(a, e, t, a.g, a.U_here, a.U_there, tile16_index(a) * TILE16, 0, a.nrhs, partials,
+                            gpart, counter, group);
+  }
 }
 
 // ---------------------------------------------------------------- FP64 / FP32, a tile of sites for every right-hand side
@@ -992,16 +1052,16 @@ struct TileN {
 };
 
 template <int P, int RECON, typename AT>
-__device__ __forceinline__ void tileN_links(const HopArgs& a, int64_t h0, TileN<AT>& t) {
+__device__ __forceinline__ void tileN_links(const void* Uh, const void* Ut, int64_t Vh, int64_t h0, TileN<AT>& t) {
   for (int k = threadIdx.x; k < 8 * TILE16; k += blockDim.x) {
     const int d = k / TILE16, i = k % TILE16;
     const int64_t h = h0 + i;
     cpx<AT> u[9];
-    if (h < a.g.Vh) {
+    if (h < Vh) {
       if (d < 4)
-        load_link<P, RECON, AT>(a.U_here, d, a.g.Vh, h, u);
+        load_link<P, RECON, AT>(Uh, d, Vh, h, u);
       else
-        load_link<P, RECON, AT>(a.U_there, d - 4, a.g.Vh, t.nb[d][i], u);
+        load_link<P, RECON, AT>(Ut, d - 4, Vh, t.nb[d][i], u);
     } else {
 #pragma unroll
       for (int w = 0; w < 9; ++w) u[w] = mk<AT>(0, 0);
@@ -1040,21 +1100,19 @@ __device__ __forceinline__ void wilson_hop_site_tileN(const HopArgs& a, const Ti
   wilson_hop_finish<P>(a, rhs, h, acc);
 }
 
-template <int P, int RECON, bool DAGGER, int MINB>
-__global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_kernel(HopArgs a) {
-  using AT = typename AccT<P>::T;
-  __shared__ TileN<AT> t;
-  const int64_t h0 = tile16_index(a) * TILE16;
+template <int P, int RECON, bool DAGGER, typename AT>
+__device__ __forceinline__ void tileN_body(const HopArgs& a, TileN<AT>& t, const Geom& g, const void* Uh,
+                                           const void* Ut, int64_t h0, int r0, int r1) {
   pdl_launch_dependents();
-  tile16_neighbours(a, h0, t);
+  tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
   __syncthreads();
-  tileN_links<P, RECON>(a, h0, t);
+  tileN_links<P, RECON>(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int64_t h = h0 + lane;
-  if (h >= a.g.Vh) return;  // no barrier follows
-  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+  if (h >= g.Vh) return;  // no barrier follows
+  for (int rhs = r0 + (threadIdx.x >> 5); rhs < r1; rhs += nw) {
     if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
     cpx<AT> acc[12];
     wilson_hop_site_tileN<P, DAGGER>(a, t, lane, rhs, h, acc);
@@ -1062,28 +1120,40 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_kernel(HopArgs a) 
   }
 }
 
-template <int P, int RECON, bool DAGGER, int MINB, class E>
-__global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_epi_kernel(HopArgs a, E e, double* partials,
-                                                                         double* gpart, unsigned* counter,
-                                                                         unsigned group) {
+template <int P, int RECON, bool DAGGER, int MINB, bool BATCH = false>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_kernel(HopArgs a) {
   using AT = typename AccT<P>::T;
   __shared__ TileN<AT> t;
-  const int64_t h0 = tile16_index(a) * TILE16;
+  if constexpr (BATCH) {
+    const BatchTile bt = batch_tile(a);
+    const HopSeg& sg = a.seg[bt.seg];
+    const Geom g = sg.g;
+    tileN_body<P, RECON, DAGGER>(a, t, g, sg.u[seg_prec<P>()][a.out_parity], sg.u[seg_prec<P>()][1 - a.out_parity],
+                                 ((int64_t)blockIdx.x - bt.tile0) * TILE16, bt.rhs0, bt.rhs0 + bt.nrhs);
+  } else {
+    tileN_body<P, RECON, DAGGER>(a, t, a.g, a.U_here, a.U_there, tile16_index(a) * TILE16, 0, a.nrhs);
+  }
+}
+
+template <int P, int RECON, bool DAGGER, class E, typename AT>
+__device__ __forceinline__ void tileN_epi_body(const HopArgs& a, const E& e, TileN<AT>& t, const Geom& g,
+                                               const void* Uh, const void* Ut, int64_t h0, int r0, int r1,
+                                               double* partials, double* gpart, unsigned* counter, unsigned group) {
   pdl_launch_dependents();
-  tile16_neighbours(a, h0, t);
+  tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
   __syncthreads();
-  tileN_links<P, RECON>(a, h0, t);
+  tileN_links<P, RECON>(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int64_t h = h0 + lane;
   const unsigned nslots = gridDim.x;
-  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+  for (int rhs = r0 + (threadIdx.x >> 5); rhs < r1; rhs += nw) {
     if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
     double red[E::NRED];
 #pragma unroll
     for (int k = 0; k < E::NRED; ++k) red[k] = 0.0;
-    if (h < a.g.Vh) {
+    if (h < g.Vh) {
       cpx<AT> acc[12];
       wilson_hop_site_tileN<P, DAGGER>(a, t, lane, rhs, h, acc);
       if constexpr (E::STORE) wilson_hop_store<P>(a, rhs, h, acc);
@@ -1098,7 +1168,33 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_epi_kernel(HopArgs
     }
     if (lane == 0) __threadfence();
   }
+  if (r0 > 0 || r1 < a.nrhs) {
+    for (int q = threadIdx.x; q < a.nrhs * E::NRED; q += blockDim.x) {
+      const int rhs = q / E::NRED;
+      if (rhs < r0 || rhs >= r1) partials[((int64_t)rhs * nslots + blockIdx.x) * E::NRED + q % E::NRED] = 0.0;
+    }
+    __threadfence();
+  }
   tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
+}
+
+template <int P, int RECON, bool DAGGER, int MINB, class E, bool BATCH = false>
+__global__ void __launch_bounds__(256, MINB) wilson_hop_tileN_epi_kernel(HopArgs a, E e, double* partials,
+                                                                         double* gpart, unsigned* counter,
+                                                                         unsigned group) {
+  using AT = typename AccT<P>::T;
+  __shared__ TileN<AT> t;
+  if constexpr (BATCH) {
+    const BatchTile bt = batch_tile(a);
+    const HopSeg& sg = a.seg[bt.seg];
+    const Geom g = sg.g;
+    tileN_epi_body<P, RECON, DAGGER>(a, e, t, g, sg.u[seg_prec<P>()][a.out_parity],
+                                     sg.u[seg_prec<P>()][1 - a.out_parity], ((int64_t)blockIdx.x - bt.tile0) * TILE16,
+                                     bt.rhs0, bt.rhs0 + bt.nrhs, partials, gpart, counter, group);
+  } else {
+    tileN_epi_body<P, RECON, DAGGER>(a, e, t, a.g, a.U_here, a.U_there, tile16_index(a) * TILE16, 0, a.nrhs, partials,
+                                     gpart, counter, group);
+  }
 }
 
 // ---------------------------------------------------------------- FP16 with the colour products on the tensor cores

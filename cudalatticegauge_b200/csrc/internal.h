@@ -152,7 +152,8 @@ struct clg_lattice_s {
 };
 
 namespace clg {
-struct HopSeg;  // dslash.cuh
+struct HopSeg;     // dslash.cuh
+struct BatchTile;  // dslash.cuh
 }
 
 struct clg_gauge_s {
@@ -161,6 +162,10 @@ struct clg_gauge_s {
   // link arrays on the device; lat is then the batch's padded virtual lattice
   const clg::HopSeg* seg = nullptr;
   const int64_t* seg_vh = nullptr;  // per right-hand side checkerboard sizes (device)
+  // the batch's tiles of 32 sites per lattice (device; the tile-form hops)
+  const clg::BatchTile* btile = nullptr;
+  int nbtile = 0;
+  int64_t btiles = 0;
   // per parity link arrays [mu][chunk][h]
   void* u64[2] = {nullptr, nullptr};   // FP64, 18 reals
   void* u32[2] = {nullptr, nullptr};   // FP32, 12 reals (SU(3)) or 18

@@ -633,6 +633,23 @@ cudaError_t launch_hop_tileN_epi(clg_context_s* ctx, const HopArgs& a0, const E&
                     e, ctx->red_partials, gpart, ctx->red_counter, group);
 }
 
+// a batch of lattices in the tile form (wilson_hop_tile16_epi_kernel /
+// wilson_hop_tileN_epi_kernel with BATCH): one block per tile of one lattice
+template <int P, int RECON, bool DAG, class E>
+cudaError_t launch_hop_batch_tile_epi(clg_context_s* ctx, const HopArgs& a, const E& e) {
+  constexpr int CAP = P == P64 ? 2 : 3;
+  const int64_t nslots = a.btiles;
+  const unsigned group = red_group(nslots, 1);
+  double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
+  const dim3 grid((unsigned)nslots), block(128);
+  if constexpr (P == P16)
+    return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, CAP, E, true>, grid, block, 0, a, e, ctx->red_partials,
+                      gpart, ctx->red_counter, group);
+  else
+    return launch_pdl(ctx, wilson_hop_tileN_epi_kernel<P, RECON, DAG, CAP, E, true>, grid, block, 0, a, e,
+                      ctx->red_partials, gpart, ctx->red_counter, group);
+}
+
 template <int P, int RECON, bool DAG, class E>
 cudaError_t launch_hop_epi(clg_context_s* ctx, const HopArgs& a, const E& e, int bs) {
   const int64_t nslots = (a.g.Vh + bs - 1) / bs;
@@ -670,6 +687,16 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
   s.nrhs = w.nrhs;
   HopArgs a;
   if (clg_status st = make_hop_args(ctx, w.U, s, a)) return st;
+  if (a.seg && a.btile) {  // a batch of lattices: the tile form
+    if (clg_status st = ensure_reduction(ctx, red2_doubles(a.btiles, w.nrhs, 1, E::NRED))) return st;
+    cudaError_t berr;
+    if constexpr (P == P64)
+      berr = dag ? launch_hop_batch_tile_epi<P, 18, true>(ctx, a, e) : launch_hop_batch_tile_epi<P, 18, false>(ctx, a, e);
+    else
+      berr = dag ? launch_hop_batch_tile_epi<P, 12, true>(ctx, a, e) : launch_hop_batch_tile_epi<P, 12, false>(ctx, a, e);
+    if (berr != cudaSuccess) return ctx->fail(cuda_status(berr), std::string("fused hop: ") + cudaGetErrorString(berr));
+    return CLG_SUCCESS;
+  }
   // the block size tuned for the plain hop of the same kind (the hops on the
   // odd checkerboard of each iteration run first and are tuned)
   HopSpec plain = s;
