@@ -1506,6 +1506,36 @@ __global__ void __launch_bounds__(256, MINB) wilson_hop_mma16_epi_kernel(HopArgs
   tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
 }
 
+// The FP16 staggered direction on half2 words: o = U chi (UDAG: U^+ chi) with
+// the link's third row rebuilt on half2 words and 2 HFMA2 per complex
+// multiply-add (as wilson_hop_dir16), then acc += s o in packed FP32 (s = eta
+// x boundary sign x the neighbour's site norm; the mat-vec is linear, so the
+// norm is applied once to its result).
+template <bool UDAG>
+__device__ __forceinline__ void staggered_dir16(float2 acc[3], const uint32_t (&v)[3], const PackedLink16& l, float s) {
+  uint32_t u[9] = {l.a.x, l.a.y, l.a.z, l.a.w, l.b.x, l.b.y, 0u, 0u, 0u};
+  link16_third_row(u);
+  const __half2 zero = __float2half2_rn(0.f);
+  __half2 g[3] = {zero, zero, zero};
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t e = UDAG ? u[3 * k + r] : u[3 * r + k];
+      g[r] = h2_cmac<UDAG>(__low2half2(as_h2(e)), __high2half2(as_h2(e)), v[k], g[r]);
+    }
+  const float2 ss = make_float2(s, s);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) acc[c] = __ffma2_rn(ss, __half22float2(g[c]), acc[c]);
+}
+__device__ __forceinline__ float load_color16(const void* __restrict__ base, const float* __restrict__ nrm, int64_t Vh,
+                                              int64_t h, uint32_t (&v)[3]) {
+  const uint32_t* b = reinterpret_cast<const uint32_t*>(base);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = __ldg(b + k * Vh + h);
+  return __ldg(nrm + h);
+}
+
 template <int P, int RECON>
 __device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
   using AT = typename AccT<P>::T;
@@ -1528,6 +1558,27 @@ __device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
   cpx<AT> acc[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) acc[k] = mk<AT>(0, 0);
+  if constexpr (P == P16) {
+    float2 a16[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+      int es = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k < mu) es += c[k];
+      const float eta = (es & 1) ? -1.f : 1.f;
+      uint32_t vf[3], vb[3];
+      PackedLink16 lf, lb;
+      const float nf = load_color16(in, in_norm, Vh, nb.hf[mu], vf);
+      load_packed_link16(a.U_here, mu, Vh, h, lf);
+      const float nbn = load_color16(in, in_norm, Vh, nb.hb[mu], vb);
+      load_packed_link16(a.U_there, mu, Vh, nb.hb[mu], lb);
+      staggered_dir16<false>(a16, vf, lf, eta * nb.sf[mu] * nf);
+      staggered_dir16<true>(a16, vb, lb, -eta * nb.sb[mu] * nbn);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = mk<AT>(a16[k].x, a16[k].y);
+  } else {
 #pragma unroll
   for (int mu = 0; mu < 4; ++mu) {
     int es = 0;
@@ -1548,6 +1599,7 @@ __device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
     const AT sb = -eta * (AT)nb.sb[mu];
 #pragma unroll
     for (int k = 0; k < 3; ++k) acc[k] = acc[k] + sb * o[k];
+  }
   }
   const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
 #pragma unroll

@@ -160,6 +160,33 @@ def test_staggered_fp64(ctx, clg, oracle, lat8, dagger):
     assert rel(f32.to_numpy(), oracle.ks_D(L, Uh, chi, m, dagger=dagger)) < 2e-6
 
 
+@pytest.mark.parametrize("dagger", [False, True])
+def test_staggered_fp16(ctx, clg, oracle, lat8, dagger):
+    """The FP16 staggered hop (half2 link products, FP32 accumulation) against
+    the FP64 oracle's D, D^+ and (D D^+)_ee, two right-hand sides."""
+    L = lat8.dims
+    m = 0.02
+    U = make_gauge(clg, lat8, "expH", 0xC1A60004)
+    Uh = U.CopyDataOut()
+    f64 = clg.CFieldFermionKSSU3(lat8, m)
+    chis = []
+    f = clg.CFieldFermionKSSU3(lat8, m, precision=2, nrhs=2)
+    for r in range(2):
+        f64.InitialField(clg.SOURCE_GAUSS, 19 + r, 2)
+        chis.append(f64.to_numpy())
+        f.from_numpy(chis[-1], r)
+    (f.Ddagger if dagger else f.D)(U)
+    for r in range(2):
+        assert rel(f.to_numpy(r), oracle.ks_D(L, Uh, chis[r], m, dagger=dagger)) < 5e-3
+    e = clg.CFieldFermionKSSU3(lat8, m, subset=clg.EVEN, precision=2)
+    pm = clg.eo_parity(L)
+    ce = chis[0].copy()
+    ce[pm == 1] = 0
+    e.from_numpy(ce)
+    e.ApplyOperator(clg.OP_DDDAG_EE, U)
+    assert rel(e.to_numpy()[pm == 0], oracle.ks_dddag_ee(L, Uh, ce, m)[pm == 0]) < 5e-3
+
+
 def test_multi_rhs_matches_single(ctx, clg, lat8):
     U = make_gauge(clg, lat8)
     n = 3
