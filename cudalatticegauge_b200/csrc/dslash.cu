@@ -226,7 +226,20 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
     // one-rhs kernel, and nothing is cached
     if (!ctx->tuning_enabled || !idempotent(a) || stream_capturing(ctx->stream))
       return launch_wilson<P16, 12>(ctx, a, dagger, nrhs, key);
-    cfg = tune_block(ctx, key + "_auto", true, go, cand);
+    std::map<int, float> times;
+    cfg = tune_block(ctx, key + "_auto", true, go, cand, 128, &times);
+    // a tile form in site order that the blocked order matches within 3 %:
+    // take the blocked one, whose fewer DRAM bytes help the fused epilogue
+    // hops (more memory traffic than the plain hop timed here) that follow
+    // this choice
+    if ((cfg >> 16) == 16 || (cfg >> 16) == 17) {
+      const int blocked = cfg + (2 << 16);
+      auto a = times.find(cfg), b = times.find(blocked);
+      if (a != times.end() && b != times.end() && b->second <= 1.03f * a->second) {
+        cfg = blocked;
+        ctx->tuned[key + "_auto"] = cfg;
+      }
+    }
     ctx->tuned.erase(key);
     ctx->tuned.erase(key + "_pair");
     ctx->tuned.erase(key + "_tile");

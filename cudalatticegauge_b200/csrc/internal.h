@@ -288,7 +288,8 @@ inline cudaError_t opt_in_smem(const void* fn, size_t bytes) {
 // timed with CUDA events on the context stream and the fastest is cached.
 template <class Go>
 int tune_block(clg_context_s* ctx, const std::string& key, bool can_repeat, Go&& go,
-               const std::vector<int>& cand = {64, 128, 256, 512}, int fallback = 128) {
+               const std::vector<int>& cand = {64, 128, 256, 512}, int fallback = 128,
+               std::map<int, float>* times = nullptr) {
   auto it = ctx->tuned.find(key);
   if (it != ctx->tuned.end()) return it->second;
   if (!ctx->tuning_enabled || !can_repeat || stream_capturing(ctx->stream)) return fallback;
@@ -305,6 +306,7 @@ int tune_block(clg_context_s* ctx, const std::string& key, bool can_repeat, Go&&
     if (cudaEventSynchronize(e1) != cudaSuccess) break;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
+    if (times) (*times)[bs] = ms;
     if (ms < best_ms) { best_ms = ms; best = bs; }
   }
   cudaEventDestroy(e0);
