@@ -348,6 +348,7 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   // CLG_AUTOTUNE=0 keeps the default block size (reproducible profiling runs)
   if (const char* t = std::getenv("CLG_AUTOTUNE")) ctx->tuning_enabled = t[0] != '0';
   if (const char* t = std::getenv("CLG_FUSED_CG")) ctx->fused_cg = t[0] != '0';
+  if (const char* t = std::getenv("CLG_FUSED_RESID")) ctx->fused_resid = t[0] != '0';
   if (const char* t = std::getenv("CLG_HOP_PAIR")) {
     int variant = -1, bs = 0;
     if (std::sscanf(t, "%d:%d", &variant, &bs) == 2 && (variant == 0 || variant == 1) &&

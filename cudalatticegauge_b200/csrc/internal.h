@@ -96,6 +96,9 @@ struct clg_context_s {
   // CG on the Wilson normal equations fuses its vector work into the Schur
   // hops; CLG_FUSED_CG=0 runs the separate kernels instead
   bool fused_cg = true;
+  // the outer residual r = b - D x of Wilson solves fused into the FP64 hop
+  // (with |r|^2 and the inner-precision copy); CLG_FUSED_RESID=0: separate passes
+  bool fused_resid = true;
   // FP16 Wilson hops over two or more right-hand sides: one right-hand side
   // per thread (the right-hand sides interleaved over the blocks, links shared
   // through L2), two per thread (wilson_hop_pair_kernel: one link load and

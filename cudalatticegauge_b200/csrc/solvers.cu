@@ -758,6 +758,84 @@ clg_status schur_hop_epi(Work& w, bool dag, const FieldRef& t_odd, const FieldRe
 }
 
 // t_o = H_oe^(dag) in_e
+}  // namespace (a kernel's template argument must not have internal linkage)
+
+// The outer residual of a Wilson D / D^+ solve fused into the FP64 hop that
+// computes D x on parity par: r = b - D x is stored in FP64 and in the inner
+// precision PI (the next inner solve's right-hand side), and |r|^2 goes to
+// out[rhs] (the first parity sets it, the second adds), so neither the
+// separate residual pass nor the copy to the inner precision reads r again.
+template <int PI>
+struct ResidHop {
+  static constexpr int NRED = 1;
+  static constexpr bool STORE = false;
+  DField b, r, rp;
+  int par;
+  bool first;
+  double* out;
+  template <typename AT>
+  __device__ void site(int rhs, int64_t h, const cpx<AT> dx[12], double* red) const {
+    cpx<double> v[12];
+    ldv<P64, 12, double>(b, rhs, par, h, v);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) v[k] = mk<double>(v[k].x - (double)dx[k].x, v[k].y - (double)dx[k].y);
+    stv<P64, 12, double>(r, rhs, par, h, v);
+    using AI = typename AccT<PI>::T;
+    cpx<AI> vi[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) vi[k] = mk<AI>((AI)v[k].x, (AI)v[k].y);
+    stv<PI, 12, AI>(rp, rhs, par, h, vi);
+    red[0] += site_norm2<12, double>(v);
+  }
+  __device__ void finalize(int rhs, const double* s) const { out[rhs] = first ? s[0] : out[rhs] + s[0]; }
+};
+
+namespace {
+
+template <int PI>
+clg_status fused_residual_t(Work& w, bool dag, const FieldRef& b, const FieldRef& x, const FieldRef& r,
+                            const FieldRef& rp, double* out) {
+  clg_context_s* ctx = w.ctx;
+  for (int par = 0; par < 2; ++par) {
+    HopSpec s{};
+    s.kind = CLG_FERMION_WILSON;
+    s.prec = CLG_PREC_DOUBLE;
+    s.dagger = dag;
+    s.out_parity = par;
+    s.in = x;
+    s.out = r;  // not written by the hop (ResidHop::STORE is false): the epilogue stores r
+    s.x = &x;
+    s.a = make_double2(-w.param, 0.0);
+    s.xa = make_double2(1.0, 0.0);
+    s.nrhs = w.nrhs;
+    HopArgs a;
+    if (clg_status st = make_hop_args(ctx, w.U, s, a)) return st;
+    const ResidHop<PI> e{dfield(b), dfield(r), dfield(rp), par, par == 0, out};
+    HopSpec plain = s;
+    plain.x = nullptr;
+    const int pc = tuned_hop_config(ctx, w.U, plain, -1);
+    cudaError_t err;
+    if (w.nrhs >= 2 && pc >= 0 && (pc >> 16) >= 16) {
+      const int64_t nslots = (w.Vh + TILE16 - 1) / TILE16;
+      if (clg_status st = ensure_reduction(ctx, red2_doubles(nslots, w.nrhs, 1, 1))) return st;
+      err = dag ? launch_hop_tileN_epi<P64, 18, true>(ctx, a, e, pc) : launch_hop_tileN_epi<P64, 18, false>(ctx, a, e, pc);
+    } else {
+      const int bs = tuned_hop_block(ctx, w.U, plain, 64);
+      if (clg_status st = ensure_reduction(ctx, red2_doubles((w.Vh + bs - 1) / bs, w.nrhs, w.nrhs, 1))) return st;
+      err = dag ? launch_hop_epi<P64, 18, true>(ctx, a, e, bs) : launch_hop_epi<P64, 18, false>(ctx, a, e, bs);
+    }
+    if (err != cudaSuccess) return ctx->fail(cuda_status(err), std::string("residual hop: ") + cudaGetErrorString(err));
+  }
+  return CLG_SUCCESS;
+}
+
+clg_status fused_residual(Work& w, bool dag, const FieldRef& b, const FieldRef& x, const FieldRef& r,
+                          const FieldRef& rp, double* out) {
+  return w.P == CLG_PREC_HALF     ? fused_residual_t<P16>(w, dag, b, x, r, rp, out)
+         : w.P == CLG_PREC_SINGLE ? fused_residual_t<P32>(w, dag, b, x, r, rp, out)
+                                  : fused_residual_t<P64>(w, dag, b, x, r, rp, out);
+}
+
 clg_status schur_hop_odd(Work& w, bool dag, const FieldRef& in_even, const FieldRef& t_odd, const int* skip, int ks) {
   HopSpec s;
   s.kind = CLG_FERMION_WILSON;
@@ -1168,8 +1246,21 @@ clg_status clg::solve_core(const SolveReq& q) {
   const char* venv = std::getenv("CLG_VERBOSE");
   const bool verbose = venv && venv[0] == '1';
   int outer = 0;
+  // the residual fused into the FP64 hop (Wilson D / D^+ on full fields, no
+  // shift, one lattice) from the second cycle on: the first cycle runs the
+  // plain hops, which also time their launch configuration
+  const bool fuse_resid = ctx->fused_resid && wilson && full && nc == 12 && !w.shift_dev && !U->seg &&
+                          (op == CLG_OP_D || op == CLG_OP_DDAG);
+  bool rp_ready = false;
   for (;; ++outer) {
     // r = b - A x  (FP64, true residual)
+    rp_ready = false;
+    if (fuse_resid && outer > 0) {
+      if ((s = fused_residual(w, op == CLG_OP_DDAG, b64.ref, x64.ref, r64.ref, rP.ref, w.red_d))) return s;
+      rp_ready = true;
+      goto residual_done;
+    }
+    {
     const FieldRef* tmp = (op == CLG_OP_DDDAG) ? nullptr : &t64.ref;
     Owned& tf = w.tf;
     if (op == CLG_OP_DDDAG) {
@@ -1196,6 +1287,8 @@ clg_status clg::solve_core(const SolveReq& q) {
       return launch_sites<1>(ctx, Resid<NN.value>{dfield(b64.ref), dfield(r64.ref), w.red_d}, 0, npar, Vh, nrhs);
     });
     if (s) return s;
+    }
+  residual_done:
     if (to_host(w, w.red_d, sizeof(double) * nrhs) != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
       return ctx->fail(CLG_ERR_CUDA, "solve: reading |r|");
     bool all = true;
@@ -1235,7 +1328,7 @@ clg_status clg::solve_core(const SolveReq& q) {
       cudaMemcpyAsync(w.outer_done_d, w.host_buf + nrhs, sizeof(int) * nrhs, cudaMemcpyHostToDevice, ctx->stream);
     }
     // e ~= A^{-1} r in the inner precision
-    if ((s = blas_copy(ctx, rP.ref, r64.ref))) return s;
+    if (!rp_ready && (s = blas_copy(ctx, rP.ref, r64.ref))) return s;
     auto schur_solve = [&](bool dag, const FieldRef& rhs, const FieldRef& sol) -> clg_status {
       clg_status q;
       FieldRef rhs_e = rhs.parity_view(0), rhs_o = rhs.parity_view(1);
