@@ -406,7 +406,9 @@ __device__ __forceinline__ void wilson_hop_finish(const HopArgs& a, int rhs, int
   const int64_t Vh = a.g.Vh;
   // the coefficients of the operators are real (-kappa, -kappa^2, 1): a real
   // fast path (uniform branch) takes half the multiplies, packed f32x2 in FP32
-  if (a.a.y == 0.0) {
+  if (a.a.y == 0.0 && a.a.x == 1.0) {
+    // the plain hop (a = 1): nothing to scale (x * 1 is exact, so skipping it changes no bit)
+  } else if (a.a.y == 0.0) {
     const AT ar = (AT)a.a.x;
     if constexpr (sizeof(AT) == 4) {
       float2* av = reinterpret_cast<float2*>(acc);
