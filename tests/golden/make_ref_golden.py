@@ -177,7 +177,7 @@ def residual(case, L, U, b, x, base, shift=0j):
 
 
 CASES = [
-    # 8^4 Haar links, one Gaussian source; D, D^+, products,
+    # the small 8^4 workload: Haar links, one Gaussian source; D, D^+, products,
     # GMRES(12), BiCGStab and the multi-shift FOM on the reference test's shifts
     {"name": "wilson_haar_8x8x8x8", "L": (8, 8, 8, 8), "links": "haar", "seed": 0xC1A60000,
      "fermion": "wilson",
@@ -196,7 +196,7 @@ CASES = [
          # restarted GMRES(12) stagnates on this field: a budget of 100 cycles
          {"ops": ["D", "Ddagger", "InverseD"], "solver": "gmres", "restart": 100},
      ]},
-    # staggered (config 5's operator) on 8^3x16, 2am = 0.02
+    # staggered (DD^+)_ee, the multi-shift workload's operator, on 8^3x16, 2am = 0.02
     {"name": "ks_expH_8x8x8x16", "L": (8, 8, 8, 16), "links": "expH", "seed": 0xC1A60005,
      "fermion": "ks",
      "jobs": [

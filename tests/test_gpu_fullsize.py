@@ -33,7 +33,7 @@ def expH(clg, lat, seed):
 
 @pytest.fixture(scope="module")
 def c2(ctx, clg, oracle):
-    """32^3x16, exp(i 0.25 H) links (seed 0xC1A60001), one Gaussian source."""
+    """The single-source 32^3x16 workload: exp(i 0.25 H) links (seed 0xC1A60001), one Gaussian source."""
     lat = clg.Lattice(ctx, (32, 32, 32, 16))
     U = expH(clg, lat, 0xC1A60001)
     Uh = U.CopyDataOut()
@@ -69,7 +69,7 @@ def test_config2_mee_all_precisions(ctx, clg, oracle, c2):
         errs[prec] = rel(e.to_numpy()[pm == 0], want)
         e.close()
         assert errs[prec] < tol, (prec, errs[prec])
-    print("config 2 M_ee error vs FP64 oracle: FP64 %.2e, FP32 %.2e, FP16 %.2e" % (errs[0], errs[1], errs[2]))
+    print("32^3x16 M_ee error vs FP64 oracle: FP64 %.2e, FP32 %.2e, FP16 %.2e" % (errs[0], errs[1], errs[2]))
     f.close()
 
 
@@ -85,7 +85,7 @@ def test_config2_headline_solve(ctx, clg, oracle, c2, inner):
     assert info["status"] == 0
     op = oracle.Operator("WILSON_D", lat.dims, Uh, KAPPA)
     r = op.true_residual(b.to_numpy(), x.to_numpy())
-    print("config 2 %s-inner CGNE: %d applications, oracle true residual %.3e" % (inner, info["iterations"], r))
+    print("32^3x16 %s-inner CGNE: %d applications, oracle true residual %.3e" % (inner, info["iterations"], r))
     assert r <= TOL
     S.close()
     x.close()
@@ -93,7 +93,7 @@ def test_config2_headline_solve(ctx, clg, oracle, c2, inner):
 
 
 def test_config5_staggered_12_shifts(ctx, clg, oracle):
-    """staggered (DD^+)_ee + sigma_k on 32^3x16, 2am = 0.02, FP32 CG-M + FP64 refinement."""
+    """The staggered multi-shift workload: staggered (DD^+)_ee + sigma_k on 32^3x16, 2am = 0.02, FP32 CG-M + FP64 refinement."""
     lat = clg.Lattice(ctx, (32, 32, 32, 16))
     m = 0.02
     U = expH(clg, lat, 0xC1A60004)
@@ -111,11 +111,11 @@ def test_config5_staggered_12_shifts(ctx, clg, oracle):
         r = op.true_residual(bh, xs[k].to_numpy(), complex(s))
         worst = max(worst, r)
         assert r <= TOL, (k, s, r)
-    print("config 5 CG-M: worst oracle true residual over 12 shifts %.3e" % worst)
+    print("staggered 32^3x16 CG-M: worst oracle true residual over 12 shifts %.3e" % worst)
 
 
 def test_config3_operator_and_solve(ctx, clg, oracle):
-    """48^3x24 (V = 2,654,208), FP64 M_ee to 1e-12, FP32 / FP16
+    """The large 48^3x24 lattice (V = 2,654,208), FP64 M_ee to 1e-12, FP32 / FP16
     errors stated, and an FP16-inner solve to the oracle's true residual 1e-10."""
     lat = clg.Lattice(ctx, (48, 48, 48, 24))
     L = lat.dims
@@ -134,7 +134,7 @@ def test_config3_operator_and_solve(ctx, clg, oracle):
         errs.append(rel(e.to_numpy()[pm == 0], want))
         e.close()
         assert errs[-1] < tol, (prec, errs[-1])
-    print("config 3 M_ee error vs FP64 oracle: FP64 %.2e, FP32 %.2e, FP16 %.2e" % tuple(errs))
+    print("48^3x24 M_ee error vs FP64 oracle: FP64 %.2e, FP32 %.2e, FP16 %.2e" % tuple(errs))
     del want
     b = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA)
     b.InitialField(clg.SOURCE_GAUSS, 0xC1A60002, 3)
@@ -144,12 +144,12 @@ def test_config3_operator_and_solve(ctx, clg, oracle):
     assert info["status"] == 0
     op = oracle.Operator("WILSON_D", L, Uh, KAPPA)
     r = op.true_residual(b.to_numpy(), x.to_numpy())
-    print("config 3 FP16-inner CGNE: %d applications, oracle true residual %.3e" % (info["iterations"], r))
+    print("48^3x24 FP16-inner CGNE: %d applications, oracle true residual %.3e" % (info["iterations"], r))
     assert r <= TOL
 
 
 def test_config4_batched_point_and_z2(ctx, clg, oracle):
-    """BASELINE config 4 shape: 32^3x32, point sources and Z2 noise in one batched
+    """The batched workload's shape: 32^3x32, point sources and Z2 noise in one batched
     FP16-inner solve (a subset of the 28 sources, to keep the oracle's checks short)."""
     lat = clg.Lattice(ctx, (32, 32, 32, 32))
     U = expH(clg, lat, 0xC1A60003)

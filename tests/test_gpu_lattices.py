@@ -56,7 +56,7 @@ def test_lattices_match_single_solves(ctx, clg, oracle, solver, inner, opname):
 
 
 def test_uneven_set_of_config4(ctx, clg, oracle):
-    """The five lattices of BASELINE config 4 (8^4, 12^4, 16^4, 16^3x32, 24^3x16),
+    """The uneven five-lattice set (8^4, 12^4, 16^4, 16^3x32, 24^3x16),
     4 Gaussian sources each, FP16-inner CGNE, in one solve."""
     dims_list = [(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (16, 16, 16, 32), (24, 24, 24, 16)]
     lats, Us, bs, xs = build(clg, ctx, dims_list, [4] * 5)
