@@ -407,7 +407,7 @@ def ours(args, world, rank, local):
     extra = {}
     if rank == 0 and not args.quick and nrhs > 1:
         extra["denominators_32x32x32x32"] = denominators(clg, ctx, stream, lat, U, kappa, W, value)
-        extra["config2_32x32x32x16"] = config2_side(clg, ctx, stream, args)
+        extra["single_source_32x32x32x16"] = single_source_side(clg, ctx, stream, args)
         if not args.no_batched:
             extra["batched_uneven_lattices"] = uneven_lattices(clg, ctx, stream, args)
         if not args.no_side:
@@ -561,7 +561,7 @@ def denominators(clg, ctx, stream, lat, U, kappa, W, batched_value):
     return out
 
 
-def config2_side(clg, ctx, stream, args, steps=5):
+def single_source_side(clg, ctx, stream, args, steps=5):
     """32^3x16 (exp(i 0.25 H) links, one complex Gaussian source): the
     single-source solve of the metric's FP16-inner CGNE, the other solvers and
     precisions, and the hop in each precision; every solution checked by the
