@@ -22,7 +22,7 @@ cudaError_t launch_wilson_tileN(clg_context_s* ctx, const HopArgs& a0, bool dagg
   constexpr int CAP = P == P64 ? 2 : 3;
   const int bs = cfg & 0xffff;
   HopArgs a = a0;
-  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
+  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs, TILE16, spinor_bytes<P>()) : 0;
   dim3 grid((unsigned)((a.g.Vh + TILE16 - 1) / TILE16));
   if ((cfg >> 16) & 1)
     return dagger ? launch_pdl(ctx, wilson_hop_tileN_kernel<P, RECON, true, CAP>, grid, dim3(bs), 0, a)
@@ -75,7 +75,8 @@ cudaError_t launch_wilson(clg_context_s* ctx, const HopArgs& a, bool dagger, int
   // several right-hand sides: the tile form (links staged once per tile)
   if (P != P16 && nrhs >= 2)
     for (int w : tile_warps(nrhs))
-      for (int v = 0; v < (tile_rows(a.g, nrhs) ? 4 : 2); ++v) cand.push_back((32 * w) | ((16 + v) << 16));
+      for (int v = 0; v < (tile_rows(a.g, nrhs, TILE16, spinor_bytes<P>()) ? 4 : 2); ++v)
+        cand.push_back((32 * w) | ((16 + v) << 16));
   return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 
@@ -129,13 +130,14 @@ cudaError_t launch_wilson_batch(clg_context_s* ctx, const HopArgs& a, bool dagge
 }  // namespace
 
 // The y-rows per chunk of the tile hops' blocked order (0: site order): the
-// largest divisor of L_y whose three x-slabs of input spinors, over all
+// largest divisor of L_y whose three x-slabs of input spinors (sbytes per
+// site and rhs: 52 FP16 with its norm, 96 FP32, 192 FP64), over all
 // right-hand sides, take at most 24 MB of L2; 0 when the z-t planes are not a
 // whole number of tiles or no chunk smaller than L_y qualifies.
-int tile_rows(const Geom& g, int nrhs, int ts) {
+int tile_rows(const Geom& g, int nrhs, int ts, int sbytes) {
   const int64_t plane = (int64_t)g.L[2] * g.L[3];
   if (plane % (2 * ts)) return 0;
-  const int64_t slab_row = plane / 2 * nrhs * 52;  // FP16 spinor + norm bytes of one y-row, all rhs
+  const int64_t slab_row = plane / 2 * nrhs * sbytes;  // spinor bytes of one y-row, all rhs
   int best = 0;
   for (int by = 1; by < g.L[1]; ++by)
     if (g.L[1] % by == 0 && 3 * by * slab_row <= (int64_t)24 << 20) best = by;

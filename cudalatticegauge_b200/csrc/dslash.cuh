@@ -881,7 +881,9 @@ __global__ void __launch_bounds__(MAXT, MINB) wilson_hop_pair_epi_kernel(HopArgs
 constexpr int TILE16 = 32;
 // the y-rows per chunk of the blocked tile order for this lattice, rhs count
 // and tile size (dslash.cu)
-int tile_rows(const Geom& g, int nrhs, int ts = TILE16);
+int tile_rows(const Geom& g, int nrhs, int ts = TILE16, int sbytes = 52);
+// bytes of one Wilson spinor per site and rhs (FP16: with its norm)
+template <int P> constexpr int spinor_bytes() { return P == P64 ? 192 : (P == P32 ? 96 : 52); }
 struct Tile16 {
   uint4 la[8][TILE16];     // link words 0-3; direction d < 4: U_d(x), d >= 4: U_(d-4)(x - mu)
   uint4 lb[8][TILE16];     // words 4-7

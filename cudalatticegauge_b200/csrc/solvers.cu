@@ -622,7 +622,7 @@ cudaError_t launch_hop_tileN_epi(clg_context_s* ctx, const HopArgs& a0, const E&
   constexpr int CAP = P == P64 ? 2 : 3;
   const int bs = cfg & 0xffff;
   HopArgs a = a0;
-  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
+  a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs, TILE16, spinor_bytes<P>()) : 0;
   const int64_t nslots = (a.g.Vh + TILE16 - 1) / TILE16;
   const unsigned group = red_group(nslots, 1);
   double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
