@@ -350,3 +350,38 @@ def test_tileN_cg_fp64(clg, oracle, pinned, cfg):
     for r in range(4):
         assert infos[r]["status"] == 0
         assert op.true_residual(b.to_numpy(r), x.to_numpy(r)) <= 1e-10
+
+
+def test_tune_file_round_trip(clg, tmp_path):
+    """CLG_TUNE_FILE: a context writes the autotuner's choices when it is
+    destroyed and the next context reads them back (clg_context_tuned shows
+    the same forms), so a later run launches the kernels an earlier run chose."""
+    import os
+
+    path = str(tmp_path / "tune.txt")
+    old = os.environ.get("CLG_TUNE_FILE")
+    os.environ["CLG_TUNE_FILE"] = path
+    try:
+        c = clg.Context(0)
+        lat = clg.Lattice(c, (8, 8, 8, 16))
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60001, 1, 0.25)
+        f = clg.CFieldFermionWilsonSquareSU3(lat, KAPPA, subset=clg.EVEN, precision=clg.HALF, nrhs=4)
+        for r in range(4):
+            f.InitialField(clg.SOURCE_GAUSS, 990 + r, 2, rhs=r)
+        f.ApplyOperator(clg.OP_MEE, U)
+        first = c.tuned()
+        assert any(k.startswith("wilson_p2_") and k.endswith("_auto") for k in first)
+        for o in (f, U, lat):
+            o.close()
+        c.close()
+        text = open(path).read()
+        assert all(f"{k}=" in text for k in first)
+        c2 = clg.Context(0)
+        assert c2.tuned() == first
+        c2.close()
+    finally:
+        if old is None:
+            del os.environ["CLG_TUNE_FILE"]
+        else:
+            os.environ["CLG_TUNE_FILE"] = old
