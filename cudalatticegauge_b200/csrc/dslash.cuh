@@ -238,14 +238,21 @@ __device__ __forceinline__ void wilson_hop_dir16_u(Acc16& A, const Packed16& p, 
     w[4 * k + 2] = p.c[k].z;
     w[4 * k + 3] = p.c[k].w;
   }
-  // projected rows j = 0, 1:  h_j[c] = psi_j[c] + i^z_j psi_perm(j)[c]
+  // projected rows j = 0, 1:  h_j[c] = psi_j[c] + i^z_j psi_perm(j)[c].  The
+  // spin-planar storage (spinor_word) holds spins (0, 1) and (2, 3) as planes:
+  // rows (0, 1) are the q = 0 words, rows perm = (2, 3) the q = 1 words and
+  // perm = (3, 2) the same with their halves swapped.
+  static_assert(gperm(MU, 0) + gperm(MU, 1) == 5 && gperm(MU, 0) >= 2, "perm pairs spins 2 and 3");
   __half2 hR[3], hI[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const uint32_t a0 = w[c], a1 = w[3 + c];
-    const uint32_t b0 = w[3 * gperm(MU, 0) + c], b1 = w[3 * gperm(MU, 1) + c];
-    const __half2 Ar = as_h2(__byte_perm(a0, a1, 0x5410)), Ai = as_h2(__byte_perm(a0, a1, 0x7632));
-    const __half2 Br = as_h2(__byte_perm(b0, b1, 0x5410)), Bi = as_h2(__byte_perm(b0, b1, 0x7632));
+    const __half2 Ar = as_h2(w[spinor_word(0, c, 0)]), Ai = as_h2(w[spinor_word(0, c, 1)]);
+    uint32_t br = w[spinor_word(1, c, 0)], bi = w[spinor_word(1, c, 1)];
+    if constexpr (gperm(MU, 0) == 3) {
+      br = h2_swap(br);
+      bi = h2_swap(bi);
+    }
+    const __half2 Br = as_h2(br), Bi = as_h2(bi);
     if constexpr ((z0 & 1) == 0) {  // i^z = +-1
       hR[c] = h2_add_signed<z0 == 0, z1 == 0>(Ar, Br);
       hI[c] = h2_add_signed<z0 == 0, z1 == 0>(Ai, Bi);
@@ -295,75 +302,6 @@ __device__ __forceinline__ void wilson_hop_dir16_u(Acc16& A, const Packed16& p, 
       A.i[3 + c] = f2_fma_signed<z2 == 1, z3 == 1>(s, gr, A.i[3 + c]);
     }
   }
-}
-
-// The interleaved form of wilson_hop_dir16_u (one half2 word per complex
-// number, the accumulators as acc[12]): the same operations in the same order,
-// bit-identical; the one-rhs kernel measured faster with it (16.3 against
-// 17.8-18.1 us on 32^3x16: fewer live registers under its 72-80 register caps),
-// the tile kernel with the planar form.
-template <int MU, int SGN, bool UDAG>
-__device__ __forceinline__ void wilson_hop_dir16_i(cpx<float> acc[12], const Packed16& p, const uint32_t (&u)[9],
-                                                   float s) {
-  constexpr int add = SGN < 0 ? 2 : 0;
-  uint32_t w[12];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    w[4 * k + 0] = p.c[k].x;
-    w[4 * k + 1] = p.c[k].y;
-    w[4 * k + 2] = p.c[k].z;
-    w[4 * k + 3] = p.c[k].w;
-  }
-  uint32_t h0[3], h1[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    h0[c] = as_u32(__hadd2(as_h2(w[c]), as_h2(h2_mul_i<gz4(MU, 0) + add>(w[3 * gperm(MU, 0) + c]))));
-    h1[c] = as_u32(__hadd2(as_h2(w[3 + c]), as_h2(h2_mul_i<gz4(MU, 1) + add>(w[3 * gperm(MU, 1) + c]))));
-  }
-  const __half2 zero = __float2half2_rn(0.f);
-  __half2 g0[3] = {zero, zero, zero}, g1[3] = {zero, zero, zero};
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      // U: row r, column k;  U^+: conj of row k, column r
-      const uint32_t e = UDAG ? u[3 * k + r] : u[3 * r + k];
-      const __half2 er = __low2half2(as_h2(e)), ei = __high2half2(as_h2(e));
-      g0[r] = h2_cmac<UDAG>(er, ei, h0[k], g0[r]);
-      g1[r] = h2_cmac<UDAG>(er, ei, h1[k], g1[r]);
-    }
-  // accumulation in FP32: rows whose phase is real (+-1) take one packed
-  // f32x2 FMA per complex number (sm_100 FFMA2); rows with an imaginary phase
-  // need the swapped pair and stay on two scalar FMAs
-  const float2 ss = make_float2(s, s), sn = make_float2(-s, -s);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const float2 f0 = __half22float2(g0[c]), f1 = __half22float2(g1[c]);
-    float2* av = reinterpret_cast<float2*>(acc);
-    av[c] = __ffma2_rn(ss, f0, av[c]);
-    av[3 + c] = __ffma2_rn(ss, f1, av[3 + c]);
-#pragma unroll
-    for (int row = 2; row < 4; ++row) {
-      const int z = (gz4(MU, row) + add) & 3;
-      const float2 f = gperm(MU, row) == 0 ? f0 : f1;
-      if (z == 0) {
-        av[3 * row + c] = __ffma2_rn(ss, f, av[3 * row + c]);
-      } else if (z == 2) {
-        av[3 * row + c] = __ffma2_rn(sn, f, av[3 * row + c]);
-      } else {
-        acc[3 * row + c] = cfma(s, mul_i(mk<float>(f.x, f.y), z), acc[3 * row + c]);
-      }
-    }
-  }
-}
-
-// The interleaved direction with the link as stored (12-real)
-template <int MU, int SGN, bool UDAG>
-__device__ __forceinline__ void wilson_hop_dir16_il(cpx<float> acc[12], const Packed16& p, const PackedLink16& l,
-                                                    float s) {
-  uint32_t u[9] = {l.a.x, l.a.y, l.a.z, l.a.w, l.b.x, l.b.y, 0u, 0u, 0u};
-  link16_third_row(u);
-  wilson_hop_dir16_i<MU, SGN, UDAG>(acc, p, u, s);
 }
 
 // The same with the link as stored (12-real): the third row is rebuilt first.
@@ -492,6 +430,8 @@ __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom&
     // (wilson_hop_dir16); the projection and the link product are linear, so
     // the neighbour's site norm is applied with the boundary sign to the 6
     // projected products when they are accumulated in FP32.
+    Acc16 A;
+    acc16_zero(A);
 #define CLG_WILSON_DIR16(MU)                                                            \
   {                                                                                     \
     Packed16 pf, pb;                                                                    \
@@ -500,14 +440,15 @@ __device__ __forceinline__ void wilson_hop_site_on(const HopArgs& a, const Geom&
     load_packed_link16(Uh, MU, lVh, h, lf);                                             \
     load_packed16(in, in_norm, Vh, nb.hb[MU], pb);                                      \
     load_packed_link16(Ut, MU, lVh, nb.hb[MU], lb);                                     \
-    wilson_hop_dir16_il<MU, SF, false>(acc, pf, lf, nb.sf[MU] * pf.n);                  \
-    wilson_hop_dir16_il<MU, SB, true>(acc, pb, lb, nb.sb[MU] * pb.n);                   \
+    wilson_hop_dir16<MU, SF, false>(A, pf, lf, nb.sf[MU] * pf.n);                       \
+    wilson_hop_dir16<MU, SB, true>(A, pb, lb, nb.sb[MU] * pb.n);                        \
   }
     CLG_WILSON_DIR16(0)
     CLG_WILSON_DIR16(1)
     CLG_WILSON_DIR16(2)
     CLG_WILSON_DIR16(3)
 #undef CLG_WILSON_DIR16
+    acc16_out(A, acc);
   } else {
 #define CLG_WILSON_DIR(MU)                                                              \
   {                                                                                     \
@@ -658,9 +599,13 @@ __device__ __forceinline__ void wilson_hop_dir16_pair(float2 accR[12], float2 ac
   for (int j = 0; j < 2; ++j)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int ia = 3 * j + c, ib = 3 * gperm(MU, j) + c;
-      const __half2 aR = as_h2(__byte_perm(w0[ia], w1[ia], 0x5410)), aI = as_h2(__byte_perm(w0[ia], w1[ia], 0x7632));
-      const __half2 bR = as_h2(__byte_perm(w0[ib], w1[ib], 0x5410)), bI = as_h2(__byte_perm(w0[ib], w1[ib], 0x7632));
+      // spin s of colour c: half (s & 1) of the spin-planar words of pair s >> 1
+      const int sa = j, sb = gperm(MU, j);
+      const int ar = spinor_word(sa >> 1, c, 0), ai = spinor_word(sa >> 1, c, 1);
+      const int br = spinor_word(sb >> 1, c, 0), bi = spinor_word(sb >> 1, c, 1);
+      const unsigned sela = (sa & 1) ? 0x7632 : 0x5410, selb = (sb & 1) ? 0x7632 : 0x5410;
+      const __half2 aR = as_h2(__byte_perm(w0[ar], w1[ar], sela)), aI = as_h2(__byte_perm(w0[ai], w1[ai], sela));
+      const __half2 bR = as_h2(__byte_perm(w0[br], w1[br], selb)), bI = as_h2(__byte_perm(w0[bi], w1[bi], selb));
       const int z = (gz4(MU, j) + add) & 3;
       if (z == 0) { hR[j][c] = __hadd2(aR, bR); hI[j][c] = __hadd2(aI, bI); }
       else if (z == 1) { hR[j][c] = __hsub2(aR, bI); hI[j][c] = __hadd2(aI, bR); }
@@ -1370,14 +1315,22 @@ __device__ __forceinline__ void mma16_stage_links(const HopArgs& a, int64_t h0, 
 template <int MU, int SGN>
 __device__ __forceinline__ void mma16_columns(__half* colsite, int rl, int d, const Packed16& p, __half2 r2) {
   constexpr int add = SGN < 0 ? 2 : 0;
-  uint32_t w[12];
+  uint32_t sp[12];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    w[4 * k + 0] = p.c[k].x;
-    w[4 * k + 1] = p.c[k].y;
-    w[4 * k + 2] = p.c[k].z;
-    w[4 * k + 3] = p.c[k].w;
+    sp[4 * k + 0] = p.c[k].x;
+    sp[4 * k + 1] = p.c[k].y;
+    sp[4 * k + 2] = p.c[k].z;
+    sp[4 * k + 3] = p.c[k].w;
   }
+  // w[3 s + c]: spin s, colour c as one (re, im) word, from the spin-planar storage
+  uint32_t w[12];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      w[3 * s + c] = __byte_perm(sp[spinor_word(s >> 1, c, 0)], sp[spinor_word(s >> 1, c, 1)],
+                                 (s & 1) ? 0x7632 : 0x5410);
   uint32_t h[2][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {

@@ -56,7 +56,25 @@ __device__ __forceinline__ void load_site(const void* __restrict__ base, const f
     }
   } else {
     const float n = __ldg(nrm + h);
-    if constexpr (NC % 4 == 0) {
+    if constexpr (NC == 12) {
+      // spin-planar words (spinor_word): word 6q + 2c + ri holds part ri of
+      // colour c of spins 2q (low half) and 2q + 1 (high half)
+      const uint4* b = reinterpret_cast<const uint4*>(base);
+      uint32_t w[12];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const uint4 d = __ldg(b + k * Vh + h);
+        w[4 * k] = d.x; w[4 * k + 1] = d.y; w[4 * k + 2] = d.z; w[4 * k + 3] = d.w;
+      }
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float2 re = h2f(w[6 * q + 2 * c]), im = h2f(w[6 * q + 2 * c + 1]);
+          v[(2 * q) * 3 + c] = mk<AT>(n * re.x, n * im.x);
+          v[(2 * q + 1) * 3 + c] = mk<AT>(n * re.y, n * im.y);
+        }
+    } else if constexpr (NC % 4 == 0) {
       const uint4* b = reinterpret_cast<const uint4*>(base);
 #pragma unroll
       for (int k = 0; k < NC / 4; ++k) {
@@ -106,7 +124,20 @@ __device__ __forceinline__ void store_site(void* __restrict__ base, float* __res
     if (!(m > 1e-30f)) m = 0.f;
     const float inv = m > 0.f ? __frcp_rn(m) : 0.f;  // the correctly rounded 1/m
     nrm[h] = m;
-    if constexpr (NC % 4 == 0) {
+    if constexpr (NC == 12) {
+      uint32_t w[12];
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const cpx<AT> lo = v[(2 * q) * 3 + c], hi = v[(2 * q + 1) * 3 + c];
+          w[6 * q + 2 * c] = f2h((float)lo.x * inv, (float)hi.x * inv);
+          w[6 * q + 2 * c + 1] = f2h((float)lo.y * inv, (float)hi.y * inv);
+        }
+      uint4* b = reinterpret_cast<uint4*>(base);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) b[k * Vh + h] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+    } else if constexpr (NC % 4 == 0) {
       uint4* b = reinterpret_cast<uint4*>(base);
 #pragma unroll
       for (int k = 0; k < NC / 4; ++k) {
@@ -192,6 +223,12 @@ __device__ __forceinline__ void load_link(const void* __restrict__ base, int mu,
 }
 
 // ------------------------------------------------------------------ packed FP16 (load now, unpack later)
+// An FP16 Wilson spinor is 12 half2 words (3 uint4 chunks) in spin-planar
+// order: word 6q + 2c + ri holds part ri (0 real, 1 imaginary) of colour c of
+// spin 2q in its low half and of spin 2q + 1 in its high half.  The hop's spin
+// projection pairs spins (0, 1) with (2, 3) or (3, 2), so it takes its half2
+// planes from these words as they are (at most a swap of halves).
+__host__ __device__ constexpr int spinor_word(int q, int c, int ri) { return 6 * q + 2 * c + ri; }
 struct Packed16 {
   uint4 c[3];
   float n;
