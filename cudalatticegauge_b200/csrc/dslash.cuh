@@ -945,6 +945,16 @@ __device__ __forceinline__ void wilson_hop_site_tile16(const HopArgs& a, const T
   wilson_hop_finish<P16>(a, rhs, h, acc);
 }
 
+// Whether any of the right-hand sides [r0, r1) still needs work (uniform over
+// the block; after the wait on the previous kernel, which may have set skips).
+// A block whose right-hand sides have all finished stages nothing.
+__device__ __forceinline__ bool tile_any_live(const HopArgs& a, int r0, int r1) {
+  if (!a.skip_dev) return r1 > r0;
+  for (int r = r0; r < r1; ++r)
+    if (!a.skip_dev[(int64_t)r * a.skip_stride]) return true;
+  return false;
+}
+
 // The work of one tile block: lattice g (links Uh, Ut), output sites
 // [h0, h0 + 32), right-hand sides [r0, r1).  In a batch of lattices g is one
 // lattice of the batch and a.g.Vh the fields' (padded) chunk stride.
@@ -954,6 +964,7 @@ __device__ __forceinline__ void tile16_body(const HopArgs& a, Tile16& t, const G
   pdl_launch_dependents();
   tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
+  if (!tile_any_live(a, r0, r1)) return;  // no barrier has been passed yet: uniform
   __syncthreads();
   tile16_links(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
@@ -997,13 +1008,14 @@ __device__ __forceinline__ void tile16_epi_body(const HopArgs& a, const E& e, Ti
   pdl_launch_dependents();
   tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
+  const bool any = tile_any_live(a, r0, r1);
   __syncthreads();
-  tile16_links(Uh, Ut, g.Vh, h0, t);
+  if (any) tile16_links(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int64_t h = h0 + lane;
   const unsigned nslots = gridDim.x;
-  for (int rhs = r0 + (threadIdx.x >> 5); rhs < r1; rhs += nw) {
+  for (int rhs = r0 + (threadIdx.x >> 5); any && rhs < r1; rhs += nw) {
     if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
     double red[E::NRED];
 #pragma unroll
@@ -1121,6 +1133,7 @@ __device__ __forceinline__ void tileN_body(const HopArgs& a, TileN<AT>& t, const
   pdl_launch_dependents();
   tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
+  if (!tile_any_live(a, r0, r1)) return;  // no barrier has been passed yet: uniform
   __syncthreads();
   tileN_links<P, RECON>(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
@@ -1157,13 +1170,14 @@ __device__ __forceinline__ void tileN_epi_body(const HopArgs& a, const E& e, Til
   pdl_launch_dependents();
   tile16_neighbours(g, a.out_parity, h0, t);
   pdl_wait();
+  const bool any = tile_any_live(a, r0, r1);
   __syncthreads();
-  tileN_links<P, RECON>(Uh, Ut, g.Vh, h0, t);
+  if (any) tileN_links<P, RECON>(Uh, Ut, g.Vh, h0, t);
   __syncthreads();
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int64_t h = h0 + lane;
   const unsigned nslots = gridDim.x;
-  for (int rhs = r0 + (threadIdx.x >> 5); rhs < r1; rhs += nw) {
+  for (int rhs = r0 + (threadIdx.x >> 5); any && rhs < r1; rhs += nw) {
     if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
     double red[E::NRED];
 #pragma unroll
