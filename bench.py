@@ -253,9 +253,9 @@ def hop_form(ctx, prec, Vh, nrhs):
         if v >= 24:
             return f"wilson_hop_mma16_kernel (tensor-core colour products; variant {v - 24})"
         if v >= 16:
+            cap = {0: "uncapped", 1: "80-register cap", 4: "72-register cap", 5: "64-register cap"}[(v - 16) & 5]
             return (f"wilson_hop_tile16_kernel (32 sites x {nrhs} rhs per block, links staged once in shared memory; "
-                    f"{bs // 32} warps, {'80-register cap' if v & 1 else 'uncapped'}, "
-                    f"{'blocked' if v & 2 else 'site'} tile order)")
+                    f"{bs // 32} warps, {cap}, {'blocked' if v & 2 else 'site'} tile order)")
         if v >= 8:
             return f"wilson_hop_pair_kernel (2 rhs per thread; block {bs}, variant {v - 8})"
         return f"wilson_hop_kernel<P16,12-real> (1 rhs per thread; block {bs}, variant {v})"

@@ -361,7 +361,8 @@ clg_status clg_context_create(int device, void* stream, clg_context* out) {
   }
   if (const char* t = std::getenv("CLG_HOP_TILE")) {
     int warps = 0, variant = -1;
-    if (std::sscanf(t, "%d:%d", &warps, &variant) == 2 && warps >= 1 && warps <= 8 && variant >= 0 && variant <= 3) {
+    if (std::sscanf(t, "%d:%d", &warps, &variant) == 2 && warps >= 1 && warps <= 8 && variant >= 0 &&
+        (variant <= 3 || (variant <= 7 && warps <= 4))) {
       ctx->hop_pair_mode = 3;
       ctx->hop_tile_config = (32 * warps) | ((16 + variant) << 16);
     } else if (std::sscanf(t, "%d:%d", &warps, &variant) == 2 && warps == 8 && variant >= 8 && variant <= 11) {

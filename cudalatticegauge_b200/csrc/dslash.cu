@@ -174,7 +174,16 @@ cudaError_t launch_wilson_tile(clg_context_s* ctx, const HopArgs& a0, bool dagge
   HopArgs a = a0;
   a.tile_rows = ((cfg >> 16) & 2) ? tile_rows(a.g, a.nrhs) : 0;
   dim3 grid((unsigned)((a.g.Vh + TILE16 - 1) / TILE16));
-  if ((cfg >> 16) & 1)
+  const int v = cfg >> 16;
+  if (v >= 20) {  // blocks of at most 128 threads: 72 (v & 1 == 0) or 64 registers
+    if (bs > 128) return cudaErrorInvalidConfiguration;
+    if (v & 1)
+      return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 8, false, 128>, grid, dim3(bs), 0, a)
+                    : launch_pdl(ctx, wilson_hop_tile16_kernel<false, 8, false, 128>, grid, dim3(bs), 0, a);
+    return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 7, false, 128>, grid, dim3(bs), 0, a)
+                  : launch_pdl(ctx, wilson_hop_tile16_kernel<false, 7, false, 128>, grid, dim3(bs), 0, a);
+  }
+  if (v & 1)
     return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 3>, grid, dim3(bs), 0, a)
                   : launch_pdl(ctx, wilson_hop_tile16_kernel<false, 3>, grid, dim3(bs), 0, a);
   return dagger ? launch_pdl(ctx, wilson_hop_tile16_kernel<true, 2>, grid, dim3(bs), 0, a)
@@ -220,8 +229,12 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
       cand.push_back(bs | (9 << 16));
     }
     cand.push_back(64 | (2 << 16));
-    for (int w : tile_warps(nrhs))
-      for (int v = 0; v < (tile_rows(a.g, nrhs) ? 4 : 2); ++v) cand.push_back((32 * w) | ((16 + v) << 16));
+    for (int w : tile_warps(nrhs)) {
+      const int nv = tile_rows(a.g, nrhs) ? 4 : 2;
+      for (int v = 0; v < nv; ++v) cand.push_back((32 * w) | ((16 + v) << 16));
+      if (w <= 4)  // the 72- and 64-register caps (more resident blocks of at most 4 warps)
+        for (int v = 0; v < nv; ++v) cand.push_back((32 * w) | ((20 + v) << 16));
+    }
     if (ctx->hop_mma)
       for (int v = 0; v < (tile_rows(a.g, nrhs, MMA_TS) ? 4 : 2); ++v) cand.push_back(256 | ((24 + v) << 16));
     // untuned (inside a capture, or the output aliases the xpay source): the
@@ -234,7 +247,7 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
     // take the blocked one, whose fewer DRAM bytes help the fused epilogue
     // hops (more memory traffic than the plain hop timed here) that follow
     // this choice
-    if ((cfg >> 16) == 16 || (cfg >> 16) == 17) {
+    if ((cfg >> 16) == 16 || (cfg >> 16) == 17 || (cfg >> 16) == 20 || (cfg >> 16) == 21) {
       const int blocked = cfg + (2 << 16);
       auto a = times.find(cfg), b = times.find(blocked);
       if (a != times.end() && b != times.end() && b->second <= 1.03f * a->second) {

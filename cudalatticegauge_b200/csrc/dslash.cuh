@@ -980,10 +980,11 @@ __device__ __forceinline__ void tile16_body(const HopArgs& a, Tile16& t, const G
 }
 
 // One block per tile of 32 output sites, blockDim = 32 x (warps sharing the
-// right-hand sides); MINB 2 leaves the registers uncapped (128), 3 caps at 80.
+// right-hand sides); MINB 2 leaves the registers uncapped (128), 3 caps at 80;
+// MAXT 128 with MINB 7 caps at 72 (7 blocks of 4 warps per SM).
 // BATCH: a batch of lattices, one block per tile of one lattice (btile).
-template <bool DAGGER, int MINB, bool BATCH = false>
-__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_kernel(HopArgs a) {
+template <bool DAGGER, int MINB, bool BATCH = false, int MAXT = 256>
+__global__ void __launch_bounds__(MAXT, MINB) wilson_hop_tile16_kernel(HopArgs a) {
   __shared__ Tile16 t;
   if constexpr (BATCH) {
     const BatchTile bt = batch_tile(a);
@@ -1045,8 +1046,8 @@ __device__ __forceinline__ void tile16_epi_body(const HopArgs& a, const E& e, Ti
   tile_reduce_finalize<E::NRED>(e, nslots, a.nrhs, group, partials, gpart, counter);
 }
 
-template <bool DAGGER, int MINB, class E, bool BATCH = false>
-__global__ void __launch_bounds__(256, MINB) wilson_hop_tile16_epi_kernel(HopArgs a, E e, double* partials,
+template <bool DAGGER, int MINB, class E, bool BATCH = false, int MAXT = 256>
+__global__ void __launch_bounds__(MAXT, MINB) wilson_hop_tile16_epi_kernel(HopArgs a, E e, double* partials,
                                                                           double* gpart, unsigned* counter,
                                                                           unsigned group) {
   __shared__ Tile16 t;

@@ -111,8 +111,9 @@ struct clg_context_s {
   // 128 registers).  Measured on 32^3x16 / 32^3x32 the two are within a few
   // per cent (13.6 against 13.4 us per rhs at 8 rhs, 27.2 against 27.5 at 28).
   // CLG_HOP_TILE="<warps>:<variant>" forces the tile form (mode 3;
-  // wilson_hop_tile16_kernel; variant bit 0: capped at 80 registers, bit 1:
-  // the blocked tile order);
+  // wilson_hop_tile16_kernel; variants 0-3: bit 0 capped at 80 registers, bit
+  // 1 the blocked tile order; 4-7 (at most 4 warps): capped at 72, bit 0 at
+  // 64 instead, bit 1 the blocked order);
   // the autotuner of mode 2 times it with the other two
   int hop_pair_mode = 2;
   int hop_tile_config = -1;

@@ -609,7 +609,19 @@ cudaError_t launch_hop_tile_epi(clg_context_s* ctx, const HopArgs& a0, const E& 
   const int64_t nslots = (a.g.Vh + TILE16 - 1) / TILE16;
   const unsigned group = red_group(nslots, 1);
   double* gpart = ctx->red_partials + nslots * a.nrhs * E::NRED;
-  if ((cfg >> 16) & 1)
+  int v = cfg >> 16;
+  // an epilogue that loads vectors of its own (the CG update: x, r, p) spills
+  // under the 72- and 64-register caps: it keeps the 80-register form
+  if (v >= 20 && !E::STORE) v = 17 + (v & 2);
+  if (v >= 20) {  // at most 128 threads: 72 or (v odd) 64 registers
+    if (bs > 128) return cudaErrorInvalidConfiguration;
+    if (v & 1)
+      return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 8, E, false, 128>, dim3((unsigned)nslots), dim3(bs),
+                        0, a, e, ctx->red_partials, gpart, ctx->red_counter, group);
+    return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 7, E, false, 128>, dim3((unsigned)nslots), dim3(bs), 0,
+                      a, e, ctx->red_partials, gpart, ctx->red_counter, group);
+  }
+  if (v & 1)
     return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 3, E>, dim3((unsigned)nslots), dim3(bs), 0, a, e,
                       ctx->red_partials, gpart, ctx->red_counter, group);
   return launch_pdl(ctx, wilson_hop_tile16_epi_kernel<DAG, 2, E>, dim3((unsigned)nslots), dim3(bs), 0, a, e,

@@ -185,15 +185,16 @@ def test_fp16_pair_variants_vs_oracle(clg, oracle, cfg):
         c.close()
 
 
-TILE_CONFIGS = ["8:0", "8:1", "4:1", "3:1", "4:3", "7:2"]
+TILE_CONFIGS = ["8:0", "8:1", "4:1", "3:1", "4:3", "7:2", "4:4", "4:7", "2:5"]
 
 
 @pytest.fixture(scope="module")
 def ctx_tiles(clg):
     """Contexts whose FP16 Wilson hops over two or more right-hand sides use
     the tile form (CLG_HOP_TILE="<warps>:<variant>": 32 sites per block, the
-    links staged once in shared memory for all right-hand sides; variant bit
-    0 caps the registers, bit 1 walks the tiles in chunks of y-rows)."""
+    links staged once in shared memory for all right-hand sides; variants 0-3:
+    bit 0 caps the registers at 80, bit 1 walks the tiles in chunks of y-rows;
+    4-7 cap at 72, or at 64 with bit 0)."""
     made = {}
 
     def get(cfg):
@@ -228,7 +229,7 @@ def test_fp16_tile_hop_bit_identical(ctx_single, ctx_tiles, clg, cfg, dims, nrhs
         np.testing.assert_array_equal(outs[0][r], outs[1][r])
 
 
-@pytest.mark.parametrize("cfg", ["8:1", "3:0", "4:3"])
+@pytest.mark.parametrize("cfg", ["8:1", "3:0", "4:3", "4:6", "4:5"])
 def test_fp16_tile_cg_epilogues(ctx_single, ctx_tiles, clg, oracle, cfg):
     """The fused CGNE iteration with the tile form's epilogues (CgHopAlpha,
     CgHopUpdate reduced per tile and in two levels) converges like the one-rhs
