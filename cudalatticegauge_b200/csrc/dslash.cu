@@ -271,15 +271,33 @@ cudaError_t launch_wilson_auto(clg_context_s* ctx, const HopArgs& a, bool dagger
 template <int P, int RECON>
 cudaError_t launch_staggered(clg_context_s* ctx, const HopArgs& a, int nrhs, const std::string& key) {
   // config = block size | (variant << 16): 0 uncapped, 1 capped at 80 registers
+  // variants 16..19 (FP64 / FP32, several rhs): the tile form, v & 1 the
+  // register cap (128 FP64, 80 FP32), v & 2 the blocked tile order
   auto go = [&](int cfg) {
     const int bs = cfg & 0xffff;
+    const int v = cfg >> 16;
+    if constexpr (P != P16) {
+      if (v >= 16) {
+        constexpr int CAP = P == P64 ? 2 : 3;
+        HopArgs at = a;
+        at.tile_rows = (v & 2) ? tile_rows(a.g, a.nrhs, TILE16, P == P64 ? 48 : 24) : 0;
+        dim3 tg((unsigned)((a.g.Vh + TILE16 - 1) / TILE16));
+        if (v & 1) return launch_pdl(ctx, staggered_tile_kernel<P, RECON, CAP>, tg, dim3(bs), 0, at);
+        return launch_pdl(ctx, staggered_tile_kernel<P, RECON, 1>, tg, dim3(bs), 0, at);
+      }
+    }
     dim3 grid((unsigned)(((a.g.Vh + bs - 1) / bs) * nrhs));
-    if ((cfg >> 16) == 1) return launch_pdl(ctx, staggered_hop_kernel_capped<P, RECON>, grid, dim3(bs), 0, a);
+    if (v == 1) return launch_pdl(ctx, staggered_hop_kernel_capped<P, RECON>, grid, dim3(bs), 0, a);
     return launch_pdl(ctx, staggered_hop_kernel<P, RECON>, grid, dim3(bs), 0, a);
   };
+  if (ctx->hop_config >= 0 && (P != P16 || (ctx->hop_config >> 16) < 16)) return go(ctx->hop_config);
   std::vector<int> cand = {64, 128, 256};
   if (P == P64)
     for (int bs : {64, 128, 256}) cand.push_back(bs | (1 << 16));
+  if (P != P16 && nrhs >= 2)
+    for (int w : tile_warps(nrhs))
+      for (int v = 0; v < (tile_rows(a.g, nrhs, TILE16, P == P64 ? 48 : 24) ? 4 : 2); ++v)
+        cand.push_back((32 * w) | ((16 + v) << 16));
   return go(tune_block(ctx, key, idempotent(a), go, cand));
 }
 

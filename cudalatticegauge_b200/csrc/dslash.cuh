@@ -1574,6 +1574,30 @@ __device__ __forceinline__ float load_color16(const void* __restrict__ base, con
   return __ldg(nrm + h);
 }
 
+// out = [scale *] (a H in + xa x) at (rhs, h), stored
+template <int P, typename AT>
+__device__ __forceinline__ void staggered_finish_store(const HopArgs& a, int rhs, int64_t h, cpx<AT> acc[3]) {
+  const int64_t Vh = a.g.Vh;
+  const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) acc[k] = ca * acc[k];
+  if (a.x) {
+    cpx<AT> xv[3];
+    const char* xp = reinterpret_cast<const char*>(a.x) + rhs * a.x_stride;
+    load_site<P, 3, AT>(xp, a.x_norm ? a.x_norm + rhs * a.x_nstride : nullptr, Vh, h, xv);
+    const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = acc[k] + cx * xv[k];
+  }
+  if (a.scale_dev) {
+    const AT sc = (AT)a.scale_dev[rhs * a.scale_stride];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = sc * acc[k];
+  }
+  store_site<P, 3, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
+                       a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
+}
+
 template <int P, int RECON>
 __device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
   using AT = typename AccT<P>::T;
@@ -1639,24 +1663,7 @@ __device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
     for (int k = 0; k < 3; ++k) acc[k] = acc[k] + sb * o[k];
   }
   }
-  const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) acc[k] = ca * acc[k];
-  if (a.x) {
-    cpx<AT> xv[3];
-    const char* xp = reinterpret_cast<const char*>(a.x) + rhs * a.x_stride;
-    load_site<P, 3, AT>(xp, a.x_norm ? a.x_norm + rhs * a.x_nstride : nullptr, Vh, h, xv);
-    const cpx<AT> cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) acc[k] = acc[k] + cx * xv[k];
-  }
-  if (a.scale_dev) {
-    const AT sc = (AT)a.scale_dev[rhs * a.scale_stride];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) acc[k] = sc * acc[k];
-  }
-  store_site<P, 3, AT>(reinterpret_cast<char*>(a.out) + rhs * a.out_stride,
-                       a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
+  staggered_finish_store<P>(a, rhs, h, acc);
 }
 
 // __launch_bounds__(256): the FP64 kernel takes 90 registers (22 warps per
@@ -1669,6 +1676,84 @@ __global__ void __launch_bounds__(256) staggered_hop_kernel(HopArgs a) {
 template <int P, int RECON>
 __global__ void __launch_bounds__(256, 3) staggered_hop_kernel_capped(HopArgs a) {
   staggered_hop_body<P, RECON>(a);
+}
+
+// The tile form of the FP64 / FP32 staggered hop for several right-hand sides
+// (the batched per-shift refinement of a multi-shift solve): the block stages
+// the 8 links of its 32 sites once (TileN, complete as load_link gives them)
+// with the neighbour indices and the signs eta_mu(x) x boundary (forward) and
+// -eta_mu(x) x boundary (backward), then its warps loop over the right-hand
+// sides.  A staggered link is 8 times the bytes of the colour vector it acts
+// on, so staging it once per tile saves most of the traffic of a one-rhs
+// launch per rhs.  Per site and rhs the arithmetic of staggered_hop_body.
+template <int P, int RECON, int MINB>
+__global__ void __launch_bounds__(256, MINB) staggered_tile_kernel(HopArgs a) {
+  using AT = typename AccT<P>::T;
+  __shared__ TileN<AT> t;
+  const int64_t h0 = tile16_index(a) * TILE16;
+  pdl_launch_dependents();
+  for (int i = threadIdx.x; i < TILE16; i += blockDim.x) {
+    const int64_t h = h0 + i;
+    uint32_t neg = 0;
+    if (h < a.g.Vh) {
+      NbrInfo nb;
+      int c[4];
+      neighbours(a.g, a.out_parity, h, nb, c);
+#pragma unroll
+      for (int mu = 0; mu < 4; ++mu) {
+        int es = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (k < mu) es += c[k];
+        const float eta = (es & 1) ? -1.f : 1.f;
+        t.nb[mu][i] = nb.hf[mu];
+        t.nb[4 + mu][i] = nb.hb[mu];
+        neg |= (eta * nb.sf[mu] < 0.f ? 1u : 0u) << mu;
+        neg |= (-eta * nb.sb[mu] < 0.f ? 1u : 0u) << (4 + mu);
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 8; ++d) t.nb[d][i] = 0;
+    }
+    t.neg[i] = neg;
+  }
+  pdl_wait();
+  if (!tile_any_live(a, 0, a.nrhs)) return;  // no barrier has been passed yet: uniform
+  __syncthreads();
+  tileN_links<P, RECON>(a.U_here, a.U_there, a.g.Vh, h0, t);
+  __syncthreads();
+  const int i = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int64_t h = h0 + i;
+  if (h >= a.g.Vh) return;  // no barrier follows
+  const int64_t Vh = a.g.Vh;
+  const uint32_t neg = t.neg[i];
+  for (int rhs = threadIdx.x >> 5; rhs < a.nrhs; rhs += nw) {
+    if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) continue;
+    const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
+    const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
+    cpx<AT> acc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = mk<AT>(0, 0);
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+      cpx<AT> v[3], u[9], o[3];
+      load_site<P, 3, AT>(in, in_norm, Vh, t.nb[mu][i], v);
+#pragma unroll
+      for (int w = 0; w < 9; ++w) u[w] = t.u[mu][w][i];
+      su3_mv<AT, false>(u, v, o);
+      const AT sf = (neg >> mu) & 1u ? (AT)-1 : (AT)1;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc[k] = acc[k] + sf * o[k];
+      load_site<P, 3, AT>(in, in_norm, Vh, t.nb[4 + mu][i], v);
+#pragma unroll
+      for (int w = 0; w < 9; ++w) u[w] = t.u[4 + mu][w][i];
+      su3_mv<AT, true>(u, v, o);
+      const AT sb = (neg >> (4 + mu)) & 1u ? (AT)-1 : (AT)1;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc[k] = acc[k] + sb * o[k];
+    }
+    staggered_finish_store<P>(a, rhs, h, acc);
+  }
 }
 
 }  // namespace clg

@@ -386,3 +386,33 @@ def test_tune_file_round_trip(clg, tmp_path):
             del os.environ["CLG_TUNE_FILE"]
         else:
             os.environ["CLG_TUNE_FILE"] = old
+
+
+@pytest.mark.parametrize("cfg", ["16:128", "19:256"])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_staggered_tile(clg, oracle, pinned, cfg, prec):
+    """The staggered tile form (links staged once per tile for all right-hand
+    sides) against the one-rhs kernel (pinned "0:128"): the same bits in FP64,
+    FP32 to its rounding; and against the oracle's D on 5 right-hand sides."""
+    m = 0.02
+    outs = []
+    for c in (pinned("0:128"), pinned(cfg)):
+        lat = clg.Lattice(c, (8, 8, 8, 16))
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60004, 1, 0.25)
+        Uh = U.CopyDataOut()
+        f64 = clg.CFieldFermionKSSU3(lat, m)
+        f = clg.CFieldFermionKSSU3(lat, m, precision=prec, nrhs=5)
+        chis = []
+        for r in range(5):
+            f64.InitialField(clg.SOURCE_GAUSS, 970 + r, 2)
+            chis.append(f64.to_numpy())
+            f.from_numpy(chis[-1], r)
+        f.D(U)
+        outs.append([f.to_numpy(r) for r in range(5)])
+    for r in range(5):
+        if prec == 0:
+            np.testing.assert_array_equal(outs[0][r], outs[1][r])
+        else:
+            assert rel(outs[1][r], outs[0][r]) < 2e-6
+        assert rel(outs[1][r], oracle.ks_D((8, 8, 8, 16), Uh, chis[r], m)) < (1e-12 if prec == 0 else 2e-6)
