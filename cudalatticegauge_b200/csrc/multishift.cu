@@ -40,24 +40,43 @@ clg_status gmres_ms_run(clg_context_s* ctx, std::unique_ptr<SolveCacheBase>& cac
                         double tol, const FieldRef** X_out, int* apps_out, int* cycles_out);
 
 constexpr int CGM_MAXSHIFT = 64;
+constexpr int CGM_RING_MAX = 8;
 
+// Ring length M of the deferred shift updates: the flush holds M residuals of
+// a site in registers (M * NC complex doubles).
+constexpr int cgm_ring(int nc) { return nc == 3 ? 8 : 2; }
+
+// Device state of a multi-shift CG.  The shifted vectors x_k, p_k are not
+// touched every iteration: within a block of M iterations starting at s they
+// are kept as coefficients over the materialised p_k^s and the block's
+// residuals r_{s+1..s+M} (the base residual ring),
+//   p_k^j = cg_k p_k^s + sum_u cc_k[u] r_{s+u},
+//   x_k^j = x_k^s + ch_k p_k^s + sum_u ce_k[u] r_{s+u},
+// and one flush per block writes x_k^{s+M}, p_k^{s+M}.
 struct CgmState {
   double rr, bb, tol2, alpha, alpha_old, beta, pq;
-  int iters, done, nshift, pad;
+  int iters, done, nshift, nvalid;  // nvalid: residuals of the current block in the ring
   double shift[CGM_MAXSHIFT];
   double zeta[CGM_MAXSHIFT], zeta_old[CGM_MAXSHIFT], zeta_new[CGM_MAXSHIFT];
-  double alpha_k[CGM_MAXSHIFT], beta_k[CGM_MAXSHIFT];
+  double alpha_k[CGM_MAXSHIFT];
   int active[CGM_MAXSHIFT];
-  int upd_x[CGM_MAXSHIFT];  // x_k takes alpha_k p_k in this iteration (active when alpha_k was formed)
+  int pend_x[CGM_MAXSHIFT];  // x_k has updates in this block
+  int pend_p[CGM_MAXSHIFT];  // p_k is needed after this block (shift still iterating)
+  double cg[CGM_MAXSHIFT], ch[CGM_MAXSHIFT];
+  double cc[CGM_MAXSHIFT][CGM_RING_MAX + 1], ce[CGM_MAXSHIFT][CGM_RING_MAX + 1];
 };
 
 namespace {
 
-// (p, q) -> alpha and the shifted alpha_k (Jegerlehner eq. for zeta_{n+1})
+// (p, q) -> alpha and the shifted alpha_k (Jegerlehner eq. for zeta_{n+1});
+// x_k^{j+1} = x_k^j + alpha_k p_k^j goes into the block coefficients.  t is
+// the iteration's position in its block (t = 0 opens a block: the previous
+// one was flushed).
 template <int P, int NC>
 struct CgmAlpha {
   DField p, q;
   CgmState* st;
+  int t;
   __device__ bool active(int) const { return !st->done; }
   __device__ void operator()(int, int par, int64_t h, double* acc) const {
     using AT = typename AccT<P>::T;
@@ -72,8 +91,16 @@ struct CgmAlpha {
   __device__ void finalize(int, const double* s) const {
     CgmState& c = *st;
     // runs on every replayed iteration, also once all shifts are done, so a
-    // finished solve never repeats its last x update
-    for (int k = 0; k < c.nshift; ++k) c.upd_x[k] = 0;
+    // flushed block is never applied twice
+    if (t == 0) {
+      c.nvalid = 0;
+      for (int k = 0; k < c.nshift; ++k) {
+        c.pend_x[k] = c.pend_p[k] = 0;
+        c.cg[k] = 1.0;
+        c.ch[k] = 0.0;
+        for (int u = 0; u <= CGM_RING_MAX; ++u) c.cc[k][u] = c.ce[k][u] = 0.0;
+      }
+    }
     if (c.done) return;
     c.iters += 1;
     if (!(s[0] > 0.0) || bad(s[0])) {
@@ -82,33 +109,39 @@ struct CgmAlpha {
     }
     const double alpha = c.rr / s[0];
     for (int k = 0; k < c.nshift; ++k) {
-      c.upd_x[k] = c.active[k];
       if (!c.active[k]) continue;
       const double zn = c.zeta[k], zo = c.zeta_old[k];
       const double den = alpha * c.beta * (zo - zn) + zo * c.alpha_old * (1.0 + c.shift[k] * alpha);
       const double znew = zn * zo * c.alpha_old / den;
       c.zeta_new[k] = znew;
-      c.alpha_k[k] = alpha * znew / zn;
+      const double ak = alpha * znew / zn;
+      c.alpha_k[k] = ak;
+      c.ch[k] += ak * c.cg[k];
+      for (int u = 1; u <= t; ++u) c.ce[k][u] += ak * c.cc[k][u];
+      c.pend_x[k] = 1;
     }
     c.alpha = alpha;
   }
 };
 
-// r -= alpha q ; |r|^2 -> beta, beta_k, convergence per shift
+// r_{j+1} = r_j - alpha q (ring slots t -> t + 1 mod M); |r|^2 -> beta,
+// beta_k, p_k^{j+1} = zeta_k r_{j+1} + beta_k p_k^j into the coefficients,
+// convergence per shift
 template <int P, int NC>
 struct CgmR {
-  DField r, q;
+  DField ring, q;
   CgmState* st;
+  int t, M;
   __device__ bool active(int) const { return !st->done; }
   __device__ void operator()(int, int par, int64_t h, double* acc) const {
     using AT = typename AccT<P>::T;
     cpx<AT> vr[NC], vq[NC];
-    ldv<P, NC, AT>(r, 0, par, h, vr);
+    ldv<P, NC, AT>(ring, t, par, h, vr);
     ldv<P, NC, AT>(q, 0, par, h, vq);
     const AT a = (AT)st->alpha;
 #pragma unroll
     for (int i = 0; i < NC; ++i) vr[i] = vr[i] - a * vq[i];
-    stv<P, NC, AT>(r, 0, par, h, vr);
+    stv<P, NC, AT>(ring, (t + 1) % M, par, h, vr);
     acc[0] += site_norm2<NC, AT>(vr);
   }
   __device__ void finalize(int, const double* s) const {
@@ -118,18 +151,25 @@ struct CgmR {
       c.done = 2;
       return;
     }
+    c.nvalid = t + 1;
     const double beta = s[0] / c.rr;
     int nact = 0;
     for (int k = 0; k < c.nshift; ++k) {
       if (!c.active[k]) continue;
       const double ratio = c.zeta_new[k] / c.zeta[k];
-      c.beta_k[k] = beta * ratio * ratio;
+      const double bk = beta * ratio * ratio;
       c.zeta_old[k] = c.zeta[k];
       c.zeta[k] = c.zeta_new[k];
-      if (c.zeta[k] * c.zeta[k] * s[0] <= c.tol2 * c.bb)
+      c.cg[k] *= bk;
+      for (int u = 1; u <= t; ++u) c.cc[k][u] *= bk;
+      c.cc[k][t + 1] = c.zeta[k];
+      if (c.zeta[k] * c.zeta[k] * s[0] <= c.tol2 * c.bb) {
         c.active[k] = 0;
-      else
+        c.pend_p[k] = 0;
+      } else {
+        c.pend_p[k] = 1;
         ++nact;
+      }
     }
     c.alpha_old = c.alpha;
     c.beta = beta;
@@ -138,55 +178,99 @@ struct CgmR {
   }
 };
 
-// One pass after the residual update, grid.y = nshift + 1:
-//   shift k < nshift:  x_k += alpha_k p_k ; p_k = zeta_k r + beta_k p_k
-//                      (both from the same, old p_k: the x update of the
-//                      shift loop deferred past r's update, as the algebra allows)
-//   y = nshift:        p = r + beta p
+// p = r_{j+1} + beta p (ring slot `slot`), inside a block
 template <int P, int NC>
-struct CgmUpdate {
-  DField x, pk, p, r;
+struct CgmP {
+  DField ring, p;
+  CgmState* st;
+  int slot;
+  __device__ bool active(int) const { return !st->done; }
+  __device__ void operator()(int, int par, int64_t h, double*) const {
+    using AT = typename AccT<P>::T;
+    cpx<AT> vr[NC], vp[NC];
+    ldv<P, NC, AT>(ring, slot, par, h, vr);
+    ldv<P, NC, AT>(p, 0, par, h, vp);
+    const AT b = (AT)st->beta;
+#pragma unroll
+    for (int i = 0; i < NC; ++i) vp[i] = vr[i] + b * vp[i];
+    stv<P, NC, AT>(p, 0, par, h, vp);
+  }
+  __device__ void finalize(int, const double*) const {}
+};
+
+// The block's last iteration: p = r_{s+M} + beta p, and every shift with
+// pending updates takes them from the M residuals r_{s+u} (ring slot u mod M,
+// only the nvalid written in this block):
+//   x_k += ch_k p_k + sum_u ce_k[u] r_{s+u};  p_k = cg_k p_k + sum_u cc_k[u] r_{s+u}
+// Each site's residuals are read once for all shifts.
+// The ring and p are in the iteration precision PR; x_k, p_k are FP64.
+template <int PR, int NC, int M>
+struct CgmFlush {
+  DField ring, x, pk, p;
   CgmState* st;
   int nshift;
-  __device__ bool active(int k) const {
-    if (k == nshift) return !st->done;
-    return st->upd_x[k] || (!st->done && st->active[k]);
-  }
-  __device__ void operator()(int k, int par, int64_t h, double*) const {
-    using AT = typename AccT<P>::T;
-    cpx<AT> vp[NC], vr[NC];
-    ldv<P, NC, AT>(r, 0, par, h, vr);
-    if (k == nshift) {
-      ldv<P, NC, AT>(p, 0, par, h, vp);
-      const AT b = (AT)st->beta;
+  __device__ bool active(int) const { return true; }
+  __device__ void operator()(int, int par, int64_t h, double*) const {
+    using AT = double;
+    const int nv = st->nvalid;
+    cpx<AT> rv[M][NC];
 #pragma unroll
-      for (int i = 0; i < NC; ++i) vp[i] = vr[i] + b * vp[i];
-      stv<P, NC, AT>(p, 0, par, h, vp);
-      return;
+    for (int u = 0; u < M; ++u) {
+      if (u < nv) {
+        ldv<PR, NC, AT>(ring, (u + 1) % M, par, h, rv[u]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < NC; ++i) rv[u][i] = mk<AT>(0, 0);
+      }
     }
-    ldv<P, NC, AT>(pk, k, par, h, vp);
-    if (st->upd_x[k]) {
-      cpx<AT> vx[NC];
-      ldv<P, NC, AT>(x, k, par, h, vx);
-      const AT a = (AT)st->alpha_k[k];
+    if (!st->done) {
+      cpx<AT> vp[NC];
+      ldv<PR, NC, AT>(p, 0, par, h, vp);
+      const AT b = st->beta;
 #pragma unroll
-      for (int i = 0; i < NC; ++i) vx[i] = vx[i] + a * vp[i];
-      stv<P, NC, AT>(x, k, par, h, vx);
+      for (int i = 0; i < NC; ++i) vp[i] = rv[M - 1][i] + b * vp[i];
+      stv<PR, NC, AT>(p, 0, par, h, vp);
     }
-    if (!st->done && st->active[k]) {
-      const AT z = (AT)st->zeta[k], b = (AT)st->beta_k[k];
+    for (int k = 0; k < nshift; ++k) {
+      const bool px = st->pend_x[k], pp = st->pend_p[k];
+      if (!px && !pp) continue;
+      cpx<AT> vk[NC];
+      ldv<P64, NC, AT>(pk, k, par, h, vk);
+      if (px) {
+        cpx<AT> vx[NC];
+        ldv<P64, NC, AT>(x, k, par, h, vx);
+        const AT a = st->ch[k];
 #pragma unroll
-      for (int i = 0; i < NC; ++i) vp[i] = z * vr[i] + b * vp[i];
-      stv<P, NC, AT>(pk, k, par, h, vp);
+        for (int i = 0; i < NC; ++i) vx[i] = vx[i] + a * vk[i];
+#pragma unroll
+        for (int u = 0; u < M - 1; ++u) {
+          const AT e = st->ce[k][u + 1];
+#pragma unroll
+          for (int i = 0; i < NC; ++i) vx[i] = vx[i] + e * rv[u][i];
+        }
+        stv<P64, NC, AT>(x, k, par, h, vx);
+      }
+      if (pp) {
+        const AT g = st->cg[k];
+#pragma unroll
+        for (int i = 0; i < NC; ++i) vk[i] = g * vk[i];
+#pragma unroll
+        for (int u = 0; u < M; ++u) {
+          const AT cu = st->cc[k][u + 1];
+#pragma unroll
+          for (int i = 0; i < NC; ++i) vk[i] = vk[i] + cu * rv[u][i];
+        }
+        stv<P64, NC, AT>(pk, k, par, h, vk);
+      }
     }
   }
   __device__ void finalize(int, const double*) const {}
 };
 
-// start: r = p = b, x_k = 0, p_k = b, |b|^2
+// start (FP64): r_0 = p = b (ring slot 0), x_k = 0, p_k = b, |b|^2
 template <int P, int NC>
 struct CgmInit {
-  DField b, r, p, x, pk;
+  DField b, ring, p, x, pk;
   CgmState* st;
   int nshift;
   __device__ bool active(int) const { return true; }
@@ -196,7 +280,7 @@ struct CgmInit {
     ldv<P, NC, AT>(b, 0, par, h, vb);
 #pragma unroll
     for (int i = 0; i < NC; ++i) z[i] = mk<AT>(0, 0);
-    stv<P, NC, AT>(r, 0, par, h, vb);
+    stv<P, NC, AT>(ring, 0, par, h, vb);
     stv<P, NC, AT>(p, 0, par, h, vb);
     for (int k = 0; k < nshift; ++k) {
       stv<P, NC, AT>(x, k, par, h, z);
@@ -210,13 +294,31 @@ struct CgmInit {
     c.alpha_old = 1.0;
     c.beta = 0.0;
     c.iters = 0;
+    c.nvalid = 0;
     c.done = s[0] > 0.0 ? 0 : 1;
     for (int k = 0; k < c.nshift; ++k) {
       c.zeta[k] = c.zeta_old[k] = 1.0;
       c.active[k] = c.done ? 0 : 1;
-      c.upd_x[k] = 0;
+      c.pend_x[k] = c.pend_p[k] = 0;
     }
   }
+};
+
+// A mixed solve leaves FP64 for the inner precision PR at a chunk boundary
+// (every shift vector flushed, the residual in ring slot 0): r and p change
+// precision, the iteration goes on.
+template <int PR, int NC>
+struct CgmSwitch {
+  DField ring64, p64, ring, p;
+  __device__ bool active(int) const { return true; }
+  __device__ void operator()(int, int par, int64_t h, double*) const {
+    cpx<double> v[NC];
+    ldv<P64, NC, double>(ring64, 0, par, h, v);
+    stv<PR, NC, double>(ring, 0, par, h, v);
+    ldv<P64, NC, double>(p64, 0, par, h, v);
+    stv<PR, NC, double>(p, 0, par, h, v);
+  }
+  __device__ void finalize(int, const double*) const {}
 };
 
 struct OwnedF {
@@ -247,30 +349,52 @@ struct OwnedF {
   }
 };
 
-// Buffers, device state, pinned summary and the captured iteration graph of a
+// The vectors of the shared iteration in one precision: the residual ring,
+// p, q = A p and the operator's temporaries.
+struct CgmIter {
+  OwnedF ring, p, q, t_odd, t_full;
+  cudaGraphExec_t exec = nullptr;  // a captured chunk of iterations
+  int64_t graph_kernels = 0;
+  bool tuned = false;  // one chunk ran eagerly (its launches are tuned)
+  ~CgmIter() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  clg_status alloc(clg_context_s* ctx, int P, int nc, int np, int fp, int M, int64_t Vh, int op) {
+    clg_status s;
+    if ((s = ring.alloc(ctx, P, nc, np, fp, M, Vh)) || (s = p.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
+        (s = q.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = t_odd.alloc(ctx, P, nc, 1, 1, 1, Vh)))
+      return s;
+    if (op == CLG_OP_DDDAG && (s = t_full.alloc(ctx, P, nc, 2, 0, 1, Vh))) return s;
+    return CLG_SUCCESS;
+  }
+};
+
+// Buffers, device state, pinned summary and the captured iteration graphs of a
 // multi-shift CG, kept in the solver between calls with the same shape and
 // gauge arrays (a call then costs the solve, not cudaMalloc/cudaFree, pinned
-// allocations and a graph capture).
+// allocations and a graph capture).  The solutions x_k, the shifted p_k and
+// the start vector are FP64; it[0] iterates in FP64, it[1] (mixed solves) in
+// the inner precision.
 struct CgmWork : SolveCacheBase {
   std::string key;
-  OwnedF X, bP, r, p, q, pk, t_odd, t_full;
+  OwnedF X, bP, pk;
+  CgmIter it[2];
+  int M = 1;  // ring length (residuals per flush block)
   CgmState* st = nullptr;
   CgmState* hs = nullptr;  // pinned copy read per chunk
-  cudaGraphExec_t exec = nullptr;
-  int64_t graph_kernels = 0;
   ~CgmWork() {
-    if (exec) cudaGraphExecDestroy(exec);
     dfree(st);
     if (hs) cudaFreeHost(hs);
   }
   clg_status alloc(clg_context_s* ctx, int P, int nc, int np, int fp, int ns, int64_t Vh, int op) {
     clg_status s;
-    if ((s = X.alloc(ctx, P, nc, np, fp, ns, Vh)) || (s = bP.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
-        (s = r.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = p.alloc(ctx, P, nc, np, fp, 1, Vh)) ||
-        (s = q.alloc(ctx, P, nc, np, fp, 1, Vh)) || (s = pk.alloc(ctx, P, nc, np, fp, ns, Vh)) ||
-        (s = t_odd.alloc(ctx, P, nc, 1, 1, 1, Vh)))
+    M = cgm_ring(nc);
+    if ((s = X.alloc(ctx, CLG_PREC_DOUBLE, nc, np, fp, ns, Vh)) ||
+        (s = bP.alloc(ctx, CLG_PREC_DOUBLE, nc, np, fp, 1, Vh)) ||
+        (s = pk.alloc(ctx, CLG_PREC_DOUBLE, nc, np, fp, ns, Vh)) ||
+        (s = it[0].alloc(ctx, CLG_PREC_DOUBLE, nc, np, fp, M, Vh, op)))
       return s;
-    if (op == CLG_OP_DDDAG && (s = t_full.alloc(ctx, P, nc, 2, 0, 1, Vh))) return s;
+    if (P != CLG_PREC_DOUBLE && (s = it[1].alloc(ctx, P, nc, np, fp, M, Vh, op))) return s;
     if ((s = dalloc(ctx, (void**)&st, sizeof(CgmState)))) return s;
     if (cudaMallocHost((void**)&hs, sizeof(CgmState)) != cudaSuccess) {
       hs = nullptr;
@@ -280,12 +404,46 @@ struct CgmWork : SolveCacheBase {
   }
 };
 
-// Multi-shift CG in precision P on a Hermitian positive operator; W.X receives
-// the nshift solutions.
+// One chunk of multi-shift CG iterations on the vectors I (precision PR);
+// iteration i sits at position t = i mod M of its flush block (a chunk holds
+// whole blocks, so every chunk ends with a flush).
+template <int PR, int NC>
+clg_status cgm_chunk(clg_context_s* ctx, CgmWork& W, CgmIter& I, clg_gauge_s* U, int kind, double param, int op,
+                     int fp, int np, int64_t Vh, int ns, int chunk) {
+  constexpr int MV = cgm_ring(NC);
+  CgmState* st = W.st;
+  const double2 one = make_double2(1, 0);
+  const int* skip = &st->done;
+  const FieldRef* tmp = (op == CLG_OP_DDDAG) ? &I.t_full.ref : &I.t_odd.ref;
+  for (int i = 0; i < chunk; ++i) {
+    const int t = i % MV;
+    clg_status e;
+    if ((e = apply_op(ctx, op, U, kind, param, I.q.ref, I.p.ref, tmp, one, 1, nullptr, 0, skip, 0))) return e;
+    if ((e = launch_sites<1>(ctx, CgmAlpha<PR, NC>{dfield(I.p.ref), dfield(I.q.ref), st, t}, fp, np, Vh, 1))) return e;
+    if ((e = launch_sites<1>(ctx, CgmR<PR, NC>{dfield(I.ring.ref), dfield(I.q.ref), st, t, MV}, fp, np, Vh, 1)))
+      return e;
+    if (t + 1 < MV)
+      e = launch_sites<0>(ctx, CgmP<PR, NC>{dfield(I.ring.ref), dfield(I.p.ref), st, t + 1}, fp, np, Vh, 1);
+    else
+      e = launch_sites<0>(
+          ctx, CgmFlush<PR, NC, MV>{dfield(I.ring.ref), dfield(W.X.ref), dfield(W.pk.ref), dfield(I.p.ref), st, ns},
+          fp, np, Vh, 1);
+    if (e) return e;
+  }
+  return CLG_SUCCESS;
+}
+
+// Multi-shift CG on a Hermitian positive operator to the recursive target
+// tol for every shift; W.X receives the nshift FP64 solutions.  The shared
+// iteration runs in FP64 until |r| <= lo_from |b| and in the inner precision P
+// after that (P = FP64: FP64 throughout).  The shifted residuals are
+// collinear with the shared one only up to the rounding of the iterations
+// that made them, so the early iterations, where |r| is large, are the FP64
+// ones.
 clg_status cgm_run(clg_context_s* ctx, CgmWork& W, clg_gauge_s* U, int kind, double param, int op, const FieldRef& b,
-                   const std::vector<double>& shifts, double tol, int max_iter, int* iters_out) {
-  const FieldRef& X = W.X.ref;
-  const int P = X.prec, nc = X.nc, np = b.nparity, fp = b.first_parity;
+                   const std::vector<double>& shifts, int P, double tol, double lo_from, int max_iter,
+                   int* iters_out) {
+  const int nc = W.X.ref.nc, np = b.nparity, fp = b.first_parity;
   const int64_t Vh = b.Vh;
   const int ns = (int)shifts.size();
   clg_status s;
@@ -298,51 +456,55 @@ clg_status cgm_run(clg_context_s* ctx, CgmWork& W, clg_gauge_s* U, int kind, dou
   for (int k = 0; k < ns; ++k) h.shift[k] = shifts[k];
   if (cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
     return ctx->fail(CLG_ERR_CUDA, "multi-shift: state upload");
-  const double2 one = make_double2(1, 0);
-  const int* skip = &st->done;
+  const bool mixed = P != CLG_PREC_DOUBLE;
   return with_pn(P, nc, [&](auto PP, auto NN) -> clg_status {
     constexpr int PV = PP.value, NV = NN.value;
-    clg_status e = launch_sites<1>(ctx, CgmInit<PV, NV>{dfield(W.bP.ref), dfield(W.r.ref), dfield(W.p.ref), dfield(X),
-                                                         dfield(W.pk.ref), st, ns},
+    CgmIter& I64 = W.it[0];
+    clg_status e = launch_sites<1>(ctx, CgmInit<P64, NV>{dfield(W.bP.ref), dfield(I64.ring.ref), dfield(I64.p.ref),
+                                                          dfield(W.X.ref), dfield(W.pk.ref), st, ns},
                                    fp, np, Vh, 1);
     if (e) return e;
-    const int chunk = 16;
-    auto body = [&]() -> clg_status {
-      clg_status e2;
-      const FieldRef* tmp = (op == CLG_OP_DDDAG) ? &W.t_full.ref : &W.t_odd.ref;
-      if ((e2 = apply_op(ctx, op, U, kind, param, W.q.ref, W.p.ref, tmp, one, 1, nullptr, 0, skip, 0))) return e2;
-      if ((e2 = launch_sites<1>(ctx, CgmAlpha<PV, NV>{dfield(W.p.ref), dfield(W.q.ref), st}, fp, np, Vh, 1))) return e2;
-      if ((e2 = launch_sites<1>(ctx, CgmR<PV, NV>{dfield(W.r.ref), dfield(W.q.ref), st}, fp, np, Vh, 1))) return e2;
-      CgmUpdate<PV, NV> up{dfield(X), dfield(W.pk.ref), dfield(W.p.ref), dfield(W.r.ref), st, ns};
-      return launch_sites<0>(ctx, up, fp, np, Vh, ns + 1);
+    int phase = 0;  // 0: FP64 iterations, 1: inner precision
+    auto to_lo = [&]() -> clg_status {
+      phase = 1;
+      CgmIter& IL = W.it[1];
+      return launch_sites<0>(ctx, CgmSwitch<PV, NV>{dfield(I64.ring.ref), dfield(I64.p.ref), dfield(IL.ring.ref),
+                                                    dfield(IL.p.ref)},
+                             fp, np, Vh, 1);
     };
+    if (mixed && !(lo_from < 1.0) && (e = to_lo())) return e;
+    const int chunk = 16;
     int done = 0, it = 0;
-    e = CLG_SUCCESS;
     for (int c = 0; c * chunk < max_iter + chunk; ++c) {
-      // the first chunk of the first call runs eagerly (it tunes the launches);
-      // the second captures the chunk, later chunks and calls replay it
-      if (c == 1 && !W.exec && ctx->stream) {
+      CgmIter& I = W.it[phase];
+      auto run = [&]() -> clg_status {
+        if (phase == 0) return cgm_chunk<P64, NV>(ctx, W, I, U, kind, param, op, fp, np, Vh, ns, chunk);
+        return cgm_chunk<PV, NV>(ctx, W, I, U, kind, param, op, fp, np, Vh, ns, chunk);
+      };
+      // a phase's first chunk runs eagerly (it tunes the launches); its second
+      // captures the chunk, later chunks and calls replay it
+      if (!I.exec && I.tuned && ctx->stream) {
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
           const int64_t k0 = ctx->kernels;  // captured launches are counted per replay
-          for (int i = 0; i < chunk && !e; ++i) e = body();
-          W.graph_kernels = ctx->kernels - k0;
+          e = run();
+          I.graph_kernels = ctx->kernels - k0;
           ctx->kernels = k0;
-          if (cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && g && !e) cudaGraphInstantiate(&W.exec, g, 0);
+          if (cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && g && !e) cudaGraphInstantiate(&I.exec, g, 0);
           if (g) cudaGraphDestroy(g);
           cudaGetLastError();
         }
       }
       if (e) break;
-      if (W.exec) {
-        if (cudaGraphLaunch(W.exec, ctx->stream) != cudaSuccess) {
+      if (I.exec) {
+        if (cudaGraphLaunch(I.exec, ctx->stream) != cudaSuccess) {
           e = ctx->fail(CLG_ERR_CUDA, "multi-shift graph launch");
           break;
         }
-        ctx->kernels += W.graph_kernels;
+        ctx->kernels += I.graph_kernels;
       } else {
-        for (int i = 0; i < chunk && !e; ++i) e = body();
-        if (e) break;
+        if ((e = run())) break;
+        I.tuned = true;
       }
       if (cudaMemcpyAsync(W.hs, st, sizeof(CgmState), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
           cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
@@ -352,6 +514,7 @@ clg_status cgm_run(clg_context_s* ctx, CgmWork& W, clg_gauge_s* U, int kind, dou
       done = W.hs->done;
       it = W.hs->iters;
       if (done || it >= max_iter) break;
+      if (mixed && phase == 0 && W.hs->rr <= lo_from * lo_from * W.hs->bb && (e = to_lo())) break;
     }
     *iters_out = it;
     return e;
@@ -428,12 +591,10 @@ clg_status clg_solve_multishift(clg_solver S, clg_field* x, int nshift, const do
       }
       W->key = key;
     }
-    // recursive-residual target of the multi-shift phase: the FP64 tolerance
-    // itself in FP64; inner_tol (floored where the precision's recurrences
-    // stop tracking the true residual) in FP32 / FP16
-    const double itol = P == CLG_PREC_DOUBLE ? prm.tol_true_rel * 0.5
-                                             : std::max(prm.inner_tol, P == CLG_PREC_SINGLE ? 1e-9 : 1e-4);
-    if ((s = cgm_run(ctx, *W, g, b->kind, b->param, op, b->ref(), real, itol, prm.max_iterations, &cgm_iters)))
+    // every shift to half the FP64 tolerance in the shared iteration; a
+    // mixed solve leaves FP64 once |r| <= inner_tol |b|
+    if ((s = cgm_run(ctx, *W, g, b->kind, b->param, op, b->ref(), real, P, prm.tol_true_rel * 0.5, prm.inner_tol,
+                     prm.max_iterations, &cgm_iters)))
       return s;
     prm.kind = CLG_SOLVER_CG;  // per-shift refinement
   } else if (S->p.kind == CLG_SOLVER_FOM_MS || S->p.kind == CLG_SOLVER_BICGSTAB_MS ||

@@ -27,6 +27,67 @@ def test_staggered_cgm_12_shifts(ctx, clg, oracle):
         assert op.true_residual(bh, xs[k].to_numpy(), complex(s)) <= TOL
 
 
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_staggered_cgm_iterates_like_oracle(ctx, clg, oracle, prec):
+    """Multi-shift CG with the shifted x_k, p_k written once per block of
+    iterations (coefficients over the block's residuals): every shift at the
+    FP64 true residual in every inner precision; in FP64 the shared Krylov
+    space takes the oracle's iteration count (same stopping rule) and the
+    solutions agree.  12 shifts on 8^3x4 (a solve that ends inside a block)."""
+    lat = clg.Lattice(ctx, (8, 8, 8, 4))
+    m = 0.02
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60071, 1, 0.25)
+    b = clg.CFieldFermionKSSU3(lat, m, subset=clg.EVEN)
+    b.InitialField(clg.SOURCE_GAUSS, 0xC1A60072, 2)
+    shifts = np.logspace(-3, 1, 12)
+    xs = [clg.CFieldFermionKSSU3(lat, m, subset=clg.EVEN) for _ in shifts]
+    S = clg.CMultiShiftCG(ctx, inner_precision=prec)
+    infos = S.Solve(xs, list(shifts), b, U, clg.OP_DDDAG_EE)
+    op = oracle.Operator("KS_DDDAG_EE", lat.dims, U.CopyDataOut(), m)
+    bh = b.to_numpy()
+    for k, s in enumerate(shifts):
+        assert infos[k]["status"] == 0
+        assert op.true_residual(bh, xs[k].to_numpy(), complex(s)) <= TOL
+    if prec == 0:
+        xo, io = oracle.cgm(op, bh, list(shifts), tol=0.5 * TOL)
+        assert abs(min(i["iterations"] for i in infos) - io["iterations"]) <= 1, (infos, io)
+        for k in range(len(shifts)):
+            assert np.linalg.norm(xs[k].to_numpy() - xo[k]) <= 1e-9 * np.linalg.norm(xo[k])
+    # a second call on the same solver replays the captured iterations
+    again = S.Solve(xs, list(shifts), b, U, clg.OP_DDDAG_EE)
+    for k, s in enumerate(shifts):
+        assert again[k]["status"] == 0
+        assert op.true_residual(bh, xs[k].to_numpy(), complex(s)) <= TOL
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_wilson_cgm(ctx, clg, oracle, prec):
+    """Multi-shift CG on the Wilson DD^+ (12 spin-colour components: a shorter
+    flush block) with 5 shifts, every shift to the FP64 true residual; FP64
+    takes the oracle's iteration count."""
+    lat = clg.Lattice(ctx, (4, 4, 6, 8))
+    kappa = 0.13
+    U = clg.CFieldGaugeSU3(lat)
+    U.InitialField(clg.GAUGE_EXPH, 0xC1A60073, 1, 0.25)
+    b = clg.CFieldFermionWilsonSquareSU3(lat, kappa)
+    b.InitialField(clg.SOURCE_GAUSS, 0xC1A60074, 2)
+    shifts = [0.003, 0.05, 0.4, 2.0, 9.0]
+    xs = [clg.CFieldFermionWilsonSquareSU3(lat, kappa) for _ in shifts]
+    S = clg.CMultiShiftCG(ctx, inner_precision=prec)
+    infos = S.Solve(xs, shifts, b, U, clg.EFO_F_DDdagger)
+    op = oracle.Operator("WILSON_DDDAG", lat.dims, U.CopyDataOut(), kappa)
+    bh = b.to_numpy()
+    for k, s in enumerate(shifts):
+        assert infos[k]["status"] == 0
+        assert op.true_residual(bh, xs[k].to_numpy(), complex(s)) <= TOL
+    if prec == 0:
+        xo, io = oracle.cgm(op, bh, shifts, tol=0.5 * TOL)
+        assert abs(min(i["iterations"] for i in infos) - io["iterations"]) <= 1, (infos, io)
+        for k in range(len(shifts)):
+            assert np.linalg.norm(xs[k].to_numpy() - xo[k]) <= 1e-9 * np.linalg.norm(xo[k])
+
+
 @pytest.mark.parametrize("op,name", [("EFO_F_D", "WILSON_D"), ("EFO_F_Ddagger", "WILSON_DDAG"),
                                      ("EFO_F_DDdagger", "WILSON_DDDAG")])
 @pytest.mark.parametrize("method", ["FOM", "GMRES", "BiCGStab"])
