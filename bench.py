@@ -1254,6 +1254,20 @@ def profile_driver(args):
             pd[k].InitialField(clg.SOURCE_GAUSS, 8, 2 + k)
         for _ in range(args.steps):
             clg.CFieldFermionKSSU3.DerivateD0(F, U, pi, pd, np.logspace(-3, 0.5, 12))
+    elif args.profile.startswith("multishift"):
+        # the 12-shift staggered solve of staggered_multishift (32^3x16)
+        lat = clg.Lattice(ctx, (32, 32, 32, 16))
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60004, 1, 0.25)
+        b = clg.CFieldFermionKSSU3(lat, 0.02, subset=clg.EVEN)
+        b.InitialField(clg.SOURCE_GAUSS, 0xC1A60004, 2)
+        shifts = [10.0 ** (-4 + 5 * k / 11) for k in range(12)]
+        xs = [clg.CFieldFermionKSSU3(lat, 0.02, subset=clg.EVEN) for _ in shifts]
+        prec = clg.DOUBLE if args.profile == "multishift-double" else clg.SINGLE
+        S = clg.CMultiShiftCG(ctx, inner_precision=prec, tol_true_rel=TOL)
+        for _ in range(args.steps):
+            infos = S.Solve(xs, shifts, b, U, clg.OP_DDDAG_EE)
+            print(max(i["iterations"] for i in infos), max(i["true_rel_residual"] for i in infos), flush=True)
     else:
         b = clg.CFieldFermionWilsonSquareSU3(lat, W["kappa"], nrhs=W["nrhs"])
         for r in range(W["nrhs"]):
@@ -1287,7 +1301,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched config-4 side measurements")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the config-3 Dslash and config-5 staggered multi-shift side measurements")
-    ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve", "force", "ks-force"],
+    ap.add_argument("--profile", default=None, choices=["hop-double", "hop-single", "hop-half", "solve", "force", "ks-force",
+                             "multishift", "multishift-double"],
                     help="profiling driver (no JSON line): `--steps` hop launches on the workload lattice, "
                          "or `--steps` solves without warm-up")
     args = ap.parse_args()

@@ -7,11 +7,22 @@
 // partials in a fixed strided order followed by a fixed shuffle / shared-memory
 // tree, so the result does not depend on which block finished last, and hands
 // the totals to f.finalize(rhs, tot) on the device.  The ticket is reset for
-// the next launch on the same stream.
+// the next launch on the same stream.  A functor with a member
+// finalize_warp(rhs, tot, lane) has it run by the 32 lanes of warp 0 instead
+// (scalar updates over many independent entries, e.g. the shifts of a
+// multi-shift solve, then take one round of global-memory latency, not one
+// per entry).
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 namespace clg {
+
+template <class F, class = void>
+struct has_warp_finalize : std::false_type {};
+template <class F>
+struct has_warp_finalize<F, std::void_t<decltype(&F::finalize_warp)>> : std::true_type {};
 
 // The last block's part: totals per right-hand side -> f.finalize.  Called by
 // every thread of that block (at most 256 threads, 8 warps).
@@ -24,6 +35,44 @@ __device__ __forceinline__ void grid_final_reduce(const F& f, unsigned nslots, i
   const int nw = (blockDim.x + 31) >> 5;
   // U independent partial loads in flight per thread and step (fixed order)
   constexpr int U = NRED >= 8 ? 1 : 8 / NRED;
+  if constexpr (!has_warp_finalize<F>::value) {
+    // several right-hand sides: warp w sums and finalises rhs w, w + nw, ...
+    // (each finalize touches only its own rhs's state), so the finalize
+    // latencies of up to nw right-hand sides overlap and no block barrier
+    // separates them
+    if (nrhs > 1) {
+      for (int r = warp; r < nrhs; r += nw) {
+        double s[NRED];
+#pragma unroll
+        for (int k = 0; k < NRED; ++k) s[k] = 0.0;
+        const double* pr = partials + (int64_t)r * nslots * NRED;
+        const unsigned ns = rhs_sites ? (unsigned)min((int64_t)nslots, (rhs_sites[r] + blockDim.x - 1) / blockDim.x)
+                                      : nslots;
+        for (unsigned b0 = lane; b0 < ns; b0 += U * 32) {
+          double v[U][NRED];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const unsigned b = b0 + u * 32;
+#pragma unroll
+            for (int k = 0; k < NRED; ++k) v[u][k] = b < ns ? __ldcg(pr + (int64_t)b * NRED + k) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k = 0; k < NRED; ++k) s[k] += v[u][k];
+        }
+#pragma unroll
+        for (int k = 0; k < NRED; ++k) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_down_sync(0xffffffffu, s[k], o);
+        }
+        if (lane == 0) f.finalize(r, s);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) *counter = 0u;
+      return;
+    }
+  }
   for (int r = 0; r < nrhs; ++r) {
     double s[NRED];
 #pragma unroll
@@ -59,7 +108,11 @@ __device__ __forceinline__ void grid_final_reduce(const F& f, unsigned nslots, i
       tot[threadIdx.x] = v;
     }
     __syncthreads();
-    if (threadIdx.x == 0) f.finalize(r, tot);
+    if constexpr (has_warp_finalize<F>::value) {
+      if (threadIdx.x < 32) f.finalize_warp(r, tot, (int)threadIdx.x);
+    } else {
+      if (threadIdx.x == 0) f.finalize(r, tot);
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) *counter = 0u;
