@@ -1598,18 +1598,13 @@ __device__ __forceinline__ void staggered_finish_store(const HopArgs& a, int rhs
                        a.out_norm ? a.out_norm + rhs * a.out_nstride : nullptr, Vh, h, acc);
 }
 
+// H in at output site h of right-hand side rhs (the sum over the 8 links,
+// before the coefficients of the finish)
 template <int P, int RECON>
-__device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
+__device__ __forceinline__ void staggered_hop_site(const HopArgs& a, int rhs, int64_t h,
+                                                   cpx<typename AccT<P>::T> acc[3]) {
   using AT = typename AccT<P>::T;
   const int64_t Vh = a.g.Vh;
-  // right-hand sides are interleaved in blockIdx.x so that the CTAs of all rhs
-  // for the same sites run back to back and share the links through L2
-  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
-  const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
-  pdl_launch_dependents();
-  pdl_wait();
-  if (h >= Vh) return;
-  if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
   const char* in = reinterpret_cast<const char*>(a.in) + rhs * a.in_stride;
   const float* in_norm = a.in_norm ? a.in_norm + rhs * a.in_nstride : nullptr;
 
@@ -1617,7 +1612,6 @@ __device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
   int c[4];
   neighbours(a.g, a.out_parity, h, nb, c);
 
-  cpx<AT> acc[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) acc[k] = mk<AT>(0, 0);
   if constexpr (P == P16) {
@@ -1663,7 +1657,56 @@ __device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
     for (int k = 0; k < 3; ++k) acc[k] = acc[k] + sb * o[k];
   }
   }
+}
+
+template <int P, int RECON>
+__device__ __forceinline__ void staggered_hop_body(const HopArgs& a) {
+  using AT = typename AccT<P>::T;
+  // right-hand sides are interleaved in blockIdx.x so that the CTAs of all rhs
+  // for the same sites run back to back and share the links through L2
+  const int rhs = (int)(blockIdx.x % (unsigned)a.nrhs);
+  const int64_t h = (int64_t)(blockIdx.x / (unsigned)a.nrhs) * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait();
+  if (h >= a.g.Vh) return;
+  if (a.skip_dev && a.skip_dev[(int64_t)rhs * a.skip_stride]) return;
+  cpx<AT> acc[3];
+  staggered_hop_site<P, RECON>(a, rhs, h, acc);
   staggered_finish_store<P>(a, rhs, h, acc);
+}
+
+// The staggered hop of one right-hand side with its xpay source x and a fused
+// reduction: out = a H in + xa x is stored, and the last block hands
+// Re sum_h <x(h), out(h)> (FP64 over the grid, out as stored: FP64 / FP32) to
+// E::finalize(0, tot) / E::finalize_warp on the device.  The second hop of the
+// Schur operator (2am)^2 p - H_eo H_oe p then yields (p, A p) of a CG
+// iteration without a separate pass over p and A p.  Every thread reaches the
+// reduction; a skipped right-hand side (skip_dev) contributes zero, and E's
+// finalize still runs.
+template <int P, int RECON, int MINB, class E>
+__global__ void __launch_bounds__(256, MINB) staggered_hop_xdot_kernel(HopArgs a, E e, double* partials,
+                                                                      unsigned* counter) {
+  static_assert(P != P16, "the FP16 result is rounded when stored: reduce it from memory");
+  using AT = typename AccT<P>::T;
+  const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait();
+  double red[1] = {0.0};
+  if (!(a.skip_dev && a.skip_dev[0]) && h < a.g.Vh) {
+    cpx<AT> acc[3], xv[3];
+    staggered_hop_site<P, RECON>(a, 0, h, acc);
+    load_site<P, 3, AT>(reinterpret_cast<const char*>(a.x), nullptr, a.g.Vh, h, xv);
+    const cpx<AT> ca = mk<AT>((AT)a.a.x, (AT)a.a.y), cx = mk<AT>((AT)a.xa.x, (AT)a.xa.y);
+    AT re = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      acc[k] = ca * acc[k] + cx * xv[k];
+      re += xv[k].x * acc[k].x + xv[k].y * acc[k].y;
+    }
+    store_site<P, 3, AT>(reinterpret_cast<char*>(a.out), nullptr, a.g.Vh, h, acc);
+    red[0] = (double)re;
+  }
+  grid_reduce_finalize<1>(red, e, 0, blockIdx.x, gridDim.x, 1, partials, counter);
 }
 
 // __launch_bounds__(256): the FP64 kernel takes 90 registers (22 warps per

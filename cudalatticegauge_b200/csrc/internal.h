@@ -94,7 +94,8 @@ struct clg_context_s {
   // 0 plain, 1 register-capped; block 64, 128 or 256); -1 lets the autotuner choose
   int hop_config = -1;
   // CG on the Wilson normal equations fuses its vector work into the Schur
-  // hops; CLG_FUSED_CG=0 runs the separate kernels instead
+  // hops, and multi-shift CG on the staggered (DD^+)_ee its (p, A p) (FP64 /
+  // FP32 iterations); CLG_FUSED_CG=0 runs the separate kernels instead
   bool fused_cg = true;
   // the outer residual r = b - D x of Wilson solves fused into the FP64 hop
   // (with |r|^2 and the inner-precision copy); CLG_FUSED_RESID=0: separate passes

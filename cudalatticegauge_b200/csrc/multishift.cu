@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "dslash.cuh"
 #include "krylov.cuh"
 
 namespace clg {
@@ -88,39 +89,65 @@ struct CgmAlpha {
     for (int k = 0; k < NC; ++k) re += a[k].x * b[k].x + a[k].y * b[k].y;
     acc[0] += (double)re;
   }
-  __device__ void finalize(int, const double* s) const {
+  // shift k's part of the finalize; every load comes before the first store,
+  // so one round of memory latency covers them
+  __device__ void shift_alpha(CgmState& c, int k, bool go, double alpha, double beta, double aold) const {
+    constexpr int R = CGM_RING_MAX;
+    const int act = c.active[k];
+    const double zn = c.zeta[k], zo = c.zeta_old[k], sh = c.shift[k];
+    double cg = 1.0, ch = 0.0, cc[R + 1], ce[R + 1];
+#pragma unroll
+    for (int u = 1; u <= R; ++u) cc[u] = ce[u] = 0.0;
+    if (t > 0) {
+      cg = c.cg[k];
+      ch = c.ch[k];
+#pragma unroll
+      for (int u = 1; u <= R; ++u)
+        if (u <= t) {
+          cc[u] = c.cc[k][u];
+          ce[u] = c.ce[k][u];
+        }
+    } else {
+      // a block opens: the previous one was flushed
+      c.pend_x[k] = c.pend_p[k] = 0;
+      c.cg[k] = 1.0;
+      c.ch[k] = 0.0;
+#pragma unroll
+      for (int u = 0; u <= R; ++u) c.cc[k][u] = c.ce[k][u] = 0.0;
+    }
+    if (!go || !act) return;
+    const double den = alpha * beta * (zo - zn) + zo * aold * (1.0 + sh * alpha);
+    const double znew = zn * zo * aold / den;
+    const double ak = alpha * znew / zn;
+    c.zeta_new[k] = znew;
+    c.alpha_k[k] = ak;
+    c.ch[k] = ch + ak * cg;
+#pragma unroll
+    for (int u = 1; u <= R; ++u)
+      if (u <= t) c.ce[k][u] = ce[u] + ak * cc[u];
+    c.pend_x[k] = 1;
+  }
+  // warp 0 of the last block: lane l owns the shifts k = l, l + 32.  Runs on
+  // every replayed iteration, also once all shifts are done, so a flushed
+  // block is never applied twice.
+  __device__ void finalize_warp(int, const double* s, int lane) const {
     CgmState& c = *st;
-    // runs on every replayed iteration, also once all shifts are done, so a
-    // flushed block is never applied twice
-    if (t == 0) {
-      c.nvalid = 0;
-      for (int k = 0; k < c.nshift; ++k) {
-        c.pend_x[k] = c.pend_p[k] = 0;
-        c.cg[k] = 1.0;
-        c.ch[k] = 0.0;
-        for (int u = 0; u <= CGM_RING_MAX; ++u) c.cc[k][u] = c.ce[k][u] = 0.0;
+    const int ns = c.nshift, done = c.done;
+    const double rr = c.rr, beta = c.beta, aold = c.alpha_old;
+    const bool ok = s[0] > 0.0 && !bad(s[0]);
+    const bool go = !done && ok;
+    const double alpha = rr / s[0];
+    if (lane < ns) shift_alpha(c, lane, go, alpha, beta, aold);
+    if (lane + 32 < ns) shift_alpha(c, lane + 32, go, alpha, beta, aold);
+    __syncwarp();
+    if (lane == 0) {
+      if (t == 0) c.nvalid = 0;
+      if (!done) {
+        c.iters += 1;
+        if (ok) c.alpha = alpha;
+        else c.done = 2;
       }
     }
-    if (c.done) return;
-    c.iters += 1;
-    if (!(s[0] > 0.0) || bad(s[0])) {
-      c.done = 2;
-      return;
-    }
-    const double alpha = c.rr / s[0];
-    for (int k = 0; k < c.nshift; ++k) {
-      if (!c.active[k]) continue;
-      const double zn = c.zeta[k], zo = c.zeta_old[k];
-      const double den = alpha * c.beta * (zo - zn) + zo * c.alpha_old * (1.0 + c.shift[k] * alpha);
-      const double znew = zn * zo * c.alpha_old / den;
-      c.zeta_new[k] = znew;
-      const double ak = alpha * znew / zn;
-      c.alpha_k[k] = ak;
-      c.ch[k] += ak * c.cg[k];
-      for (int u = 1; u <= t; ++u) c.ce[k][u] += ak * c.cc[k][u];
-      c.pend_x[k] = 1;
-    }
-    c.alpha = alpha;
   }
 };
 
@@ -144,37 +171,54 @@ struct CgmR {
     stv<P, NC, AT>(ring, (t + 1) % M, par, h, vr);
     acc[0] += site_norm2<NC, AT>(vr);
   }
-  __device__ void finalize(int, const double* s) const {
+  // shift k's part; loads before stores (one round of memory latency).
+  // Returns whether shift k still iterates.
+  __device__ int shift_r(CgmState& c, int k, double beta, double s0, double lim) const {
+    constexpr int R = CGM_RING_MAX;
+    const int act = c.active[k];
+    const double znew = c.zeta_new[k], z = c.zeta[k], cg = c.cg[k];
+    double cc[R + 1];
+#pragma unroll
+    for (int u = 1; u <= R; ++u) cc[u] = u <= t ? c.cc[k][u] : 0.0;
+    if (!act) return 0;
+    const double ratio = znew / z;
+    const double bk = beta * ratio * ratio;
+    c.zeta_old[k] = z;
+    c.zeta[k] = znew;
+    c.cg[k] = cg * bk;
+#pragma unroll
+    for (int u = 1; u <= R; ++u)
+      if (u <= t) c.cc[k][u] = cc[u] * bk;
+    c.cc[k][t + 1] = znew;
+    const bool conv = znew * znew * s0 <= lim;
+    if (conv) c.active[k] = 0;
+    c.pend_p[k] = conv ? 0 : 1;
+    return conv ? 0 : 1;
+  }
+  // warp 0 of the last block: lane l owns the shifts k = l, l + 32
+  __device__ void finalize_warp(int, const double* s, int lane) const {
     CgmState& c = *st;
-    if (c.done) return;
+    const int ns = c.nshift, done = c.done;
+    const double rr = c.rr, lim = c.tol2 * c.bb;
+    if (done) return;
     if (bad(s[0])) {
-      c.done = 2;
+      __syncwarp();
+      if (lane == 0) c.done = 2;
       return;
     }
-    c.nvalid = t + 1;
-    const double beta = s[0] / c.rr;
+    const double beta = s[0] / rr;
     int nact = 0;
-    for (int k = 0; k < c.nshift; ++k) {
-      if (!c.active[k]) continue;
-      const double ratio = c.zeta_new[k] / c.zeta[k];
-      const double bk = beta * ratio * ratio;
-      c.zeta_old[k] = c.zeta[k];
-      c.zeta[k] = c.zeta_new[k];
-      c.cg[k] *= bk;
-      for (int u = 1; u <= t; ++u) c.cc[k][u] *= bk;
-      c.cc[k][t + 1] = c.zeta[k];
-      if (c.zeta[k] * c.zeta[k] * s[0] <= c.tol2 * c.bb) {
-        c.active[k] = 0;
-        c.pend_p[k] = 0;
-      } else {
-        c.pend_p[k] = 1;
-        ++nact;
-      }
+    if (lane < ns) nact += shift_r(c, lane, beta, s[0], lim);
+    if (lane + 32 < ns) nact += shift_r(c, lane + 32, beta, s[0], lim);
+    nact = __reduce_add_sync(0xffffffffu, nact);
+    __syncwarp();  // every lane has read rr before lane 0 replaces it
+    if (lane == 0) {
+      c.nvalid = t + 1;
+      c.alpha_old = c.alpha;
+      c.beta = beta;
+      c.rr = s[0];
+      if (nact == 0) c.done = 1;
     }
-    c.alpha_old = c.alpha;
-    c.beta = beta;
-    c.rr = s[0];
-    if (nact == 0) c.done = 1;
   }
 };
 
@@ -404,6 +448,55 @@ struct CgmWork : SolveCacheBase {
   }
 };
 
+// q = (DD^+)_ee p = (2am)^2 p - H_eo H_oe p for the staggered Schur operator
+// (FP64 / FP32) with (p, q) -> alpha (CgmAlpha) reduced in the second hop's
+// epilogue: the iteration needs no separate pass over p and q.
+template <int PR, int NC>
+clg_status cgm_schur_alpha(clg_context_s* ctx, CgmIter& I, clg_gauge_s* U, int kind, double param, CgmState* st,
+                           int t) {
+  HopSpec s1;
+  s1.kind = kind;
+  s1.prec = PR;
+  s1.dagger = false;
+  s1.out_parity = 1;
+  s1.in = I.p.ref;
+  s1.out = I.t_odd.ref;
+  s1.x = nullptr;
+  s1.a = make_double2(1, 0);
+  s1.xa = make_double2(0, 0);
+  s1.scale_dev = nullptr;
+  s1.scale_stride = 0;
+  s1.skip_dev = &st->done;
+  s1.skip_stride = 0;
+  s1.nrhs = 1;
+  if (clg_status e = hop(ctx, U, s1)) return e;
+  HopSpec s2 = s1;
+  s2.out_parity = 0;
+  s2.in = I.t_odd.ref;
+  s2.out = I.q.ref;
+  s2.x = &I.p.ref;
+  s2.a = make_double2(-1, 0);
+  s2.xa = make_double2(param * param, 0);
+  HopArgs a;
+  if (clg_status e = make_hop_args(ctx, U, s2, a)) return e;
+  const int bs = 256;
+  const int64_t nb = (a.g.Vh + bs - 1) / bs;
+  if (clg_status e = ensure_reduction(ctx, nb)) return e;
+  const CgmAlpha<PR, NC> f{dfield(I.p.ref), dfield(I.q.ref), st, t};
+  cudaError_t err;
+  if constexpr (PR == P64)
+    err = launch_pdl(ctx, staggered_hop_xdot_kernel<P64, 18, 3, CgmAlpha<PR, NC>>, dim3((unsigned)nb), dim3(bs), 0, a,
+                     f, ctx->red_partials, ctx->red_counter);
+  else if (U->recon32 == 12)
+    err = launch_pdl(ctx, staggered_hop_xdot_kernel<P32, 12, 4, CgmAlpha<PR, NC>>, dim3((unsigned)nb), dim3(bs), 0, a,
+                     f, ctx->red_partials, ctx->red_counter);
+  else
+    err = launch_pdl(ctx, staggered_hop_xdot_kernel<P32, 18, 4, CgmAlpha<PR, NC>>, dim3((unsigned)nb), dim3(bs), 0, a,
+                     f, ctx->red_partials, ctx->red_counter);
+  if (err != cudaSuccess) return ctx->fail(cuda_status(err), std::string("multi-shift hop: ") + cudaGetErrorString(err));
+  return CLG_SUCCESS;
+}
+
 // One chunk of multi-shift CG iterations on the vectors I (precision PR);
 // iteration i sits at position t = i mod M of its flush block (a chunk holds
 // whole blocks, so every chunk ends with a flush).
@@ -418,8 +511,16 @@ clg_status cgm_chunk(clg_context_s* ctx, CgmWork& W, CgmIter& I, clg_gauge_s* U,
   for (int i = 0; i < chunk; ++i) {
     const int t = i % MV;
     clg_status e;
-    if ((e = apply_op(ctx, op, U, kind, param, I.q.ref, I.p.ref, tmp, one, 1, nullptr, 0, skip, 0))) return e;
-    if ((e = launch_sites<1>(ctx, CgmAlpha<PR, NC>{dfield(I.p.ref), dfield(I.q.ref), st, t}, fp, np, Vh, 1))) return e;
+    bool fused = false;
+    if constexpr (PR != P16 && NC == 3) fused = op == CLG_OP_DDDAG_EE && ctx->fused_cg;
+    if (fused) {
+      if constexpr (PR != P16 && NC == 3)
+        if ((e = cgm_schur_alpha<PR, NC>(ctx, I, U, kind, param, st, t))) return e;
+    } else {
+      if ((e = apply_op(ctx, op, U, kind, param, I.q.ref, I.p.ref, tmp, one, 1, nullptr, 0, skip, 0))) return e;
+      if ((e = launch_sites<1>(ctx, CgmAlpha<PR, NC>{dfield(I.p.ref), dfield(I.q.ref), st, t}, fp, np, Vh, 1)))
+        return e;
+    }
     if ((e = launch_sites<1>(ctx, CgmR<PR, NC>{dfield(I.ring.ref), dfield(I.q.ref), st, t, MV}, fp, np, Vh, 1)))
       return e;
     if (t + 1 < MV)
