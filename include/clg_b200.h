@@ -289,8 +289,10 @@ clg_status clg_solve(clg_solver s, clg_field x, clg_field b, clg_gauge g, int op
 /* CMultiShiftSolver::Solve (SparseLinearAlgebra/CMultiShiftSolver.h:38-47):
  * (op + c_n) x_n = b for n < nshift; shifts_re_im holds nshift complex shifts
  * (real for CGM); x[n] must not alias b (CMultiShiftSolver.h:35).
- *   CLG_SOLVER_CGM: multi-shift CG over one Krylov space in the inner precision
- *     (Hermitian positive op, real shifts >= 0), then per-shift FP64 refinement.
+ *   CLG_SOLVER_CGM: multi-shift CG over one Krylov space (Hermitian positive
+ *     op, real shifts >= 0): the shared iteration in FP64 until |r| <= inner_tol
+ *     |b| (default 1e-4), then in the inner precision, the shifted x_n, p_n in
+ *     FP64; every shift's FP64 true residual is checked and, if needed, refined.
  *   CLG_SOLVER_FOM_MS: restarted FOM(max_dim <= 32) over one Krylov space for
  *     every complex shift, FP64 (b and x FP64), restart = cycles, stop when every
  *     shift's residual |beta_n| <= tol_true_rel |b|; then the true residuals are
