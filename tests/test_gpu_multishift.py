@@ -62,6 +62,39 @@ def test_staggered_cgm_iterates_like_oracle(ctx, clg, oracle, prec):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
+def test_staggered_cgm_fused_matches_unfused(clg, oracle, prec, monkeypatch):
+    """Multi-shift CG with (p, A p) reduced in the second hop of the staggered
+    Schur operator (the default for FP64 / FP32 iterations) against the separate
+    operator and dot passes (CLG_FUSED_CG=0): every shift at the FP64 true
+    residual in both, the same iteration count to within one (they differ only
+    in the summation order of (p, A p)), solutions within the tolerance."""
+    infos, sols = {}, {}
+    shifts = list(np.logspace(-3, 1, 8))
+    for fused in ("1", "0"):
+        monkeypatch.setenv("CLG_FUSED_CG", fused)
+        c = clg.Context(0)
+        lat = clg.Lattice(c, (8, 8, 8, 8))
+        U = clg.CFieldGaugeSU3(lat)
+        U.InitialField(clg.GAUGE_EXPH, 0xC1A60075, 1, 0.25)
+        b = clg.CFieldFermionKSSU3(lat, 0.02, subset=clg.EVEN)
+        b.InitialField(clg.SOURCE_GAUSS, 0xC1A60076, 2)
+        xs = [clg.CFieldFermionKSSU3(lat, 0.02, subset=clg.EVEN) for _ in shifts]
+        S = clg.CMultiShiftCG(c, inner_precision=prec)
+        infos[fused] = S.Solve(xs, shifts, b, U, clg.OP_DDDAG_EE)
+        op = oracle.Operator("KS_DDDAG_EE", lat.dims, U.CopyDataOut(), 0.02)
+        bh = b.to_numpy()
+        for k, s in enumerate(shifts):
+            assert infos[fused][k]["status"] == 0
+            assert op.true_residual(bh, xs[k].to_numpy(), complex(s)) <= TOL
+        sols[fused] = [x.to_numpy() for x in xs]
+        S.close()
+        c.close()
+    for k in range(len(shifts)):
+        assert abs(infos["1"][k]["iterations"] - infos["0"][k]["iterations"]) <= 1
+        assert np.linalg.norm(sols["1"][k] - sols["0"][k]) <= 1e-8 * np.linalg.norm(sols["0"][k])
+
+
+@pytest.mark.parametrize("prec", [0, 1])
 def test_wilson_cgm(ctx, clg, oracle, prec):
     """Multi-shift CG on the Wilson DD^+ (12 spin-colour components: a shorter
     flush block) with 5 shifts, every shift to the FP64 true residual; FP64
