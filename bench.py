@@ -184,6 +184,51 @@ def hop_bytes_launch(prec: int, nrhs: int) -> int:
     return (hop_bytes_per_site(prec) - links) * nrhs + links
 
 
+def cg_iteration(clg, ctx, stream, lat, U, kappa, b, inner, peak, n1=8, n2=24):
+    """The inner CG iteration of the batched solve timed live through the public
+    solver: the same FP16-inner CGNE solve of the batch b, cut off after n1 and
+    after n2 CG iterations (one defect-correction cycle; n2 below the ~24
+    iterations after which the first FP16 inner solves reach their 2e-3 floor),
+    so (t2 - t1) / (n2 - n1) is one iteration of the solve's own
+    kernels without its setup and FP64 residuals.  An iteration is the two odd
+    hops, the D^+ hop with its (p, A p) epilogue, the D hop with the x / r update
+    epilogue and p = r + beta p; its algorithmic bytes per output site and rhs
+    (FP16 spinor 52 B, the links once per hop launch): odd hops 2 x 104, alpha
+    hop 156, update hop 364 (the xpay source, x, r, p read, x, r written; A p is
+    never stored), p = r + beta p 156."""
+    import torch
+
+    nrhs, Vh = b.nrhs, lat.volume // 2
+    x = clg.CFieldFermionWilsonSquareSU3(lat, kappa, nrhs=nrhs)
+    res = {}
+    for n in (n1, n2):
+        S = clg.CSLASolverCG(ctx, inner_precision=inner, tol_true_rel=1e-30, inner_tol=1e-30, max_outer=1,
+                             max_iterations=2 * n)
+        S.Solve(x, b, U, clg.EFO_F_D, raise_on_fail=False)  # graphs captured, launches tuned
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        infos = S.Solve(x, b, U, clg.EFO_F_D, raise_on_fail=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[n] = (e0.elapsed_time(e1) / 1e3, min(i["iterations"] for i in infos) / 2,
+                  max(i["iterations"] for i in infos) / 2)
+        S.close()
+    x.close()
+    (t1, lo1, hi1), (t2, lo2, hi2) = res[n1], res[n2]
+    if lo1 != hi1 or lo2 != hi2 or lo2 <= lo1:
+        return {"unmeasured": f"iteration counts {lo1}-{hi1} / {lo2}-{hi2} (expected {n1} / {n2} for every rhs)"}
+    t_it = (t2 - t1) / (lo2 - lo1)
+    links = 8 * 12 * 2
+    per_site = 2 * 104 * nrhs + 156 * nrhs + 364 * nrhs + 156 * nrhs + 4 * links
+    alg = per_site * Vh
+    return {"us_per_iteration": round(t_it * 1e6, 1), "iterations_timed": int(lo2 - lo1),
+            "bytes_per_iteration": alg, "achieved_GB/s": round(alg / t_it / 1e9, 1),
+            "frac": round(alg / t_it / 1e9 / peak, 4),
+            "kernels": "2 odd FP16 tile hops, D^+ hop + (p, A p), D hop + x / r update, p = r + beta p",
+            "method": f"(t({n2} iterations) - t({n1} iterations)) / {n2 - n1}, CUDA events on the solver stream"}
+
+
 def time_hops(clg, ctx, lat, U, prec, stream, reps=60, nrhs=1):
     """Average device duration of the checkerboard Wilson hop (odd -> even).
 
@@ -406,6 +451,7 @@ def ours(args, world, rank, local):
 
     extra = {}
     if rank == 0 and not args.quick and nrhs > 1:
+        extra["cg_iteration_32x32x32x32"] = cg_iteration(clg, ctx, stream, lat, U, kappa, b, inner, peak)
         extra["denominators_32x32x32x32"] = denominators(clg, ctx, stream, lat, U, kappa, W, value)
         extra["single_source_32x32x32x16"] = single_source_side(clg, ctx, stream, args)
         if not args.no_batched:
