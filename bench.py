@@ -448,6 +448,20 @@ def ours(args, world, rank, local):
     if nrhs > 1:
         # the same launch counted as nrhs separate one-rhs hops (links re-read per rhs)
         roof["frac_links_per_rhs"] = round(hop_bytes_per_site(inner) * nrhs * Vh / t_hop / 1e9 / peak, 4)
+    if inner == clg.HALF:
+        # the FP16 hop's other bound: its real multiply-adds on the CUDA cores'
+        # FMA pipe (HFMA2 / FFMA2 occupy it twice as long as FFMA, so each real
+        # operation costs one lane-cycle whatever the precision): per output
+        # site and rhs 576 (colour products) + 96 (spin projections) + 192
+        # (FP32 accumulation) = 864; peak 128 lanes x SMs x SM clock
+        ops = 864 * nrhs * Vh
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        fma = {"lane_ops_per_launch": ops, "achieved_Tops": round(ops / t_hop / 1e12, 2)}
+        ck = clk if isinstance(clk, dict) else {}
+        for key, mhz in (("frac_at_sm_max_clock", ck.get("sm_max_mhz")), ("frac_at_median_clock", ck.get("sm_mhz"))):
+            if mhz:
+                fma[key] = round(ops / t_hop / (128 * sms * mhz * 1e6), 4)
+        roof["fma_pipe"] = fma
 
     extra = {}
     if rank == 0 and not args.quick and nrhs > 1:
